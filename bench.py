@@ -1,0 +1,432 @@
+"""Throughput benchmark of the B200 DSMC timestep.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+One "step" is one DSMC timestep of the whole workload (scan, scatter, cell
+kernel with collisions, move, sampling every 100 steps, inflow injection).
+The metric is particle-timesteps per second: the particles in cells summed
+over the timed steps (counted on the device) divided by the device time of
+the timed region (CUDA events, max over ranks).  With N > 1 every rank runs
+an independent replica of the workload (the timestep does not shard; the only
+cross-rank traffic is the reduction of the timings).
+
+--impl reference times the CPU restatement of the reference's step (oracle/,
+OpenMP over all host cores) on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+KB = 1.380649e-23
+ARGON = dict(gas_mass=6.63e-26, gas_diam=4.17e-10, gas_tref=273.0, gas_omega=0.81)
+
+# ------------------------------------------------------------- workloads ----
+
+
+def wl_capsule_4m():
+    """Hypersonic argon over a blunt capsule, 4M particles, 128x64x64 cells."""
+    dom = (1.2, 0.6, 0.6)
+    dim = (128, 64, 64)
+    cell_v = (dom[0] / dim[0]) * (dom[1] / dim[1]) * (dom[2] / dim[2])
+    n_inf, T_inf, mach = 1e20, 200.0, 7.0
+    a = math.sqrt(5.0 / 3.0 * KB * T_inf / ARGON["gas_mass"])
+    U = mach * a
+    fnum = n_inf * cell_v / 8.4
+    s = dict(grid_min=(0, 0, 0), grid_max=dom, grid_dim=dim, density=n_inf, fnum=fnum, temp=T_inf,
+             stream_vel=(U, 0.0, 0.0), dt=2e-6, rng="philox", ntc_local=1, sample_every=100,
+             init_kind="maxwell", wall_diffuse=1, wall_temp=500.0, capacity_factor=1.6, seed=20261203,
+             geom_nearest=1,
+             face_kind={"-x": "inflow", "+x": "outflow", "-y": "outflow", "+y": "outflow",
+                        "-z": "outflow", "+z": "outflow"}, **ARGON)
+    mesh = dict(kind="capsule", nose_radius=0.15, cone_deg=20.0, length=0.26,
+                nose_center=(0.35 + 0.15, 0.3, 0.3), ntarget=20000, seed=7, grid=(24, 32, 32))
+    return dict(name="capsule_mach7_argon_4M_128x64x64", settings=s, mesh=mesh,
+                desc=f"argon VHS w=0.81, Mach {mach:.0f} (U={U:.0f} m/s), T=200 K, n=1e20, "
+                     "diffuse capsule wall 500 K (nose r=0.15 m, 20 deg cone, ~20k tris), "
+                     "inflow -x, outflow elsewhere, 1.2x0.6x0.6 m, 128x64x64 cells, ~4.2M particles")
+
+
+def wl_sphere_500k():
+    dom = (1.2, 0.6, 0.6)
+    dim = (64, 32, 32)
+    cell_v = (dom[0] / dim[0]) * (dom[1] / dim[1]) * (dom[2] / dim[2])
+    fnum = 1e20 * cell_v / 7.63
+    s = dict(grid_min=(0, 0, 0), grid_max=dom, grid_dim=dim, density=1e20, fnum=fnum, temp=200.0,
+             stream_vel=(1500.0, 0.0, 0.0), dt=4e-6, rng="philox", ntc_local=1, sample_every=100,
+             init_kind="maxwell", wall_diffuse=1, wall_temp=300.0, capacity_factor=1.6, seed=20261203,
+             geom_nearest=1,
+             face_kind={"-x": "inflow", "+x": "outflow", "-y": "outflow", "+y": "outflow",
+                        "-z": "outflow", "+z": "outflow"}, **ARGON)
+    mesh = dict(kind="icosphere", level=3, radius=0.1, center=(0.4, 0.3, 0.3), grid=(16, 16, 16))
+    return dict(name="sphere_argon_500k_64x32x32", settings=s, mesh=mesh,
+                desc="argon VHS, U=1500 m/s, T=200 K, diffuse icosphere(3) r=0.1 m at 300 K, "
+                     "inflow -x, 64x32x32 cells, ~500k particles")
+
+
+def wl_box_100k():
+    s = dict(grid_min=(0, 0, 0), grid_max=(1, 1, 1), grid_dim=(16, 16, 16), density=1e20, fnum=1e15,
+             temp=400.0, init_temp2=600.0, dt=1e-5, rng="philox", periodic="n", sample_every=100,
+             init_kind="bimodal", seed=20261203, **ARGON)
+    s["temp"] = 200.0
+    return dict(name="box_argon_bimodal_100k_16cube", settings=s, mesh=None,
+                desc="argon VHS in a closed 1 m specular box, 16^3 cells, 98,304 particles, "
+                     "equal mix of 200 K and 600 K Maxwellians")
+
+
+WORKLOADS = {"capsule4m": wl_capsule_4m, "sphere500k": wl_sphere_500k, "box100k": wl_box_100k}
+DEFAULT_WORKLOAD = "capsule4m"
+
+
+def build_solver(wl, seed_offset=0):
+    import cudadsmc_b200 as cb
+    st = dict(wl["settings"])
+    st["seed"] = st.get("seed", 1) + seed_offset
+    s = cb.settings_t().set(**st)
+    sol = cb.DSMCSolver().Init(s)
+    m = wl["mesh"]
+    if m is not None:
+        if m["kind"] == "capsule":
+            v, t = cb.mesh_capsule(m["nose_radius"], m["cone_deg"], m["length"], m["nose_center"],
+                                   m["ntarget"], m["seed"])
+        else:
+            v, t = cb.mesh_icosphere(m["level"], m["radius"], m["center"])
+        sol.SetModel(v, t, m["grid"])
+    return sol
+
+
+# ------------------------------------------------------------------ clocks ---
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                mhz.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[3 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ------------------------------------------------------------- CPU oracle ---
+
+def cpu_oracle_sample(wl, budget_s=12.0, max_threads=None):
+    """The oracle's reference step (OpenMP) on a bounded sample of the
+    workload: an x-slab of its cells with its free-stream fill (closed slab
+    walls, the mesh specular, HybridTaus, the workload's VHS exponent).
+    Returns (particle-timesteps/s, threads, description)."""
+    from oracle import oracle as O
+    if max_threads:
+        O.set_threads(max_threads)
+    s = wl["settings"]
+    dim = list(s["grid_dim"])
+    gmin, gmax = np.asarray(s["grid_min"], np.float64), np.asarray(s["grid_max"], np.float64)
+    cell = (gmax - gmin) / np.asarray(dim)
+    nx = max(1, min(dim[0], 16))
+    x0 = dim[0] // 3
+    sub_min = gmin.copy()
+    sub_max = gmax.copy()
+    sub_min[0] = gmin[0] + x0 * cell[0]
+    sub_max[0] = sub_min[0] + nx * cell[0]
+    sub_dim = (nx, dim[1], dim[2])
+    import math as _m
+    w = s.get("gas_omega", 0.5)
+    gref = 0.0
+    if abs(w - 0.5) > 1e-9:
+        gref = _m.sqrt(2 * KB * s["gas_tref"] / (0.5 * s["gas_mass"])) * _m.gamma(2.5 - w) ** (-1 / (2 * w - 1))
+    sim = O.sim_from(sub_min, sub_max, sub_dim, s["fnum"], O.cross_section_of(s["gas_diam"]), "n", w, gref)
+    ppc = int(np.float32(s["density"]) * np.float32(sim.cell_volume) / np.float32(s["fnum"]))
+    rng = np.random.default_rng(1)
+    n = ppc * sim.cells
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(sub_min, sub_max, (n, 3))
+    vstd = math.sqrt(KB * s["temp"] / s["gas_mass"])
+    vel[:, :3] = rng.normal(0, vstd, (n, 3)) + np.asarray(s.get("stream_vel", (0, 0, 0)))
+    geom = None
+    m = wl["mesh"]
+    if m is not None:
+        import cudadsmc_b200 as cb
+        if m["kind"] == "capsule":
+            v, t = cb.mesh_capsule(m["nose_radius"], m["cone_deg"], m["length"], m["nose_center"],
+                                   m["ntarget"], m["seed"])
+        else:
+            v, t = cb.mesh_icosphere(m["level"], m["radius"], m["center"])
+        bbox, gc, count, ids, flags = O.build_grid(v, t, m["grid"])
+        nrm = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
+        nrm = (nrm / np.linalg.norm(nrm, axis=1, keepdims=True)).astype(np.float32)
+        geom = O.geom_from(bbox, gc, m["grid"], count, ids, flags, v, t, nrm)
+    seeds = ((rng.integers(0, 2**32, (sim.cells, 4), dtype=np.uint64) % (2**32 - 129)) + 128).astype(np.uint32)
+    mr = np.zeros((sim.cells, 2), np.float32)
+    mr[:, 0] = O.max_rel_vel_of(s["gas_diam"], s["temp"])
+    mr[:, 1] = rng.uniform(0, 1, sim.cells)
+    st4 = np.zeros((sim.cells, 4), np.float32)
+    dt = s["dt"]
+    steps, t_total = 0, 0.0
+    while t_total < budget_s and steps < 50:
+        t0 = time.perf_counter()
+        pos, vel, _ = O.step(sim, geom, pos, vel, dt, float(ppc), mr, st4, seeds)
+        t_total += time.perf_counter() - t0
+        steps += 1
+    desc = (f"oracle reference step on an x-slab of the workload ({sub_dim[0]}x{sub_dim[1]}x{sub_dim[2]} cells, "
+            f"{n} particles, {steps} steps, {O.threads()} threads)")
+    return n * steps / t_total, O.threads(), desc, n, steps, t_total
+
+
+# ---------------------------------------------------------------- our arm ---
+
+def algorithmic_bytes(kernel, n_particles, cells, rng_taus, sample_frac):
+    """Bytes a kernel must move per launch (SoA FP32 state, 24 B/particle)."""
+    if kernel == "scatter":
+        return n_particles * (8 + 24 + 24 + 4)
+    if kernel == "cell":
+        per_cell = 4 + 16 + (32 if rng_taus else 0) + sample_frac * 80
+        return n_particles * (24 + 4 + 24 + 8) + cells * per_cell
+    if kernel == "scan":
+        return cells * 12
+    return 0
+
+
+def run_ours(args, rank, world):
+    import torch
+    import cudadsmc_b200 as cb
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    wl = WORKLOADS[args.workload]()
+    sol = build_solver(wl, seed_offset=rank)
+    sol.SetStream(torch.cuda.current_stream().cuda_stream)
+    n0 = sol.InitSystemState()
+    dt = wl["settings"]["dt"]
+    # warm-up (also develops the flow a little)
+    sol.RunSimulationStep(dt, args.warmup)
+    sol.Sync()
+    info0 = sol.Info()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0) if world == 1 else dev.index
+    with ClockSampler(gpu_index) as clk:
+        sol.Profile(True)
+        ev0.record()
+        sol.RunSimulationStep(dt, args.steps)
+        ev1.record()
+        torch.cuda.synchronize()
+        prof = sol.ProfileRead()
+    ms = ev0.elapsed_time(ev1)
+    sol.Sync()
+    info1 = sol.Info()
+    pst = int(info1.particle_steps - info0.particle_steps)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    c = torch.tensor([float(pst)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
+    ms_max = float(t.item())
+    total_ps = float(c.item())
+    value = total_ps / (ms_max * 1e-3)
+    launches = sum(v[1] for v in prof.values())
+    n_avg = pst / args.steps
+    # dominant kernel and its roofline
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dom = max(("scatter", "cell"), key=lambda k: prof[k][0])
+    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+    taus = wl["settings"].get("rng", "taus") == "taus"
+    alg = algorithmic_bytes(dom, n_avg, sol.Info().cells, taus, 1.0 / 100)
+    achieved = alg / (dom_ms * 1e-3) / 1e9
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            tr = json.load(open(tr_path)).get(args.workload, {}).get(dom)
+            if tr:
+                traffic = tr["bytes_per_particle"] * n_avg
+        except (OSError, ValueError, KeyError):
+            traffic = None
+    kernels = {k: {"ms_per_launch": (v[0] / v[1] if v[1] else None), "launches": v[1],
+                   "share": v[0] / max(sum(x[0] for x in prof.values()), 1e-12)} for k, v in prof.items()}
+    # whole-step roofline at 128 B per particle-timestep (algorithmic)
+    step_frac = value / max(world, 1) * 128 / (peak * 1e9)
+    # end-to-end through the C ABI with host buffers
+    e2e = run_e2e(args, wl, rank, world, dev)
+    out = {
+        "metric": "particle-timesteps/s", "value": value, "unit": "particle-timesteps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded free-stream fill, generated mesh)",
+        "config": {"workload": wl["name"], "description": wl["desc"], "particles_initial": n0,
+                   "particles_avg_timed": n_avg, "cells": sol.Info().cells, "dt": dt,
+                   "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
+                   "l2_policy": "working set (2 x 24 B x N state + 12 B x N keys) > 126 MB L2",
+                   "rng": wl["settings"].get("rng")},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg, "ms_per_launch": dom_ms,
+                     "step_frac_128B": step_frac},
+        "kernels": kernels,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "e2e": e2e,
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        v, cores, desc, *_ = cpu_oracle_sample(wl, budget_s=args.cpu_budget)
+        out["cpu_baseline"] = {"value": v, "unit": "particle-timesteps/s", "cores": cores, "kind": "port",
+                               "sample": desc}
+    sol.close()
+    return out
+
+
+def run_e2e(args, wl, rank, world, dev):
+    """The same metric through the C ABI with host buffers: per run the
+    pinned initial state is uploaded (h2d), then every step is one dsmc_step
+    call followed by a device->host read of that step's collision totals, and
+    the sampled fields are read back at the end (d2h)."""
+    import torch
+    sol = build_solver(wl, seed_offset=rank)
+    n0 = sol.InitSystemState()
+    state = sol.DownloadState()  # the initial state, as a host would provide it
+    host = torch.from_numpy(state).pin_memory()
+    dt = wl["settings"]["dt"]
+    k = max(3, min(args.steps, args.e2e_steps))
+    sol.UploadState(host.numpy(), soa=True)  # warm the path once
+    sol.RunSimulationStep(dt, 3)
+    sol.Sync()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sol.UploadState(host.numpy(), soa=True)
+    i0 = sol.Info().particle_steps
+    for _ in range(k):
+        sol.RunSimulationStep(dt, 1)
+        sol.Totals()
+    fields = sol.Fields()
+    t1 = time.perf_counter()
+    pst = sol.Info().particle_steps - i0
+    el = torch.tensor([t1 - t0], dtype=torch.float64, device=dev)
+    c = torch.tensor([float(pst)], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(el, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
+    sol.close()
+    return {"value": float(c.item()) / float(el.item()), "unit": "particle-timesteps/s",
+            "h2d_bytes_per_step": int(state.nbytes / k),
+            "d2h_bytes_per_step": int(24 + fields.nbytes / k), "steps": k,
+            "note": "upload of the initial pinned state + one C-ABI dsmc_step and a totals read per step "
+                    "+ the sampled fields at the end"}
+
+
+# ---------------------------------------------------------- reference arm ---
+
+def run_reference(args):
+    wl = WORKLOADS[args.workload]()
+    budget = max(10.0, min(120.0, 4.0 * (args.steps + args.warmup)))
+    from oracle import oracle as O
+    O.set_threads(os.cpu_count() or 1)
+    v, cores, desc, n, steps, tt = cpu_oracle_sample(wl, budget_s=budget)
+    out = {"metric": "particle-timesteps/s", "value": v, "unit": "particle-timesteps/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt / steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "impl": "reference",
+           "config": {"workload": wl["name"], "description": wl["desc"]},
+           "cpu_baseline": {"value": v, "unit": "particle-timesteps/s", "cores": cores, "kind": "port",
+                            "sample": desc},
+           "e2e": {"value": v, "unit": "particle-timesteps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    if world > 1:
+        import torch
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    out = run_ours(args, rank, world)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

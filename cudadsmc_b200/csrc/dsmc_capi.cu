@@ -1,0 +1,1211 @@
+// C ABI of the B200 DSMC timestep (declared in include/dsmc_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "dsmc_b200.h"
+#include "dsmc_host.hpp"
+#include "dsmc_kernels.cuh"
+
+using dsmcb::GridGeom;
+using dsmcb::Meta;
+using dsmcb::SoA;
+
+struct dsmc_handle {
+  dsmc_config cfg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+
+  uint32_t ppc = 0, cells = 0, capacity = 0, n_scan_tiles = 0, n_tiles = 0, cells_per_tile = 0;
+  float cell_size[3]{}, cell_volume = 0.f, cross_section = 0.f, max_rel_vel = 0.f;
+  float vhs_gref = 0.f;
+  GridGeom grid{};
+
+  float* A[6]{};
+  float* B[6]{};
+  uint32_t* orig = nullptr;
+  uint2* kt = nullptr;
+  uint32_t* count = nullptr;
+  uint32_t* start = nullptr;
+  uint32_t* tile_sum = nullptr;
+  float2* maxrem = nullptr;
+  uint4* seeds = nullptr;
+  double* acc = nullptr;
+  Meta* meta = nullptr;
+  float* inj_rem = nullptr;
+  uint32_t* inj_plan = nullptr;
+
+  bool has_geom = false;
+  dsmcb::GeomGrid ggrid;
+  uint32_t* gflags = nullptr;
+  uint2* gse = nullptr;
+  float4* gtri = nullptr;
+
+  bool has_state = false;
+  uint64_t step = 0;
+  double sim_time = 0.0;
+
+  std::vector<dsmcb::Inflow> inflows;
+
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  float graph_dt = -1.f;
+
+  // per-kernel event timing (dsmc_profile)
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev;      // pairs
+  std::vector<int> ev_kernel;       // kernel id of each pair
+  size_t ev_used = 0;
+  double prof_ms[4] = {0, 0, 0, 0};
+  uint32_t prof_n[4] = {0, 0, 0, 0};
+
+  std::string err;
+};
+
+namespace {
+
+std::string g_create_error;
+
+int fail(dsmc_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(dsmc_handle* h, cudaError_t e, const char* where) {
+  return fail(h, e == cudaErrorMemoryAllocation ? DSMC_ERR_OOM : DSMC_ERR_CUDA,
+              std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(h, call, where)                              \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
+  } while (0)
+
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <class T>
+cudaError_t dalloc(T** p, size_t n) {
+  return cudaMalloc((void**)p, n * sizeof(T) + 16);
+}
+
+void free_all(dsmc_handle* h) {
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  h->ev.clear();
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->graph_exec = nullptr;
+  h->graph = nullptr;
+  for (int i = 0; i < 6; i++) {
+    cudaFree(h->A[i]);
+    cudaFree(h->B[i]);
+    h->A[i] = h->B[i] = nullptr;
+  }
+  void* ps[] = {h->orig, h->kt, h->count, h->start, h->tile_sum, h->maxrem, h->seeds, h->acc,
+                h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gse, h->gtri};
+  for (void* p : ps) cudaFree(p);
+}
+
+SoA soa_of(float* const a[6]) { return SoA{a[0], a[1], a[2], a[3], a[4], a[5]}; }
+
+// VHS reference speed for sigma(g) = sigma_ref (g_ref / g)^(2 omega - 1):
+// g_ref = sqrt(2 k T_ref / m_r) * Gamma(5/2 - omega)^(-1/(2 omega - 1)), m_r = m/2.
+float vhs_gref_of(const dsmc_config& c) {
+  double w = c.gas_omega;
+  if (std::fabs(w - 0.5) < 1e-9) return 0.f;
+  double mr = 0.5 * c.gas_mass;
+  double g0 = std::sqrt(2.0 * 1.380649e-23 * c.gas_tref / mr);
+  return (float)(g0 * std::pow(std::tgamma(2.5 - w), -1.0 / (2.0 * w - 1.0)));
+}
+
+dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
+  dsmcb::StepParams p{};
+  p.grid = h->grid;
+  p.cells = h->cells;
+  p.cell_volume = h->cell_volume;
+  p.cross_section = h->cross_section;
+  p.fnum = h->cfg.fnum;
+  p.avg_conc = (float)h->ppc;
+  p.dt = dt;
+  p.periodic = h->cfg.periodic;
+  p.hard_sphere = std::fabs(h->cfg.gas_omega - 0.5f) < 1e-9f;
+  p.vhs_exp = 2.f * h->cfg.gas_omega - 1.f;
+  p.vhs_gref = h->vhs_gref;
+  p.ntc_local = h->cfg.ntc_local;
+  p.rng_kind = h->cfg.rng;
+  p.seed = make_uint2((uint32_t)h->cfg.seed, (uint32_t)(h->cfg.seed >> 32));
+  p.face_mode = h->cfg.face_mode;
+  for (int i = 0; i < 6; i++) {
+    p.face_kind[i] = h->cfg.face_kind[i];
+    p.face_vstd[i] = std::sqrt(1.3806e-23f * h->cfg.face_temp[i] / h->cfg.gas_mass);
+  }
+  p.has_geom = h->has_geom && h->cfg.geometry;
+  if (p.has_geom) {
+    const auto& g = h->ggrid;
+    p.geom.grid.gmin = make_float3(g.bbox[0], g.bbox[1], g.bbox[2]);
+    p.geom.grid.gmax = make_float3(g.bbox[3], g.bbox[4], g.bbox[5]);
+    p.geom.grid.cell = make_float3(g.cell[0], g.cell[1], g.cell[2]);
+    p.geom.grid.dim = make_uint3(g.dim[0], g.dim[1], g.dim[2]);
+    p.geom.flags = h->gflags;
+    p.geom.start_end = h->gse;
+    p.geom.tri = h->gtri;
+    p.geom.diffuse = h->cfg.wall_diffuse;
+    p.geom.nearest = h->cfg.geom_nearest;
+    p.geom.wall_vstd = std::sqrt(1.3806e-23f * h->cfg.wall_temp / h->cfg.gas_mass);
+  }
+  p.start = h->start;
+  p.count = h->count;
+  p.tile_sum = h->tile_sum;
+  p.n_scan_tiles = h->n_scan_tiles;
+  p.maxrem = h->maxrem;
+  p.seeds = h->seeds;
+  p.stat4 = nullptr;
+  p.acc = h->acc;
+  p.meta = h->meta;
+  p.sample_every = h->cfg.sample_every;
+  p.cells_per_tile = (int)h->cells_per_tile;
+  p.n_tiles = h->n_tiles;
+  p.step_override = 0;
+  return p;
+}
+
+constexpr size_t kProfPairs = 4096;
+
+void prof_flush(dsmc_handle* h) {
+  if (!h->ev_used) return;
+  cudaEventSynchronize(h->ev[2 * (h->ev_used - 1) + 1]);
+  for (size_t i = 0; i < h->ev_used; i++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->ev[2 * i], h->ev[2 * i + 1]) == cudaSuccess) {
+      h->prof_ms[h->ev_kernel[i]] += ms;
+      h->prof_n[h->ev_kernel[i]] += 1;
+    }
+  }
+  h->ev_used = 0;
+}
+
+// Launches `launch` with CUDA events around it when the handle is profiling.
+template <class F>
+cudaError_t timed(dsmc_handle* h, int kernel, F launch) {
+  if (!h->profiling) return launch();
+  if (h->ev_used == kProfPairs) prof_flush(h);
+  size_t i = h->ev_used++;
+  h->ev_kernel[i] = kernel;
+  cudaEventRecord(h->ev[2 * i], h->stream);
+  cudaError_t e = launch();
+  cudaEventRecord(h->ev[2 * i + 1], h->stream);
+  return e;
+}
+
+// One timestep: scan -> scatter -> cell (-> inflow injection).
+cudaError_t enqueue_step(dsmc_handle* h, float dt) {
+  cudaError_t e;
+  e = timed(h, 0, [&] {
+    return dsmcb::launch_scan(h->count, h->start, h->cells, h->tile_sum, h->n_scan_tiles, h->meta,
+                              1, h->stream);
+  });
+  if (e) return e;
+  e = timed(h, 1, [&] {
+    return dsmcb::launch_scatter(soa_of(h->A), soa_of(h->B), h->kt, h->start, h->orig, h->cells,
+                                 h->tile_sum, h->n_scan_tiles, h->meta, h->capacity, h->stream);
+  });
+  if (e) return e;
+  dsmcb::StepParams p = base_params(h, dt);
+  p.in = soa_of(h->B);
+  p.in_orig = h->orig;
+  p.out = soa_of(h->A);
+  p.out_kt = h->kt;
+  p.flags = dsmcb::kDoFixup | dsmcb::kDoCollide | dsmcb::kDoMove | dsmcb::kDoKeys;
+  if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
+  e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
+  if (e) return e;
+  for (const auto& in : h->inflows) {
+    dsmcb::InjectParams ip{};
+    ip.grid = h->grid;
+    ip.cells = h->cells;
+    ip.inflow = in;
+    ip.dt = dt;
+    ip.seed = p.seed;
+    ip.capacity = h->capacity;
+    ip.remainder = h->inj_rem + in.face;
+    ip.st = soa_of(h->A);
+    ip.kt = h->kt;
+    ip.count = h->count;
+    ip.tile_sum = h->tile_sum;
+    ip.plan = h->inj_plan + 2 * in.face;
+    ip.meta = h->meta;
+    e = timed(h, 3, [&] { return dsmcb::launch_inject(ip, h->stream); });
+    if (e) return e;
+  }
+  return cudaSuccess;
+}
+
+// Inflow fluxes of the faces marked DSMC_FACE_INFLOW: number flux of a
+// drifting Maxwellian through a face, n c_mp / (2 sqrt(pi)) [exp(-s^2) +
+// sqrt(pi) s (1 + erf(s))], s = U.n_in / c_mp, in simulator particles.
+void setup_inflows(dsmc_handle* h) {
+  h->inflows.clear();
+  if (!h->cfg.face_mode) return;
+  const dsmc_config& c = h->cfg;
+  double vstd = std::sqrt(1.3806e-23 * c.temp / c.gas_mass);
+  double cmp = std::sqrt(2.0) * vstd;
+  for (int f = 0; f < 6; f++) {
+    if (c.face_kind[f] != DSMC_FACE_INFLOW) continue;
+    int ax = f >> 1;
+    double sign = (f & 1) ? -1.0 : 1.0;
+    double un = sign * c.stream_vel[ax];
+    double s = un / cmp;
+    double flux = c.density * cmp / (2.0 * std::sqrt(M_PI)) *
+                  (std::exp(-s * s) + std::sqrt(M_PI) * s * (1.0 + std::erf(s)));
+    int a1 = (ax + 1) % 3, a2 = (ax + 2) % 3;
+    double area = (double)(c.grid_max[a1] - c.grid_min[a1]) * (c.grid_max[a2] - c.grid_min[a2]);
+    dsmcb::Inflow in{};
+    in.face = f;
+    in.number_flux = (float)(flux / c.fnum);
+    in.stream = make_float3(c.stream_vel[0], c.stream_vel[1], c.stream_vel[2]);
+    in.vstd = (float)vstd;
+    in.area = (float)area;
+    h->inflows.push_back(in);
+  }
+}
+
+int check_device_flags(dsmc_handle* h) {
+  uint32_t err = 0;
+  CK(h, cudaMemcpy(&err, &h->meta->error, 4, cudaMemcpyDeviceToHost), "read error flags");
+  if (err) {
+    std::string m = "device error flags:";
+    if (err & dsmcb::kErrCapacity) m += " particle capacity exceeded (raise capacity_factor);";
+    if (err & dsmcb::kErrKeyRange) m += " cell key out of range;";
+    return fail(h, DSMC_ERR_DEVICE, m);
+  }
+  return DSMC_OK;
+}
+
+int reindex(dsmc_handle* h, uint32_t n) {
+  CK(h, cudaMemsetAsync(h->count, 0, (h->cells + 1) * sizeof(uint32_t), h->stream), "memset");
+  CK(h, cudaMemsetAsync(h->tile_sum, 0, h->n_scan_tiles * sizeof(uint32_t), h->stream), "memset");
+  CK(h, dsmcb::launch_index(h->grid, h->cells, h->A[0], h->A[1], h->A[2], n, h->kt, h->count,
+                            h->tile_sum, h->n_scan_tiles, h->cfg.face_mode, h->stream),
+     "index kernel");
+  uint32_t m2[2] = {n, 0u};
+  CK(h, cudaMemcpyAsync(h->meta, m2, sizeof(m2), cudaMemcpyHostToDevice, h->stream), "meta");
+  CK(h, cudaStreamSynchronize(h->stream), "index sync");
+  h->has_state = true;
+  return DSMC_OK;
+}
+
+int read_meta(dsmc_handle* h, Meta& m) {
+  CK(h, cudaStreamSynchronize(h->stream), "sync");
+  CK(h, cudaMemcpy(&m, h->meta, sizeof(Meta), cudaMemcpyDeviceToHost), "read meta");
+  return DSMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dsmc_status_string(int s) {
+  switch (s) {
+    case DSMC_OK: return "ok";
+    case DSMC_ERR_ARG: return "invalid argument";
+    case DSMC_ERR_CONFIG: return "configuration error";
+    case DSMC_ERR_CUDA: return "CUDA error";
+    case DSMC_ERR_OOM: return "out of device memory";
+    case DSMC_ERR_STATE: return "call out of order";
+    case DSMC_ERR_CAPACITY: return "particle capacity exceeded";
+    case DSMC_ERR_IO: return "I/O error";
+    case DSMC_ERR_DEVICE: return "device error flag";
+  }
+  return "unknown status";
+}
+
+const char* dsmc_last_error(const dsmc_handle* h) {
+  if (!h) return g_create_error.empty() ? dsmcb::g_config_error.c_str() : g_create_error.c_str();
+  return h->err.c_str();
+}
+
+int dsmc_config_default(dsmc_config* cfg) {
+  if (!cfg) return DSMC_ERR_ARG;
+  return dsmcb::config_default(cfg);
+}
+
+int dsmc_config_read_xml(const char* path, dsmc_config* cfg) {
+  if (!path || !cfg) return DSMC_ERR_ARG;
+  g_create_error.clear();
+  return dsmcb::config_read_xml(path, cfg);
+}
+
+int dsmc_config_from_args(int argc, const char* const* argv, dsmc_config* cfg, float* run_for) {
+  if (!cfg || (argc > 0 && !argv)) return DSMC_ERR_ARG;
+  g_create_error.clear();
+  return dsmcb::config_from_args(argc, argv, cfg, run_for);
+}
+
+int dsmc_create(const dsmc_config* cfg, dsmc_handle** out) {
+  if (!cfg || !out) return fail(nullptr, DSMC_ERR_ARG, "null argument");
+  *out = nullptr;
+  const dsmc_config& c = *cfg;
+  for (int k = 0; k < 3; k++) {
+    if (c.grid_dim[k] <= 0 || !(c.grid_max[k] > c.grid_min[k]))
+      return fail(nullptr, DSMC_ERR_CONFIG, "grid dims must be > 0 and max > min");
+  }
+  if (!(c.fnum > 0) || !(c.density > 0) || !(c.gas_mass > 0) || !(c.gas_diam > 0))
+    return fail(nullptr, DSMC_ERR_CONFIG, "density, fnum, gas mass and diameter must be > 0");
+  if (c.gas_omega < 0.5f || c.gas_omega > 1.0f)
+    return fail(nullptr, DSMC_ERR_CONFIG, "VHS omega must lie in [0.5, 1]");
+  if (c.rng != DSMC_RNG_TAUS && c.rng != DSMC_RNG_PHILOX)
+    return fail(nullptr, DSMC_ERR_CONFIG, "unknown rng");
+  uint64_t cells64 = (uint64_t)c.grid_dim[0] * c.grid_dim[1] * c.grid_dim[2];
+  if (cells64 > (uint64_t)dsmcb::kMaxScanTiles * dsmcb::kScanTile)
+    return fail(nullptr, DSMC_ERR_CONFIG, "too many cells (max 4194304)");
+
+  dsmc_handle* h = new dsmc_handle();
+  h->cfg = c;
+  cudaGetDevice(&h->device);
+  h->cells = (uint32_t)cells64;
+  // settings_t / main (src/sim_settings.cpp:100-103, kernels/dsmc.cu:324-330)
+  for (int k = 0; k < 3; k++)
+    h->cell_size[k] = (c.grid_max[k] - c.grid_min[k]) / (float)(uint32_t)c.grid_dim[k];
+  h->cell_volume = h->cell_size[0] * h->cell_size[1] * h->cell_size[2];
+  h->ppc = c.part_per_cell ? c.part_per_cell : (uint32_t)(c.density * h->cell_volume / c.fnum);
+  // InitSimulationProperties (kernels/dsmc_kernel.cu:323-331)
+  const float pi_f = 3.14159265358979f;
+  h->cross_section = (float)(double)(pi_f * c.gas_diam * c.gas_diam);
+  h->max_rel_vel = (float)(double)(c.gas_diam * c.gas_diam * pi_f * sqrtf((float)(c.temp / 300.0)) * 300);
+  h->vhs_gref = vhs_gref_of(c);
+  h->grid.gmin = make_float3(c.grid_min[0], c.grid_min[1], c.grid_min[2]);
+  h->grid.gmax = make_float3(c.grid_max[0], c.grid_max[1], c.grid_max[2]);
+  h->grid.cell = make_float3(h->cell_size[0], h->cell_size[1], h->cell_size[2]);
+  h->grid.dim = make_uint3(c.grid_dim[0], c.grid_dim[1], c.grid_dim[2]);
+  h->n_scan_tiles = (h->cells + dsmcb::kScanTile - 1) / dsmcb::kScanTile;
+  uint32_t target = 2048;
+  uint32_t ct = 256;
+  while (ct > 32 && (uint64_t)ct * std::max<uint32_t>(h->ppc, 1) > target) ct >>= 1;
+  h->cells_per_tile = ct;
+  h->n_tiles = (h->cells + ct - 1) / ct;
+  float capf = c.capacity_factor < 1.f ? 1.f : c.capacity_factor;
+  uint64_t cap = (uint64_t)std::ceil((double)h->ppc * h->cells * capf) + 1024;
+  if (cap > 0xF0000000ull) {
+    delete h;
+    return fail(nullptr, DSMC_ERR_CONFIG, "particle capacity exceeds 32-bit indexing");
+  }
+  h->capacity = (uint32_t)cap;
+  setup_inflows(h);
+
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 6 && !e; i++) {
+    e = dalloc(&h->A[i], h->capacity);
+    if (!e) e = dalloc(&h->B[i], h->capacity);
+  }
+  if (!e) e = dalloc(&h->orig, h->capacity);
+  if (!e) e = dalloc(&h->kt, h->capacity);
+  if (!e) e = dalloc(&h->count, h->cells + 1);
+  if (!e) e = dalloc(&h->start, h->cells + 1);
+  if (!e) e = dalloc(&h->tile_sum, h->n_scan_tiles);
+  if (!e) e = dalloc(&h->maxrem, h->cells);
+  if (!e) e = dalloc(&h->seeds, h->cells);
+  if (!e) e = dalloc(&h->acc, 5 * (size_t)h->cells);
+  if (!e) e = dalloc(&h->meta, 1);
+  if (!e) e = dalloc(&h->inj_rem, 6);
+  if (!e) e = dalloc(&h->inj_plan, 12);
+  if (e) {
+    std::string m = std::string("allocation: ") + cudaGetErrorString(e);
+    free_all(h);
+    delete h;
+    return fail(nullptr, e == cudaErrorMemoryAllocation ? DSMC_ERR_OOM : DSMC_ERR_CUDA, m);
+  }
+  cudaMemset(h->count, 0, (h->cells + 1) * sizeof(uint32_t));
+  cudaMemset(h->start, 0, (h->cells + 1) * sizeof(uint32_t));
+  cudaMemset(h->tile_sum, 0, h->n_scan_tiles * sizeof(uint32_t));
+  cudaMemset(h->acc, 0, 5 * (size_t)h->cells * sizeof(double));
+  cudaMemset(h->meta, 0, sizeof(Meta));
+  cudaMemset(h->inj_rem, 0, 6 * sizeof(float));
+  // per-cell (sigma*g)max and remainder (InitMaximums, kernels/dsmc_kernel.cu:1104-1120)
+  // and HybridTaus seeds (CreateRandomSeedsUint4, :1846-1886), from the seed
+  std::vector<float2> mr(h->cells);
+  std::vector<uint4> sd(h->cells);
+  uint64_t s = c.seed ^ 0x5eed5eed12345678ull;
+  for (uint32_t i = 0; i < h->cells; i++) {
+    mr[i].x = h->max_rel_vel;
+    mr[i].y = (float)((splitmix64(s) >> 40) * (1.0 / 16777216.0));
+    uint32_t v[4];
+    for (int k = 0; k < 4; k++) v[k] = (uint32_t)(splitmix64(s) % (4294967296ull - 129)) + 128;
+    sd[i] = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+  cudaMemcpy(h->maxrem, mr.data(), h->cells * sizeof(float2), cudaMemcpyHostToDevice);
+  cudaMemcpy(h->seeds, sd.data(), h->cells * sizeof(uint4), cudaMemcpyHostToDevice);
+  e = cudaDeviceSynchronize();
+  if (e) {
+    std::string m = std::string("init: ") + cudaGetErrorString(e);
+    free_all(h);
+    delete h;
+    return fail(nullptr, DSMC_ERR_CUDA, m);
+  }
+  *out = h;
+  return DSMC_OK;
+}
+
+int dsmc_destroy(dsmc_handle* h) {
+  if (!h) return DSMC_ERR_ARG;
+  cudaStreamSynchronize(h->stream);
+  free_all(h);
+  delete h;
+  return DSMC_OK;
+}
+
+int dsmc_set_stream(dsmc_handle* h, void* stream) {
+  if (!h) return DSMC_ERR_ARG;
+  h->stream = (cudaStream_t)stream;
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->graph_exec = nullptr;
+  h->graph = nullptr;
+  h->graph_dt = -1.f;
+  return DSMC_OK;
+}
+
+int dsmc_sync(dsmc_handle* h) {
+  if (!h) return DSMC_ERR_ARG;
+  CK(h, cudaStreamSynchronize(h->stream), "stream sync");
+  return check_device_flags(h);
+}
+
+int dsmc_get_info(dsmc_handle* h, dsmc_info* info) {
+  if (!h || !info) return DSMC_ERR_ARG;
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  info->part_per_cell = h->ppc;
+  info->cells = h->cells;
+  info->capacity = h->capacity;
+  info->num_particles = h->has_state ? m.n_alive + m.n_pending : 0;
+  for (int k = 0; k < 3; k++) info->cell_size[k] = h->cell_size[k];
+  info->cell_volume = h->cell_volume;
+  info->cross_section = h->cross_section;
+  info->max_rel_vel = h->max_rel_vel;
+  info->step = h->step;
+  info->samples = m.samples;
+  info->sim_time = h->sim_time;
+  info->particle_steps = m.particle_steps;
+  info->injected = m.injected;
+  info->removed = m.removed;
+  info->giant_cells = m.giant_cells;
+  return DSMC_OK;
+}
+
+int dsmc_profile(dsmc_handle* h, int enable) {
+  if (!h) return DSMC_ERR_ARG;
+  if (enable) {
+    if (h->ev.empty()) {
+      h->ev.resize(2 * kProfPairs);
+      h->ev_kernel.resize(kProfPairs);
+      for (auto& e : h->ev) CK(h, cudaEventCreate(&e), "event create");
+    }
+    h->ev_used = 0;
+    for (int k = 0; k < 4; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+  } else {
+    prof_flush(h);
+  }
+  h->profiling = enable != 0;
+  return DSMC_OK;
+}
+
+int dsmc_profile_read(dsmc_handle* h, double ms[4], uint32_t launches[4]) {
+  if (!h || !ms || !launches) return DSMC_ERR_ARG;
+  prof_flush(h);
+  for (int k = 0; k < 4; k++) { ms[k] = h->prof_ms[k]; launches[k] = h->prof_n[k]; }
+  h->profiling = false;
+  return DSMC_OK;
+}
+
+int dsmc_build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tris,
+                             uint32_t ntris, const int grid_dim[3], float bbox[6], float cell[3],
+                             uint32_t* cell_count, uint32_t* tri_ids, uint64_t cap, uint8_t* flags,
+                             uint64_t* n_entries) {
+  if (!verts || !tris || !grid_dim || grid_dim[0] <= 0 || grid_dim[1] <= 0 || grid_dim[2] <= 0)
+    return DSMC_ERR_ARG;
+  for (uint32_t i = 0; i < 3 * ntris; i++)
+    if (tris[i] >= nverts) return DSMC_ERR_ARG;
+  dsmcb::GeomGrid g;
+  dsmcb::build_geometry_grid(verts, nverts, tris, ntris, grid_dim, g);
+  if (bbox) std::memcpy(bbox, g.bbox, sizeof(g.bbox));
+  if (cell) std::memcpy(cell, g.cell, sizeof(g.cell));
+  if (cell_count) std::memcpy(cell_count, g.count.data(), g.count.size() * 4);
+  if (flags) std::memcpy(flags, g.flags.data(), g.flags.size());
+  if (tri_ids) {
+    size_t n = std::min<size_t>(cap, g.tri_ids.size());
+    std::memcpy(tri_ids, g.tri_ids.data(), n * 4);
+  }
+  if (n_entries) *n_entries = g.tri_ids.size();
+  return DSMC_OK;
+}
+
+static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
+                           const uint32_t* tris, uint32_t ntris, const float* normals) {
+  const auto& g = h->ggrid;
+  std::vector<float> nrm;
+  if (!normals) {
+    std::vector<float> v(verts, verts + 3 * (size_t)nverts);
+    std::vector<uint32_t> t(tris, tris + 3 * (size_t)ntris);
+    dsmcb::face_normals(v, t, nrm);
+    normals = nrm.data();
+  }
+  const uint32_t gc = g.dim[0] * g.dim[1] * g.dim[2];
+  std::vector<uint32_t> flags(gc);
+  std::vector<uint2> se(gc);
+  std::vector<float4> tri(3 * g.tri_ids.size() + 3);
+  size_t off = 0;
+  for (uint32_t c = 0; c < gc; c++) {
+    flags[c] = g.flags[c];
+    if (g.count[c]) se[c] = make_uint2((uint32_t)off, (uint32_t)(off + g.count[c]));
+    else se[c] = make_uint2(0xffffffffu, 0xffffffffu);
+    for (uint32_t k = 0; k < g.count[c]; k++) {
+      uint32_t t = g.tri_ids[off + k];
+      const float* a = verts + 3 * (size_t)tris[3 * t];
+      const float* b = verts + 3 * (size_t)tris[3 * t + 1];
+      const float* cc = verts + 3 * (size_t)tris[3 * t + 2];
+      const float* n = normals + 3 * (size_t)t;
+      tri[3 * (off + k)] = make_float4(a[0], a[1], a[2], n[0]);
+      tri[3 * (off + k) + 1] = make_float4(b[0], b[1], b[2], n[1]);
+      tri[3 * (off + k) + 2] = make_float4(cc[0], cc[1], cc[2], n[2]);
+    }
+    off += g.count[c];
+  }
+  cudaFree(h->gflags);
+  cudaFree(h->gse);
+  cudaFree(h->gtri);
+  h->gflags = nullptr; h->gse = nullptr; h->gtri = nullptr;
+  CK(h, dalloc(&h->gflags, gc), "geometry alloc");
+  CK(h, dalloc(&h->gse, gc), "geometry alloc");
+  CK(h, dalloc(&h->gtri, tri.size()), "geometry alloc");
+  CK(h, cudaMemcpy(h->gflags, flags.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
+  CK(h, cudaMemcpy(h->gse, se.data(), gc * sizeof(uint2), cudaMemcpyHostToDevice), "geometry upload");
+  CK(h, cudaMemcpy(h->gtri, tri.data(), tri.size() * sizeof(float4), cudaMemcpyHostToDevice),
+     "geometry upload");
+  h->has_geom = true;
+  h->cfg.geometry = 1;
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->graph_exec = nullptr;
+  h->graph = nullptr;
+  h->graph_dt = -1.f;
+  return DSMC_OK;
+}
+
+int dsmc_set_mesh(dsmc_handle* h, const float* verts, uint32_t nverts, const uint32_t* tris,
+                  uint32_t ntris, const float* normals, const int grid_dim[3]) {
+  if (!h || !verts || !tris || !grid_dim || ntris == 0) return fail(h, DSMC_ERR_ARG, "bad mesh");
+  for (int k = 0; k < 3; k++)
+    if (grid_dim[k] <= 0) return fail(h, DSMC_ERR_ARG, "geometry grid dims must be > 0");
+  for (uint32_t i = 0; i < 3 * ntris; i++)
+    if (tris[i] >= nverts) return fail(h, DSMC_ERR_ARG, "triangle index out of range");
+  dsmcb::build_geometry_grid(verts, nverts, tris, ntris, grid_dim, h->ggrid);
+  return upload_geometry(h, verts, nverts, tris, ntris, normals);
+}
+
+int dsmc_set_geometry_grid(dsmc_handle* h, const float bbox[6], const float cell[3],
+                           const int dim[3], const uint32_t* cell_count, const uint32_t* tri_ids,
+                           const uint8_t* flags, const float* verts, uint32_t nverts,
+                           const uint32_t* tris, uint32_t ntris, const float* normals) {
+  if (!h || !bbox || !cell || !dim || !cell_count || !flags || !verts || !tris)
+    return fail(h, DSMC_ERR_ARG, "null argument");
+  for (int k = 0; k < 3; k++)
+    if (dim[k] <= 0) return fail(h, DSMC_ERR_ARG, "geometry grid dims must be > 0");
+  auto& g = h->ggrid;
+  std::memcpy(g.bbox, bbox, sizeof(g.bbox));
+  std::memcpy(g.cell, cell, sizeof(g.cell));
+  for (int k = 0; k < 3; k++) g.dim[k] = (uint32_t)dim[k];
+  uint32_t gc = g.dim[0] * g.dim[1] * g.dim[2];
+  g.count.assign(cell_count, cell_count + gc);
+  g.flags.assign(flags, flags + gc);
+  size_t total = 0;
+  for (uint32_t c = 0; c < gc; c++) total += g.count[c];
+  if (total && !tri_ids) return fail(h, DSMC_ERR_ARG, "tri_ids missing");
+  g.tri_ids.assign(tri_ids, tri_ids + total);
+  for (uint32_t t : g.tri_ids)
+    if (t >= ntris) return fail(h, DSMC_ERR_ARG, "triangle id out of range");
+  for (uint32_t i = 0; i < 3 * ntris; i++)
+    if (tris[i] >= nverts) return fail(h, DSMC_ERR_ARG, "triangle index out of range");
+  return upload_geometry(h, verts, nverts, tris, ntris, normals);
+}
+
+int dsmc_read_raw_mesh(const char* path, float* verts, uint32_t* nverts, uint32_t* tris,
+                       uint32_t* ntris, float* face_normals) {
+  if (!path || !nverts || !ntris) return DSMC_ERR_ARG;
+  std::vector<float> v, fn;
+  std::vector<uint32_t> t;
+  int st = dsmcb::read_raw_mesh(path, v, t, fn);
+  if (st) return st;
+  *nverts = (uint32_t)(v.size() / 3);
+  *ntris = (uint32_t)(t.size() / 3);
+  if (verts) std::memcpy(verts, v.data(), v.size() * 4);
+  if (tris) std::memcpy(tris, t.data(), t.size() * 4);
+  if (face_normals) {
+    if (fn.size() == t.size()) std::memcpy(face_normals, fn.data(), fn.size() * 4);
+    else {
+      std::vector<float> n;
+      dsmcb::face_normals(v, t, n);
+      std::memcpy(face_normals, n.data(), n.size() * 4);
+    }
+  }
+  return DSMC_OK;
+}
+
+int dsmc_mesh_icosphere(int level, float radius, const float center[3], float* verts,
+                        uint32_t* nverts, uint32_t* tris, uint32_t* ntris) {
+  if (level < 0 || level > 8 || !(radius > 0) || !center || !nverts || !ntris) return DSMC_ERR_ARG;
+  std::vector<float> v;
+  std::vector<uint32_t> t;
+  dsmcb::mesh_icosphere(level, radius, center, v, t);
+  *nverts = (uint32_t)(v.size() / 3);
+  *ntris = (uint32_t)(t.size() / 3);
+  if (verts) std::memcpy(verts, v.data(), v.size() * 4);
+  if (tris) std::memcpy(tris, t.data(), t.size() * 4);
+  return DSMC_OK;
+}
+
+int dsmc_mesh_capsule(float nose_radius, float cone_half_angle_deg, float length,
+                      const float nose_center[3], uint32_t ntarget, uint64_t seed, float* verts,
+                      uint32_t* nverts, uint32_t* tris, uint32_t* ntris) {
+  if (!(nose_radius > 0) || !(cone_half_angle_deg > 0) || cone_half_angle_deg >= 90 ||
+      !(length > nose_radius) || !nose_center || !nverts || !ntris)
+    return DSMC_ERR_ARG;
+  std::vector<float> v;
+  std::vector<uint32_t> t;
+  dsmcb::mesh_capsule(nose_radius, cone_half_angle_deg, length, nose_center, ntarget, seed, v, t);
+  *nverts = (uint32_t)(v.size() / 3);
+  *ntris = (uint32_t)(t.size() / 3);
+  if (verts) std::memcpy(verts, v.data(), v.size() * 4);
+  if (tris) std::memcpy(tris, t.data(), t.size() * 4);
+  return DSMC_OK;
+}
+
+// Cells whose corners touch a flagged geometry cell get no particles
+// (IsGeometryInCell, kernels/dsmc_kernel.cu:478-546).
+static bool geometry_in_cell(const dsmcb::GeomGrid& g, const float cmin[3], const float cs[3]) {
+  auto flagged = [&](float x, float y, float z) {
+    if (x < g.bbox[0] || y < g.bbox[1] || z < g.bbox[2] || x > g.bbox[3] || y > g.bbox[4] ||
+        z > g.bbox[5])
+      return false;
+    auto cvt = [](float f) -> uint32_t { return f > 0.f ? (f >= 4294967296.0f ? 0xffffffffu : (uint32_t)f) : 0u; };
+    uint32_t ix = std::min(cvt((x - g.bbox[0]) / g.cell[0]), g.dim[0] - 1);
+    uint32_t iy = std::min(cvt((y - g.bbox[1]) / g.cell[1]), g.dim[1] - 1);
+    uint32_t iz = std::min(cvt((z - g.bbox[2]) / g.cell[2]), g.dim[2] - 1);
+    return g.flags[iz * g.dim[0] * g.dim[1] + iy * g.dim[0] + ix] != 0;
+  };
+  float x0 = cmin[0], y0 = cmin[1], z0 = cmin[2];
+  float x1 = x0 + cs[0], y1 = y0 + cs[1], z1 = z0 + cs[2];
+  return flagged(x0, y0, z0) || flagged(x1, y0, z0) || flagged(x1, y1, z0) ||
+         flagged(x1, y1, z1) || flagged(x0, y1, z0) || flagged(x0, y1, z1) ||
+         flagged(x0, y0, z1) || flagged(x1, y0, z1);
+}
+
+int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) {
+  if (!h) return DSMC_ERR_ARG;
+  const dsmc_config& c = h->cfg;
+  std::vector<uint32_t> slot(h->cells + 1);
+  uint64_t n = 0;
+  const bool geo = h->has_geom && c.geometry;
+  for (uint32_t cell = 0; cell < h->cells; cell++) {
+    uint32_t cx = cell % c.grid_dim[0], cy = (cell / c.grid_dim[0]) % c.grid_dim[1],
+             cz = cell / (c.grid_dim[0] * c.grid_dim[1]);
+    float cmin[3] = {c.grid_min[0] + cx * h->cell_size[0], c.grid_min[1] + cy * h->cell_size[1],
+                     c.grid_min[2] + cz * h->cell_size[2]};
+    if (geo && geometry_in_cell(h->ggrid, cmin, h->cell_size)) {
+      slot[cell] = 0xffffffffu;
+      continue;
+    }
+    slot[cell] = (uint32_t)n;
+    n += h->ppc;
+  }
+  if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "initial particles exceed capacity");
+  CK(h, cudaMemcpyAsync(h->start, slot.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
+     "init upload");
+  dsmcb::InitParams ip{};
+  ip.grid = h->grid;
+  ip.cells = h->cells;
+  ip.ppc = h->ppc;
+  ip.kind = c.init_kind;
+  ip.vstd = std::sqrt(1.3806e-23f * c.temp / c.gas_mass);
+  ip.vstd2 = std::sqrt(1.3806e-23f * (c.init_temp2 > 0 ? c.init_temp2 : c.temp) / c.gas_mass);
+  ip.vmp = std::sqrt(2 * 1.3806e-23f * c.temp / c.gas_mass);
+  const float* sv = stream_vel ? stream_vel : c.stream_vel;
+  ip.stream = make_float3(sv[0], sv[1], sv[2]);
+  ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
+  ip.cell_slot = h->start;
+  ip.out = soa_of(h->A);
+  CK(h, dsmcb::launch_init_fill(ip, h->stream), "init fill");
+  int st = reindex(h, (uint32_t)n);
+  if (st) return st;
+  if (n_out) *n_out = (uint32_t)n;
+  return DSMC_OK;
+}
+
+int dsmc_upload_state(dsmc_handle* h, const float* pos, const float* vel, uint32_t n, int soa) {
+  if (!h || (n && (!pos || (!vel && !soa)))) return fail(h, DSMC_ERR_ARG, "null state");
+  if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "state exceeds particle capacity");
+  if (soa) {
+    for (int k = 0; k < 6; k++)
+      CK(h, cudaMemcpyAsync(h->A[k], pos + (size_t)k * n, (size_t)n * 4, cudaMemcpyHostToDevice,
+                            h->stream), "upload");
+  } else {
+    std::vector<float> t((size_t)n * 6);
+    for (uint32_t i = 0; i < n; i++)
+      for (int k = 0; k < 3; k++) {
+        t[(size_t)k * n + i] = pos[4 * (size_t)i + k];
+        t[(size_t)(3 + k) * n + i] = vel[4 * (size_t)i + k];
+      }
+    for (int k = 0; k < 6; k++)
+      CK(h, cudaMemcpyAsync(h->A[k], t.data() + (size_t)k * n, (size_t)n * 4,
+                            cudaMemcpyHostToDevice, h->stream), "upload");
+    CK(h, cudaStreamSynchronize(h->stream), "upload sync");
+  }
+  return reindex(h, n);
+}
+
+int dsmc_download_state(dsmc_handle* h, float* pos, float* vel, uint32_t* n_io, int soa) {
+  if (!h || !n_io) return fail(h, DSMC_ERR_ARG, "null argument");
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  uint32_t n = h->has_state ? m.n_alive + m.n_pending : 0;
+  uint32_t cap = *n_io;
+  *n_io = n;
+  if (!pos) return DSMC_OK;
+  if (cap < n) return fail(h, DSMC_ERR_ARG, "output buffer too small");
+  if (soa) {
+    for (int k = 0; k < 6; k++)
+      CK(h, cudaMemcpy(pos + (size_t)k * n, h->A[k], (size_t)n * 4, cudaMemcpyDeviceToHost),
+         "download");
+  } else {
+    std::vector<float> t((size_t)n * 6);
+    for (int k = 0; k < 6; k++)
+      CK(h, cudaMemcpy(t.data() + (size_t)k * n, h->A[k], (size_t)n * 4, cudaMemcpyDeviceToHost),
+         "download");
+    for (uint32_t i = 0; i < n; i++) {
+      for (int k = 0; k < 3; k++) {
+        pos[4 * (size_t)i + k] = t[(size_t)k * n + i];
+        if (vel) vel[4 * (size_t)i + k] = t[(size_t)(3 + k) * n + i];
+      }
+      pos[4 * (size_t)i + 3] = 1.f;
+      if (vel) vel[4 * (size_t)i + 3] = 0.f;
+    }
+  }
+  return DSMC_OK;
+}
+
+int dsmc_set_cell_state(dsmc_handle* h, const float* maxrem, const uint32_t* seeds) {
+  if (!h) return DSMC_ERR_ARG;
+  if (maxrem)
+    CK(h, cudaMemcpy(h->maxrem, maxrem, h->cells * sizeof(float2), cudaMemcpyHostToDevice), "upload");
+  if (seeds)
+    CK(h, cudaMemcpy(h->seeds, seeds, h->cells * sizeof(uint4), cudaMemcpyHostToDevice), "upload");
+  return DSMC_OK;
+}
+
+int dsmc_get_cell_state(dsmc_handle* h, float* maxrem, uint32_t* seeds) {
+  if (!h) return DSMC_ERR_ARG;
+  CK(h, cudaStreamSynchronize(h->stream), "sync");
+  if (maxrem)
+    CK(h, cudaMemcpy(maxrem, h->maxrem, h->cells * sizeof(float2), cudaMemcpyDeviceToHost), "download");
+  if (seeds)
+    CK(h, cudaMemcpy(seeds, h->seeds, h->cells * sizeof(uint4), cudaMemcpyDeviceToHost), "download");
+  return DSMC_OK;
+}
+
+int dsmc_step(dsmc_handle* h, float dt, int nsteps) {
+  if (!h || nsteps < 0) return DSMC_ERR_ARG;
+  if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
+  for (int i = 0; i < nsteps; i++) {
+    cudaError_t e = enqueue_step(h, dt);
+    if (e) return cuda_fail(h, e, "step launch");
+    h->step++;
+    h->sim_time += dt;
+  }
+  return DSMC_OK;
+}
+
+int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps) {
+  if (!h || nsteps < 0) return DSMC_ERR_ARG;
+  if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
+  if (!h->graph_exec || h->graph_dt != dt) {
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->graph_exec = nullptr;
+    h->graph = nullptr;
+    cudaStream_t cap = nullptr;
+    CK(h, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph stream");
+    cudaStream_t saved = h->stream;
+    const bool prof = h->profiling;
+    h->profiling = false;  // per-kernel events are not captured into the graph
+    h->stream = cap;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    if (!e) e = enqueue_step(h, dt);
+    cudaError_t e2 = cudaStreamEndCapture(cap, &h->graph);
+    h->stream = saved;
+    h->profiling = prof;
+    cudaStreamDestroy(cap);
+    if (e || e2) return cuda_fail(h, e ? e : e2, "graph capture");
+    CK(h, cudaGraphInstantiate(&h->graph_exec, h->graph, 0), "graph instantiate");
+    h->graph_dt = dt;
+  }
+  for (int i = 0; i < nsteps; i++) {
+    CK(h, cudaGraphLaunch(h->graph_exec, h->stream), "graph launch");
+    h->step++;
+    h->sim_time += dt;
+  }
+  return DSMC_OK;
+}
+
+int dsmc_sample(dsmc_handle* h) {
+  if (!h) return DSMC_ERR_ARG;
+  if (!h->has_state) return fail(h, DSMC_ERR_STATE, "no particle state");
+  if (h->step == 0) return fail(h, DSMC_ERR_STATE, "sampling needs the cell order of a step");
+  CK(h, dsmcb::launch_sample_cells(h->A[3], h->A[4], h->A[5], h->start, h->cells, h->acc, h->cells,
+                                   1, h->stream), "sample");
+  // one more sampling pass
+  static const uint32_t one = 1;
+  (void)one;
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  m.samples += 1;
+  CK(h, cudaMemcpy(&h->meta->samples, &m.samples, 4, cudaMemcpyHostToDevice), "meta");
+  return DSMC_OK;
+}
+
+int dsmc_reset_samples(dsmc_handle* h) {
+  if (!h) return DSMC_ERR_ARG;
+  CK(h, cudaMemsetAsync(h->acc, 0, 5 * (size_t)h->cells * sizeof(double), h->stream), "memset");
+  CK(h, cudaMemsetAsync(&h->meta->samples, 0, 4, h->stream), "memset");
+  CK(h, cudaStreamSynchronize(h->stream), "sync");
+  return DSMC_OK;
+}
+
+int dsmc_read_cell_sums(dsmc_handle* h, double* sums5, uint32_t* nsamples) {
+  if (!h) return DSMC_ERR_ARG;
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  if (nsamples) *nsamples = m.samples;
+  if (sums5) {
+    std::vector<double> t(5 * (size_t)h->cells);
+    CK(h, cudaMemcpy(t.data(), h->acc, t.size() * 8, cudaMemcpyDeviceToHost), "download");
+    for (uint32_t c = 0; c < h->cells; c++)
+      for (int f = 0; f < 5; f++) sums5[5 * (size_t)c + f] = t[(size_t)f * h->cells + c];
+  }
+  return DSMC_OK;
+}
+
+int dsmc_read_fields(dsmc_handle* h, double* fields5) {
+  if (!h || !fields5) return DSMC_ERR_ARG;
+  std::vector<double> s(5 * (size_t)h->cells);
+  uint32_t ns = 0;
+  int st = dsmc_read_cell_sums(h, s.data(), &ns);
+  if (st) return st;
+  const double k = 1.3806e-23, m = h->cfg.gas_mass;
+  for (uint32_t c = 0; c < h->cells; c++) {
+    const double* a = &s[5 * (size_t)c];
+    double* o = &fields5[5 * (size_t)c];
+    double N = a[0];
+    o[0] = ns ? h->cfg.fnum * N / (h->cell_volume * (double)ns) : 0.0;
+    if (N > 0) {
+      double ux = a[1] / N, uy = a[2] / N, uz = a[3] / N;
+      o[1] = ux; o[2] = uy; o[3] = uz;
+      o[4] = m * (a[4] / N - (ux * ux + uy * uy + uz * uz)) / (3.0 * k);
+    } else {
+      o[1] = o[2] = o[3] = o[4] = 0.0;
+    }
+  }
+  return DSMC_OK;
+}
+
+int dsmc_get_totals(dsmc_handle* h, double totals[3]) {
+  if (!h || !totals) return DSMC_ERR_ARG;
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  totals[0] = (double)m.selections;
+  totals[1] = (double)m.collisions;
+  totals[2] = m.sum_g;
+  return DSMC_OK;
+}
+
+// ProcessAndOutputStatistics, kernels/dsmc_base.cu:104-163.
+int dsmc_dump_statistics(dsmc_handle* h, const char* path) {
+  if (!h || !path) return DSMC_ERR_ARG;
+  double tot[3];
+  int st = dsmc_get_totals(h, tot);
+  if (st) return st;
+  std::vector<double> f(5 * (size_t)h->cells), s(5 * (size_t)h->cells);
+  uint32_t ns = 0;
+  if ((st = dsmc_read_cell_sums(h, s.data(), &ns))) return st;
+  if ((st = dsmc_read_fields(h, f.data()))) return st;
+  FILE* out = std::fopen(path, "w");
+  if (!out) return fail(h, DSMC_ERR_IO, std::string("cannot write ") + path);
+  std::fprintf(out, "Selections: %g\nCollisions: %g\nMean separation: %g\nCollision ratio: %g\n",
+               tot[0], tot[1], tot[1] > 0 ? tot[2] / tot[1] : 0.0, tot[0] > 0 ? tot[1] / tot[0] : 0.0);
+  std::fprintf(out, "Simulation time: %g Running time: 0\n", h->sim_time);
+  std::fprintf(out, "Cell N  ||  SampNum  ||  Dens  ||          Velocity          ||  Temperature\n");
+  double tavg = 0, navg = 0;
+  for (uint32_t c = 0; c < h->cells; c++) {
+    const double* o = &f[5 * (size_t)c];
+    tavg += o[4];
+    navg += o[0];
+    std::fprintf(out, "%u  ||  %u  ||  %g  ||  %g,%g,%g  ||  %g\n", c, (uint32_t)s[5 * (size_t)c], o[0],
+                 o[1], o[2], o[3], o[4]);
+  }
+  tavg /= h->cells;
+  navg /= h->cells;
+  const dsmc_config& c = h->cfg;
+  double gv = (double)(c.grid_max[0] - c.grid_min[0]) * (c.grid_max[1] - c.grid_min[1]) *
+              (c.grid_max[2] - c.grid_min[2]);
+  double n2d2 = (double)c.density * c.gas_diam * c.gas_diam * c.density;
+  double tcoll = 2.0 * h->sim_time * n2d2 * gv * M_PI * std::pow(tavg / c.gas_tref, 0.25) *
+                 std::sqrt(1.3806e-23 * c.gas_tref / (M_PI * c.gas_mass)) / c.fnum;
+  std::fprintf(out, "\n\nExpected collisions: %g Ratio: %g\n", tcoll, tot[1] > 0 ? tcoll / tot[1] : 0.0);
+  std::fprintf(out, "Average temperature: %g Reference temperature is: %g\nAverage density: %g Reference density: %g\n\n\n",
+               tavg, c.temp, navg, c.density);
+  std::fclose(out);
+  return DSMC_OK;
+}
+
+// Snapshot: magic, version, config, counters, particles (SoA), per-cell state.
+static const char kSnapMagic[8] = {'D', 'S', 'M', 'C', 'B', '2', '0', '0'};
+
+int dsmc_snapshot(dsmc_handle* h, const char* path) {
+  if (!h || !path) return DSMC_ERR_ARG;
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  uint32_t n = h->has_state ? m.n_alive + m.n_pending : 0;
+  std::vector<float> part((size_t)n * 6);
+  for (int k = 0; k < 6; k++)
+    CK(h, cudaMemcpy(part.data() + (size_t)k * n, h->A[k], (size_t)n * 4, cudaMemcpyDeviceToHost), "snapshot");
+  std::vector<float2> mr(h->cells);
+  std::vector<uint4> sd(h->cells);
+  std::vector<double> acc(5 * (size_t)h->cells);
+  std::vector<float> rem(6);
+  CK(h, cudaMemcpy(mr.data(), h->maxrem, h->cells * sizeof(float2), cudaMemcpyDeviceToHost), "snapshot");
+  CK(h, cudaMemcpy(sd.data(), h->seeds, h->cells * sizeof(uint4), cudaMemcpyDeviceToHost), "snapshot");
+  CK(h, cudaMemcpy(acc.data(), h->acc, acc.size() * 8, cudaMemcpyDeviceToHost), "snapshot");
+  CK(h, cudaMemcpy(rem.data(), h->inj_rem, 6 * 4, cudaMemcpyDeviceToHost), "snapshot");
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return fail(h, DSMC_ERR_IO, std::string("cannot write ") + path);
+  uint32_t ver = 1;
+  f.write(kSnapMagic, 8);
+  f.write((const char*)&ver, 4);
+  f.write((const char*)&h->cfg, sizeof(dsmc_config));
+  f.write((const char*)&h->cells, 4);
+  f.write((const char*)&n, 4);
+  f.write((const char*)&h->step, 8);
+  f.write((const char*)&h->sim_time, 8);
+  f.write((const char*)&m, sizeof(Meta));
+  f.write((const char*)part.data(), part.size() * 4);
+  f.write((const char*)mr.data(), mr.size() * sizeof(float2));
+  f.write((const char*)sd.data(), sd.size() * sizeof(uint4));
+  f.write((const char*)acc.data(), acc.size() * 8);
+  f.write((const char*)rem.data(), rem.size() * 4);
+  if (!f) return fail(h, DSMC_ERR_IO, "snapshot write failed");
+  return DSMC_OK;
+}
+
+int dsmc_restore(dsmc_handle* h, const char* path) {
+  if (!h || !path) return DSMC_ERR_ARG;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return fail(h, DSMC_ERR_IO, std::string("cannot read ") + path);
+  char mg[8];
+  uint32_t ver = 0, cells = 0, n = 0;
+  dsmc_config cfg;
+  f.read(mg, 8);
+  f.read((char*)&ver, 4);
+  if (!f || std::memcmp(mg, kSnapMagic, 8) != 0 || ver != 1)
+    return fail(h, DSMC_ERR_IO, "not a dsmc_b200 snapshot");
+  f.read((char*)&cfg, sizeof(cfg));
+  f.read((char*)&cells, 4);
+  f.read((char*)&n, 4);
+  if (cells != h->cells) return fail(h, DSMC_ERR_CONFIG, "snapshot cell count differs from the handle's");
+  if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "snapshot particles exceed capacity");
+  uint64_t step = 0;
+  double t = 0;
+  Meta m{};
+  f.read((char*)&step, 8);
+  f.read((char*)&t, 8);
+  f.read((char*)&m, sizeof(Meta));
+  std::vector<float> part((size_t)n * 6);
+  std::vector<float2> mr(cells);
+  std::vector<uint4> sd(cells);
+  std::vector<double> acc(5 * (size_t)cells);
+  std::vector<float> rem(6);
+  f.read((char*)part.data(), part.size() * 4);
+  f.read((char*)mr.data(), mr.size() * sizeof(float2));
+  f.read((char*)sd.data(), sd.size() * sizeof(uint4));
+  f.read((char*)acc.data(), acc.size() * 8);
+  f.read((char*)rem.data(), rem.size() * 4);
+  if (!f) return fail(h, DSMC_ERR_IO, "truncated snapshot");
+  int st = dsmc_upload_state(h, part.data(), nullptr, n, 1);
+  if (st) return st;
+  CK(h, cudaMemcpy(h->maxrem, mr.data(), cells * sizeof(float2), cudaMemcpyHostToDevice), "restore");
+  CK(h, cudaMemcpy(h->seeds, sd.data(), cells * sizeof(uint4), cudaMemcpyHostToDevice), "restore");
+  CK(h, cudaMemcpy(h->acc, acc.data(), acc.size() * 8, cudaMemcpyHostToDevice), "restore");
+  CK(h, cudaMemcpy(h->inj_rem, rem.data(), 6 * 4, cudaMemcpyHostToDevice), "restore");
+  Meta cur{};
+  CK(h, cudaMemcpy(&cur, h->meta, sizeof(Meta), cudaMemcpyDeviceToHost), "restore");
+  cur.step = m.step;
+  cur.selections = m.selections;
+  cur.collisions = m.collisions;
+  cur.sum_g = m.sum_g;
+  cur.samples = m.samples;
+  cur.injected = m.injected;
+  cur.removed = m.removed;
+  CK(h, cudaMemcpy(h->meta, &cur, sizeof(Meta), cudaMemcpyHostToDevice), "restore");
+  h->step = step;
+  h->sim_time = t;
+  return DSMC_OK;
+}
+
+// ------------------------------------------------------------ stage API ----
+
+static GridGeom grid_of(const dsmc_grid* g) {
+  GridGeom r;
+  r.gmin = make_float3(g->gmin[0], g->gmin[1], g->gmin[2]);
+  r.gmax = make_float3(g->gmax[0], g->gmax[1], g->gmax[2]);
+  r.cell = make_float3(g->cell[0], g->cell[1], g->cell[2]);
+  r.dim = make_uint3(g->dim[0], g->dim[1], g->dim[2]);
+  return r;
+}
+
+int dsmc_stage_cell_index(const dsmc_grid* g, const float* x, const float* y, const float* z,
+                          uint32_t n, uint32_t* keys, uint32_t* idx, void* stream) {
+  if (!g || (n && (!x || !y || !z || !keys))) return DSMC_ERR_ARG;
+  cudaError_t e = dsmcb::launch_cell_ids(grid_of(g), x, y, z, n, keys, idx, (cudaStream_t)stream);
+  return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+int dsmc_stage_sort_workspace(uint32_t n, uint32_t nkeys, size_t* bytes) {
+  if (!bytes || nkeys == 0) return DSMC_ERR_ARG;
+  uint32_t tiles = (nkeys + dsmcb::kScanTile - 1) / dsmcb::kScanTile;
+  if (tiles > (uint32_t)dsmcb::kMaxScanTiles) return DSMC_ERR_ARG;
+  *bytes = align256(4ull * (nkeys + 1)) * 2 + align256(4ull * tiles) + align256(4ull * n) * 3 +
+           align256(sizeof(Meta));
+  return DSMC_OK;
+}
+
+int dsmc_stage_sort(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t nkeys,
+                    uint32_t* cell_start, void* workspace, size_t workspace_bytes, void* stream) {
+  size_t need = 0;
+  if (dsmc_stage_sort_workspace(n, nkeys, &need)) return DSMC_ERR_ARG;
+  if (n && (!keys || !vals)) return DSMC_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  bool own = false;
+  if (!workspace) {
+    if (cudaMallocAsync(&workspace, need, s) != cudaSuccess) return DSMC_ERR_OOM;
+    own = true;
+  } else if (workspace_bytes < need) {
+    return DSMC_ERR_ARG;
+  }
+  char* w = (char*)workspace;
+  uint32_t tiles = (nkeys + dsmcb::kScanTile - 1) / dsmcb::kScanTile;
+  uint32_t* count = (uint32_t*)w; w += align256(4ull * (nkeys + 1));
+  uint32_t* start = (uint32_t*)w; w += align256(4ull * (nkeys + 1));
+  uint32_t* tsum = (uint32_t*)w; w += align256(4ull * tiles);
+  uint32_t* ticket = (uint32_t*)w; w += align256(4ull * n);
+  uint32_t* tval = (uint32_t*)w; w += align256(4ull * n);
+  uint32_t* tpos = (uint32_t*)w; w += align256(4ull * n);
+  Meta* meta = (Meta*)w;
+  cudaError_t e = cudaMemsetAsync(count, 0, 4ull * (nkeys + 1), s);
+  if (!e) e = cudaMemsetAsync(tsum, 0, 4ull * tiles, s);
+  if (!e) e = cudaMemsetAsync(meta, 0, sizeof(Meta), s);
+  if (!e && n) e = dsmcb::launch_count_keys(keys, n, nkeys, ticket, count, tsum, tiles, s);
+  if (!e) e = dsmcb::launch_scan(count, start, nkeys, tsum, tiles, meta, 0, s);
+  if (!e && n) e = dsmcb::launch_scatter_kv(keys, vals, ticket, start, n, nkeys, tval, tpos, s);
+  if (!e && n) e = dsmcb::launch_segment_fixup(start, nkeys, tval, tpos, keys, vals, s);
+  if (!e && cell_start) e = cudaMemcpyAsync(cell_start, start, 4ull * (nkeys + 1), cudaMemcpyDeviceToDevice, s);
+  if (own) cudaFreeAsync(workspace, s);
+  return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+int dsmc_stage_bounds_reorder(const uint32_t* sorted_keys, const uint32_t* sorted_idx, uint32_t n,
+                              uint32_t ncells, uint32_t* cell_start_end, const float* const src[6],
+                              float* const dst[6], void* stream) {
+  if (n && (!sorted_keys || !cell_start_end)) return DSMC_ERR_ARG;
+  if ((src || dst) && (!src || !dst || !sorted_idx)) return DSMC_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(cell_start_end, 0, 8ull * ncells, s);
+  if (!e && n) e = dsmcb::launch_bounds_reorder(sorted_keys, sorted_idx, n, ncells, cell_start_end, src, dst, s);
+  return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+int dsmc_stage_collide(const dsmc_collide_params* cp, float* u, float* v, float* w,
+                       const uint32_t* cell_start, float* maxrem, uint32_t* seeds, float* stat4,
+                       void* stream) {
+  if (!cp || !u || !v || !w || !cell_start || !maxrem) return DSMC_ERR_ARG;
+  if (cp->rng == DSMC_RNG_TAUS && !seeds) return DSMC_ERR_ARG;
+  dsmcb::StepParams p{};
+  p.cells = cp->ncells;
+  p.cell_volume = cp->cell_volume;
+  p.cross_section = cp->cross_section;
+  p.fnum = cp->fnum;
+  p.avg_conc = cp->avg_conc;
+  p.dt = cp->dt;
+  p.hard_sphere = std::fabs(cp->omega - 0.5f) < 1e-9f;
+  p.vhs_exp = 2.f * cp->omega - 1.f;
+  p.vhs_gref = cp->vhs_gref;
+  p.ntc_local = cp->ntc_local;
+  p.rng_kind = cp->rng;
+  p.seed = make_uint2((uint32_t)cp->seed, (uint32_t)(cp->seed >> 32));
+  p.in = SoA{u, v, w, u, v, w};
+  p.out = p.in;
+  p.start = cell_start;
+  p.maxrem = (float2*)maxrem;
+  p.seeds = (uint4*)seeds;
+  p.stat4 = (float4*)stat4;
+  p.meta = nullptr;
+  p.flags = dsmcb::kDoCollide | dsmcb::kVelOnly;
+  p.cells_per_tile = 256;
+  p.n_tiles = (cp->ncells + 255) / 256;
+  p.step_override = cp->step ? cp->step : 1u;
+  cudaError_t e = dsmcb::launch_cell(p, (cudaStream_t)stream);
+  return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+int dsmc_stage_move(dsmc_handle* h, const dsmc_move_params* mp, float* x, float* y, float* z,
+                    float* u, float* v, float* w, uint32_t n, void* stream) {
+  if (!mp || (n && (!x || !y || !z || !u || !v || !w))) return DSMC_ERR_ARG;
+  dsmcb::StepParams p{};
+  if (h) p = base_params(h, mp->dt);
+  p.grid = grid_of(&mp->grid);
+  p.dt = mp->dt;
+  p.periodic = mp->periodic;
+  p.face_mode = mp->face_mode;
+  for (int i = 0; i < 6; i++) {
+    p.face_kind[i] = mp->face_kind[i];
+    p.face_vstd[i] = mp->face_vstd[i];
+  }
+  p.seed = make_uint2((uint32_t)mp->seed, (uint32_t)(mp->seed >> 32));
+  if (!h) p.has_geom = 0;
+  p.out = SoA{x, y, z, u, v, w};
+  cudaError_t e = dsmcb::launch_move(p, n, mp->step ? mp->step : 1u, (cudaStream_t)stream);
+  return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint32_t* cell_start,
+                      uint32_t ncells, double* sums5, void* stream) {
+  if (!u || !v || !w || !cell_start || !sums5) return DSMC_ERR_ARG;
+  cudaError_t e = dsmcb::launch_sample_cells(u, v, w, cell_start, ncells, sums5, 1, 5,
+                                             (cudaStream_t)stream);
+  return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,355 @@
+// Device arithmetic for the DSMC timestep.
+//
+// Every function that has a counterpart in the reference evaluates the same
+// FP32 expressions in the same order (with the same promotions to double), so
+// nvcc makes the same contraction choices and the results agree with the
+// reference's own kernels.  Counterparts are cited as file:line of
+// denglide/CudaDsmc.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dsmcb {
+
+constexpr float kPiF = 3.14159265358979f;      // DSMC_PI, include/dsmc.h:26
+constexpr double kBounceDelta = 0.001;         // BOUNCE_DELTA, kernels/dsmc_kernel.cu:53
+constexpr uint32_t kCollisionLimit = 10u;      // COLLISION_LIMIT, kernels/dsmc_kernel.cu:1250
+constexpr float kPathEps = 0.0001f;            // EPS, kernels/dsmc_kernel.cu:1251
+constexpr float kModelWidth = 0.0001f;         // MODEL_WIDTH, kernels/dsmc_kernel.cu:1253
+constexpr double kTriEpsilon = 0.000001;       // EPSILON, kernels/tri_intersect.cu:1
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr uint32_t kDeadKey = 0xffffffffu;     // key of a particle that left the domain
+constexpr float kBoltzmann = 1.3806e-23f;      // DSMC_BOLZ, include/dsmc.h:33
+
+// ------------------------------------------------------------------ RNG ----
+
+// TausStep / LCGStep / HybridTausRng(Int), kernels/mtwister.cu:118-153.
+__device__ __forceinline__ uint32_t taus_step(uint32_t& z, int s1, int s2, int s3, uint32_t m) {
+  uint32_t b = ((z << s1) ^ z) >> s2;
+  z = ((z & m) << s3) ^ b;
+  return z;
+}
+
+__device__ __forceinline__ uint32_t hybrid_taus_int(uint4& s) {
+  uint32_t a = taus_step(s.x, 13, 19, 12, 4294967294u);
+  uint32_t b = taus_step(s.y, 2, 25, 4, 4294967288u);
+  uint32_t c = taus_step(s.z, 3, 11, 17, 4294967280u);
+  s.w = s.w * 1664525u + 1013904223u;
+  return a ^ b ^ c ^ s.w;
+}
+
+__device__ __forceinline__ float hybrid_taus_float(uint4& s) {
+  return (float)(2.3283064365387e-10 * (double)hybrid_taus_int(s));
+}
+
+// Philox-4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, SC'11):
+// ten rounds of two 32x32->64 multiplies mixed with the key, the key bumped by
+// the Weyl increments between rounds.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// A Philox stream: (key, counter words 1..3 fixed) and a running block index
+// in word 0; hands out 32-bit words four at a time.
+struct PhiloxStream {
+  uint2 key;
+  uint32_t c1, c2, c3;
+  uint32_t block;
+  uint4 buf;
+  int used;
+  __device__ __forceinline__ void init(uint2 k, uint32_t a, uint32_t b, uint32_t c) {
+    key = k; c1 = a; c2 = b; c3 = c; block = 0; used = 4;
+  }
+  __device__ __forceinline__ uint32_t next() {
+    if (used == 4) {
+      buf = philox4x32_10(make_uint4(block++, c1, c2, c3), key);
+      used = 0;
+    }
+    uint32_t r = used == 0 ? buf.x : used == 1 ? buf.y : used == 2 ? buf.z : buf.w;
+    used++;
+    return r;
+  }
+  // uniform in (0, 1): 24 random bits, offset by half an ulp of 2^-24
+  __device__ __forceinline__ float uniform() {
+    return ((float)(next() >> 8) + 0.5f) * (1.0f / 16777216.0f);
+  }
+};
+
+// ------------------------------------------------------------ geometry ----
+
+// float -> uint as the reference's implicit conversions compile
+// (cvt.rzi.u32.f32: truncation, saturation, NaN -> 0).
+__device__ __forceinline__ uint32_t f2u(float f) { return (uint32_t)f; }
+
+struct GridGeom {
+  float3 gmin, gmax, cell;
+  uint3 dim;
+};
+
+// GetCellID3D, kernels/dsmc_kernel.cu:1701-1710.
+__device__ __forceinline__ uint32_t cell_id3d(const GridGeom& g, float px, float py, float pz) {
+  uint32_t x = (px - g.gmin.x) / g.cell.x;
+  uint32_t y = (py - g.gmin.y) / g.cell.y;
+  uint32_t z = (pz - g.gmin.z) / g.cell.z;
+  return min(z, g.dim.z - 1) * g.dim.x * g.dim.y + min(y, g.dim.y - 1) * g.dim.x +
+         min(x, g.dim.x - 1);
+}
+
+// GetCollisionCellID(float4), kernels/dsmc_kernel.cu:180-204.
+__device__ __forceinline__ uint32_t coll_cell_id(const GridGeom& g, float3 p) {
+  if (p.x < g.gmin.x || p.y < g.gmin.y || p.z < g.gmin.z || p.x > g.gmax.x || p.y > g.gmax.y ||
+      p.z > g.gmax.z)
+    return kNone;
+  uint32_t x = (p.x - g.gmin.x) / g.cell.x;
+  uint32_t y = (p.y - g.gmin.y) / g.cell.y;
+  uint32_t z = (p.z - g.gmin.z) / g.cell.z;
+  x = min(x, g.dim.x - 1);
+  y = min(y, g.dim.y - 1);
+  z = min(z, g.dim.z - 1);
+  return z * g.dim.x * g.dim.y + y * g.dim.x + x;
+}
+
+// normalize / length / distance4 / reflect4, kernels/vectors.cu:24-106.
+__device__ __forceinline__ float3 normalize3(float3 v) {
+  float l = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
+  if (l > 0) return make_float3(v.x / l, v.y / l, v.z / l);
+  return v;
+}
+
+__device__ __forceinline__ float length3(float3 vec) {
+  return sqrtf(vec.x * vec.x + vec.y * vec.y + vec.z * vec.z);
+}
+
+__device__ __forceinline__ float distance3(float3 v1, float3 v2) {
+  return sqrtf((v2.x - v1.x) * (v2.x - v1.x) + (v2.y - v1.y) * (v2.y - v1.y) +
+               (v2.z - v1.z) * (v2.z - v1.z));
+}
+
+__device__ __forceinline__ float3 reflect3(float3 v, float3 n) {
+  float dt = v.x * n.x + v.y * n.y + v.z * n.z;
+  return make_float3(v.x - 2 * dt * n.x, v.y - 2 * dt * n.y, v.z - 2 * dt * n.z);
+}
+
+// Moller-Trumbore ray/triangle test, kernels/tri_intersect.cu:14-56.
+__device__ __forceinline__ bool intersect_triangle(float3 orig, float3 dir, float3 vert0,
+                                                   float3 vert1, float3 vert2, float* t, float* u,
+                                                   float* v) {
+  float3 edge1, edge2, tvec, pvec, qvec;
+  edge1.x = vert1.x - vert0.x; edge1.y = vert1.y - vert0.y; edge1.z = vert1.z - vert0.z;
+  edge2.x = vert2.x - vert0.x; edge2.y = vert2.y - vert0.y; edge2.z = vert2.z - vert0.z;
+  pvec.x = dir.y * edge2.z - dir.z * edge2.y;
+  pvec.y = dir.z * edge2.x - dir.x * edge2.z;
+  pvec.z = dir.x * edge2.y - dir.y * edge2.x;
+  float det = edge1.x * pvec.x + edge1.y * pvec.y + edge1.z * pvec.z;
+  if (det > -kTriEpsilon && det < kTriEpsilon) return false;
+  float inv_det = __frcp_rn(det);  // == (float)(1.0 / (double)det), correctly rounded
+  tvec.x = orig.x - vert0.x; tvec.y = orig.y - vert0.y; tvec.z = orig.z - vert0.z;
+  *u = (tvec.x * pvec.x + tvec.y * pvec.y + tvec.z * pvec.z) * inv_det;
+  if (*u < 0.0f || *u > 1.0f) return false;
+  qvec.x = tvec.y * edge1.z - tvec.z * edge1.y;
+  qvec.y = tvec.z * edge1.x - tvec.x * edge1.z;
+  qvec.z = tvec.x * edge1.y - tvec.y * edge1.x;
+  *v = (dir.x * qvec.x + dir.y * qvec.y + dir.z * qvec.z) * inv_det;
+  if (*v < 0.0f || *u + *v > 1.0f) return false;
+  *t = (edge2.x * qvec.x + edge2.y * qvec.y + edge2.z * qvec.z) * inv_det;
+  return true;
+}
+
+// Geometry on the device: the uniform grid over the body, a per-cell flag,
+// per-cell [start,end) into the bin entries, and per bin entry the three
+// vertices with the face normal packed into the .w lanes.
+struct GeomView {
+  GridGeom grid;
+  const uint32_t* flags;
+  const uint2* start_end;
+  const float4* tri;  // 3 float4 per bin entry: (v0, n.x), (v1, n.y), (v2, n.z)
+  int diffuse;        // 0: specular (reference); 1: diffuse at wall_temp
+  float wall_vstd;    // sqrt(k T_wall / m)
+  int nearest;        // 0: reference first-hit in start/end cells; 1: nearest hit along the path
+};
+
+// Ray/triangle test with a determinant threshold relative to the triangle's
+// size (the reference's absolute 1e-6 rejects near-grazing rays on small
+// triangles).
+__device__ __forceinline__ bool intersect_triangle_rel(float3 o, float3 d, float3 a, float3 b,
+                                                       float3 c, float* t) {
+  float3 e1 = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
+  float3 e2 = make_float3(c.x - a.x, c.y - a.y, c.z - a.z);
+  float3 pv = make_float3(d.y * e2.z - d.z * e2.y, d.z * e2.x - d.x * e2.z, d.x * e2.y - d.y * e2.x);
+  float det = e1.x * pv.x + e1.y * pv.y + e1.z * pv.z;
+  float scale = (e1.x * e1.x + e1.y * e1.y + e1.z * e1.z) + (e2.x * e2.x + e2.y * e2.y + e2.z * e2.z);
+  if (fabsf(det) <= 1e-9f * scale) return false;
+  float inv = 1.0f / det;
+  float3 tv = make_float3(o.x - a.x, o.y - a.y, o.z - a.z);
+  float u = (tv.x * pv.x + tv.y * pv.y + tv.z * pv.z) * inv;
+  if (u < 0.f || u > 1.f) return false;
+  float3 qv = make_float3(tv.y * e1.z - tv.z * e1.y, tv.z * e1.x - tv.x * e1.z, tv.x * e1.y - tv.y * e1.x);
+  float v = (d.x * qv.x + d.y * qv.y + d.z * qv.z) * inv;
+  if (v < 0.f || u + v > 1.f) return false;
+  *t = (e2.x * qv.x + e2.y * qv.y + e2.z * qv.z) * inv;
+  return true;
+}
+
+// Nearest triangle crossed by the segment o + s d, s in [0, dist] (d unit),
+// among the triangles of every geometry cell the segment passes through
+// (Amanatides-Woo traversal of the uniform grid).
+__device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, float3 d, float dist,
+                                                 float* t_out, uint32_t* entry_out) {
+  const GridGeom& g = G.grid;
+  float t0 = 0.f, t1 = dist;
+  float oa[3] = {o.x, o.y, o.z}, da[3] = {d.x, d.y, d.z};
+  float lo[3] = {g.gmin.x, g.gmin.y, g.gmin.z}, hi[3] = {g.gmax.x, g.gmax.y, g.gmax.z};
+  float cs[3] = {g.cell.x, g.cell.y, g.cell.z};
+  int dm[3] = {(int)g.dim.x, (int)g.dim.y, (int)g.dim.z};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (fabsf(da[a]) < 1e-30f) {
+      if (oa[a] < lo[a] || oa[a] > hi[a]) return false;
+    } else {
+      float ta = (lo[a] - oa[a]) / da[a], tb = (hi[a] - oa[a]) / da[a];
+      if (ta > tb) { float s = ta; ta = tb; tb = s; }
+      t0 = fmaxf(t0, ta);
+      t1 = fminf(t1, tb);
+    }
+  }
+  if (t0 > t1) return false;
+  int idx[3], stp[3];
+  float tmax[3], tdel[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    float p = oa[a] + da[a] * t0;
+    int i = (int)floorf((p - lo[a]) / cs[a]);
+    idx[a] = min(max(i, 0), dm[a] - 1);
+    if (da[a] > 0.f) {
+      stp[a] = 1;
+      tmax[a] = (lo[a] + (idx[a] + 1) * cs[a] - oa[a]) / da[a];
+      tdel[a] = cs[a] / da[a];
+    } else if (da[a] < 0.f) {
+      stp[a] = -1;
+      tmax[a] = (lo[a] + idx[a] * cs[a] - oa[a]) / da[a];
+      tdel[a] = -cs[a] / da[a];
+    } else {
+      stp[a] = 0;
+      tmax[a] = 3.0e38f;
+      tdel[a] = 3.0e38f;
+    }
+  }
+  float best = 3.0e38f;
+  uint32_t best_i = kNone;
+  const int max_iter = dm[0] + dm[1] + dm[2] + 3;
+  for (int it = 0; it < max_iter; it++) {
+    uint32_t c = ((uint32_t)idx[2] * g.dim.y + (uint32_t)idx[1]) * g.dim.x + (uint32_t)idx[0];
+    if (__ldg(&G.flags[c]) != 0) {
+      uint2 se = __ldg(&G.start_end[c]);
+      for (uint32_t i = se.x; i < se.y; i++) {
+        float4 A = __ldg(&G.tri[3 * (size_t)i]);
+        float4 B = __ldg(&G.tri[3 * (size_t)i + 1]);
+        float4 C = __ldg(&G.tri[3 * (size_t)i + 2]);
+        float t;
+        if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
+                                   make_float3(C.x, C.y, C.z), &t) &&
+            t >= 0.f && t <= dist && t < best) {
+          best = t;
+          best_i = i;
+        }
+      }
+    }
+    float texit = fminf(tmax[0], fminf(tmax[1], tmax[2]));
+    if (best <= texit || texit > t1) break;
+    int a = (tmax[0] <= tmax[1] && tmax[0] <= tmax[2]) ? 0 : (tmax[1] <= tmax[2] ? 1 : 2);
+    idx[a] += stp[a];
+    if (idx[a] < 0 || idx[a] >= dm[a]) break;
+    tmax[a] += tdel[a];
+  }
+  if (best_i == kNone) return false;
+  *t_out = best;
+  *entry_out = best_i;
+  return true;
+}
+
+// Diffuse re-emission about the unit normal n on the side the particle came
+// from (full accommodation at the wall temperature): normal speed from the
+// flux-weighted half-range Maxwellian, tangential components Gaussian.
+__device__ __forceinline__ float3 diffuse_emit(float3 n_out, float vstd, PhiloxStream& rng) {
+  float r1 = rng.uniform(), r2 = rng.uniform(), r3 = rng.uniform();
+  float vn = vstd * sqrtf(-2.0f * logf(r1));
+  float rad = vstd * sqrtf(-2.0f * logf(r2));
+  float s, c;
+  sincosf(6.2831853f * r3, &s, &c);
+  float t1 = rad * c, t2 = rad * s;
+  // orthonormal tangent basis of n_out
+  float3 a = fabsf(n_out.x) < 0.9f ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
+  float3 e1 = normalize3(make_float3(a.y * n_out.z - a.z * n_out.y, a.z * n_out.x - a.x * n_out.z,
+                                     a.x * n_out.y - a.y * n_out.x));
+  float3 e2 = make_float3(n_out.y * e1.z - n_out.z * e1.y, n_out.z * e1.x - n_out.x * e1.z,
+                          n_out.x * e1.y - n_out.y * e1.x);
+  return make_float3(vn * n_out.x + t1 * e1.x + t2 * e2.x, vn * n_out.y + t1 * e1.y + t2 * e2.y,
+                     vn * n_out.z + t1 * e1.z + t2 * e2.z);
+}
+
+// CollideWithGeometry, kernels/dsmc_kernel.cu:1256-1314: the first triangle
+// of the cell's list (in list order) that the path crosses reflects the
+// particle; the remaining path continues from the hit point.
+__device__ __forceinline__ bool collide_with_geometry(const GeomView& G, float3* pos, float3* vel,
+                                                      float3* old_pos, uint32_t cellid,
+                                                      PhiloxStream* rng) {
+  uint2 idx_stend = __ldg(&G.start_end[cellid]);
+  float3 dir = normalize3(*vel);
+  float t, u, v;
+  float dist = distance3(*old_pos, *pos);
+  if (dist < kPathEps) return false;
+  for (uint32_t i = idx_stend.x; i < idx_stend.y; i++) {
+    float4 a = __ldg(&G.tri[3 * (size_t)i]);
+    float4 b = __ldg(&G.tri[3 * (size_t)i + 1]);
+    float4 c = __ldg(&G.tri[3 * (size_t)i + 2]);
+    float3 v1 = make_float3(a.x, a.y, a.z), v2 = make_float3(b.x, b.y, b.z),
+           v3 = make_float3(c.x, c.y, c.z);
+    if (intersect_triangle(*old_pos, dir, v1, v2, v3, &t, &u, &v)) {
+      if (t >= 0 && t <= dist) {
+        float uv = 1 - u - v;
+        float3 norm = make_float3(a.w, b.w, c.w);
+        float3 width = make_float3(norm.x * kModelWidth, norm.y * kModelWidth, norm.z * kModelWidth);
+        float3 p;
+        p.x = v1.x * uv + v2.x * u + v3.x * v;
+        p.y = v1.y * uv + v2.y * u + v3.y * v;
+        p.z = v1.z * uv + v2.z * u + v3.z * v;
+        if (G.diffuse) {
+          // re-emit on the side the particle arrived from; the rest of the
+          // step's flight time continues at the new velocity
+          float sp = length3(*vel);
+          float side = (dir.x * norm.x + dir.y * norm.y + dir.z * norm.z) > 0.f ? -1.f : 1.f;
+          float3 n_out = make_float3(side * norm.x, side * norm.y, side * norm.z);
+          *vel = diffuse_emit(n_out, G.wall_vstd, *rng);
+          width = make_float3(n_out.x * kModelWidth, n_out.y * kModelWidth, n_out.z * kModelWidth);
+          float tau = (dist - t) / sp;
+          pos->x = p.x + vel->x * tau;
+          pos->y = p.y + vel->y * tau;
+          pos->z = p.z + vel->z * tau;
+        } else {
+          *vel = reflect3(*vel, norm);
+          float3 p1p = normalize3(*vel);
+          float od = dist - t;
+          pos->x = p.x + p1p.x * od;
+          pos->y = p.y + p1p.y * od;
+          pos->z = p.z + p1p.z * od;
+        }
+        old_pos->x = p.x + width.x;
+        old_pos->y = p.y + width.y;
+        old_pos->z = p.z + width.z;
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
+}  // namespace dsmcb

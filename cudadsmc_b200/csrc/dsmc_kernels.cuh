@@ -1,0 +1,190 @@
+// Kernel parameter blocks and launch helpers for the DSMC timestep.
+//
+// One timestep (dsmc_step) is three launches on the handle's stream:
+//   scan     per-cell particle counts -> exclusive cell starts (counts reset)
+//   scatter  each particle to start[key] + ticket of the sorted array, with its
+//            position in the unsorted array (`orig`)
+//   cell     per tile of cells, staged in shared memory: restore the stable
+//            (key, orig) order inside each cell, NTC collisions, free flight
+//            with mesh and boundary collisions, optional FP64 sampling, the
+//            next step's cell key and a ticket from the per-cell counter.
+// The cell kernel writes the state back in sorted order, which is the array the
+// next step's scatter reads: the reference's sort + reorder + collide + move
+// sequence (include/gpu_dsmc.inl:220-274) with two passes over particle memory.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dsmc_device.cuh"
+
+namespace dsmcb {
+
+constexpr int kCellThreads = 256;     // threads of the cell kernel
+constexpr int kTileCapacity = 3072;   // particles staged per chunk of a tile
+constexpr int kMaxCellsPerTile = 256;
+constexpr int kScanTile = 2048;       // cells per scan block (256 threads x 8)
+constexpr int kScanShift = 11;
+constexpr int kMaxScanTiles = 2048;   // => at most 4M cells
+
+// Device-side counters shared by the step's kernels.
+struct Meta {
+  uint32_t n_alive;   // particles placed in cells by the last scan
+  uint32_t n_pending; // particles appended after them since (inflow)
+  uint32_t n_scatter; // particles the current step's scatter reads
+  uint32_t step;      // timestep counter (reference m_state->stepCount)
+  uint32_t error;     // error bits (kErr*)
+  unsigned long long selections;
+  unsigned long long collisions;
+  double sum_g;
+  uint32_t giant_cells;  // cells handled by the out-of-shared-memory path
+  uint32_t samples;      // sampling passes
+  uint32_t injected;     // particles injected by the inflow faces (total)
+  uint32_t removed;      // particles removed through outflow faces (total)
+  uint32_t pad;
+  unsigned long long particle_steps;  // sum over steps of the particles placed by the scan
+};
+
+enum : uint32_t {
+  kErrCapacity = 1u,   // injection would exceed the buffer capacity
+  kErrKeyRange = 2u,   // a key >= cells reached the scatter
+};
+
+struct SoA {
+  float* x; float* y; float* z; float* u; float* v; float* w;
+};
+
+enum : int {
+  kDoFixup = 1,    // restore (key, orig) order inside each cell
+  kDoCollide = 2,
+  kDoMove = 4,
+  kDoKeys = 8,     // next-step key + ticket + tile histogram
+  kDoSample = 16,  // FP64 sampling after the move (every sample_every steps)
+  kSampleForce = 32,  // sample regardless of the step counter
+  kVelOnly = 64,      // stage only velocities (collide stage)
+};
+
+// Inflow description for a face that injects (extension).
+struct Inflow {
+  int face;            // 0..5 (-x,+x,-y,+y,-z,+z); -1: none
+  float number_flux;   // simulator particles per unit area per second
+  float3 stream;       // free-stream velocity
+  float vstd;          // sqrt(k T / m)
+  float area;
+};
+
+struct StepParams {
+  GridGeom grid;
+  uint32_t cells;
+  float cell_volume;
+  float cross_section;
+  float fnum;
+  float avg_conc;
+  float dt;
+  int periodic;
+  int hard_sphere;
+  float vhs_exp;   // 2*omega - 1
+  float vhs_gref;
+  int ntc_local;
+  int rng_kind;    // 0 HybridTaus per cell, 1 Philox
+  uint2 seed;
+  int face_mode;
+  int face_kind[6];
+  float face_vstd[6];
+  int has_geom;
+  GeomView geom;
+
+  // buffers
+  SoA in;             // state the cell kernel reads (sorted by scatter)
+  const uint32_t* in_orig;
+  SoA out;            // state the cell kernel writes (sorted order)
+  uint2* out_kt;      // next-step (key, ticket)
+  const uint32_t* start;   // cells+1 exclusive starts
+  uint32_t* count;         // per-cell counters for the next step
+  uint32_t* tile_sum;      // per scan tile counters for the next step
+  uint32_t n_scan_tiles;
+  float2* maxrem;
+  uint4* seeds;
+  float4* stat4;           // optional per-cell (selections, collisions, sum g)
+  double* acc;             // 5 x cells FP64 accumulators (SoA), optional
+  Meta* meta;
+  int flags;
+  int sample_every;
+  int cells_per_tile;
+  uint32_t n_tiles;
+  uint32_t step_override;  // 0: use meta->step
+};
+
+// Launchers (all asynchronous on `stream`).
+cudaError_t launch_index(const GridGeom& g, uint32_t cells, const float* x, const float* y,
+                         const float* z, uint32_t n, uint2* kt, uint32_t* count,
+                         uint32_t* tile_sum, uint32_t n_scan_tiles, int face_mode,
+                         cudaStream_t stream);
+cudaError_t launch_scan(uint32_t* count, uint32_t* start, uint32_t cells, const uint32_t* tile_sum,
+                        uint32_t n_scan_tiles, Meta* meta, int bump_step, cudaStream_t stream);
+cudaError_t launch_scatter(const SoA& src, SoA dst, const uint2* kt, const uint32_t* start,
+                           uint32_t* orig, uint32_t cells, uint32_t* tile_sum,
+                           uint32_t n_scan_tiles, Meta* meta, uint32_t capacity,
+                           cudaStream_t stream);
+cudaError_t launch_cell(const StepParams& p, cudaStream_t stream);
+int cell_kernel_smem_bytes();
+// Free flight + boundaries in place on p.out for n particles (move stage);
+// particles that leave through an outflow face get x = NaN.
+cudaError_t launch_move(const StepParams& p, uint32_t n, uint32_t step, cudaStream_t stream);
+// keys[i] = cell id of particle i, idx[i] = i (cell-index stage).
+cudaError_t launch_cell_ids(const GridGeom& g, const float* x, const float* y, const float* z,
+                            uint32_t n, uint32_t* keys, uint32_t* idx, cudaStream_t stream);
+
+// Sort stage pieces (dsmc_stage_sort).
+cudaError_t launch_count_keys(const uint32_t* keys, uint32_t n, uint32_t nkeys, uint32_t* ticket,
+                              uint32_t* count, uint32_t* tile_sum, uint32_t n_scan_tiles,
+                              cudaStream_t stream);
+cudaError_t launch_scatter_kv(const uint32_t* keys, const uint32_t* vals, const uint32_t* ticket,
+                              const uint32_t* start, uint32_t n, uint32_t nkeys, uint32_t* tmp_val,
+                              uint32_t* tmp_pos, cudaStream_t stream);
+cudaError_t launch_segment_fixup(const uint32_t* start, uint32_t nkeys, const uint32_t* tmp_val,
+                                 const uint32_t* tmp_pos, uint32_t* keys_out, uint32_t* vals_out,
+                                 cudaStream_t stream);
+cudaError_t launch_bounds_reorder(const uint32_t* keys, const uint32_t* idx, uint32_t n,
+                                  uint32_t ncells, uint32_t* cse, const float* const src[6], float* const dst[6],
+                                  cudaStream_t stream);
+// acc[field * fstride + cell * cstride] += sums (field 0..4: n, u, v, w, |v|^2)
+cudaError_t launch_sample_cells(const float* u, const float* v, const float* w,
+                                const uint32_t* start, uint32_t cells, double* acc,
+                                size_t fstride, size_t cstride, cudaStream_t stream);
+
+// Initial fill (dsmc_init_state).
+struct InitParams {
+  GridGeom grid;
+  uint32_t cells;
+  uint32_t ppc;
+  int kind;          // 0 reference sampler, 1 Maxwellian, 2 bimodal
+  float vstd;        // sqrt(kT/m)
+  float vstd2;       // bimodal second temperature
+  float vmp;         // sqrt(2kT/m), reference sampler
+  float3 stream;
+  uint2 seed;
+  const uint32_t* cell_slot;  // per cell: first particle index, kNone = skipped cell
+  SoA out;
+};
+cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);
+
+// Inflow injection: appends particles after meta->n_alive and sets n_total.
+struct InjectParams {
+  GridGeom grid;
+  uint32_t cells;
+  Inflow inflow;
+  float dt;
+  uint2 seed;
+  uint32_t capacity;
+  float* remainder;  // device float carrying the fractional particle count
+  SoA st;            // the array the next scatter reads
+  uint2* kt;
+  uint32_t* count;
+  uint32_t* tile_sum;
+  uint32_t* plan;    // 2 words of device scratch: first slot, count
+  Meta* meta;
+};
+cudaError_t launch_inject(const InjectParams& p, cudaStream_t stream);
+
+}  // namespace dsmcb

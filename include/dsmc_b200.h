@@ -1,0 +1,326 @@
+/* dsmc_b200 - B200-native DSMC timestep behind a plain C ABI.
+ *
+ * Drop-in boundary for the GPU solver path of denglide/CudaDsmc.  Every entry
+ * point names the reference interface it replaces (file:line in that
+ * project).  Conventions, compared with the reference:
+ *   - state lives in a handle (the reference keeps it in module-level statics,
+ *     kernels/dsmc_kernel.cu:117-137), so several solvers can coexist;
+ *   - work is ordered on the handle's CUDA stream (dsmc_set_stream);
+ *   - no exceptions cross the ABI: every call returns DSMC_OK or an error
+ *     code and dsmc_last_error() describes the last failure (the reference
+ *     polls cudaGetLastError and throws std::runtime_error,
+ *     kernels/dsmc_kernel.cu:2053-2072);
+ *   - particle state is structure-of-arrays FP32 (x, y, z, u, v, w) on the
+ *     device; the host-side upload/download calls also accept the reference's
+ *     float4 AoS layout.
+ */
+#ifndef DSMC_B200_H
+#define DSMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSMC_B200_ABI_VERSION 1
+
+/* Status codes. */
+enum {
+  DSMC_OK = 0,
+  DSMC_ERR_ARG = 1,      /* invalid argument */
+  DSMC_ERR_CONFIG = 2,   /* unreadable or inconsistent configuration */
+  DSMC_ERR_CUDA = 3,     /* a CUDA call failed */
+  DSMC_ERR_OOM = 4,      /* device allocation failed */
+  DSMC_ERR_STATE = 5,    /* call out of order (e.g. step before init) */
+  DSMC_ERR_CAPACITY = 6, /* particle count exceeded the handle's capacity */
+  DSMC_ERR_IO = 7,       /* file could not be read */
+  DSMC_ERR_DEVICE = 8    /* a kernel reported an error flag */
+};
+
+/* Boundary kinds of the six domain faces (extension; the reference only has
+ * its four boundary functors, kernels/dsmc_kernel.cu:1316-1555). */
+enum {
+  DSMC_FACE_SPECULAR = 0,
+  DSMC_FACE_DIFFUSE = 1,
+  DSMC_FACE_OUTFLOW = 2,
+  DSMC_FACE_PERIODIC = 3,
+  DSMC_FACE_INFLOW = 4 /* outflow face that also injects free-stream particles */
+};
+
+enum { DSMC_RNG_TAUS = 0, DSMC_RNG_PHILOX = 1 };
+enum { DSMC_INIT_REFERENCE = 0, DSMC_INIT_MAXWELL = 1, DSMC_INIT_BIMODAL = 2 };
+
+/* Simulation settings: settings_t (include/sim_settings.h:32-69) plus the
+ * extensions this library adds.  dsmc_config_default() gives the reference
+ * defaults (include/dsmc.h, src/sim_settings.cpp:35-44). */
+typedef struct dsmc_config {
+  /* --- reference settings_t --- */
+  float grid_min[3];
+  float grid_max[3];
+  int grid_dim[3];
+  float density;        /* number density, m^-3 */
+  float fnum;           /* real molecules per simulator particle */
+  float temp;           /* free-stream temperature, K */
+  float stream_vel[3];  /* m/s */
+  char periodic;        /* 'x','y','z' or 'n' (reference boundary functors) */
+  float gas_mass;       /* kg */
+  float gas_diam;       /* m, at gas_tref */
+  float gas_tref;       /* K */
+  float dt;             /* s */
+  int geometry;         /* 1: collide with the mesh set by dsmc_set_mesh */
+  int benchmark;
+  /* --- extensions --- */
+  float gas_omega;      /* VHS viscosity exponent; 0.5 = hard sphere (reference) */
+  int ntc_local;        /* 0: NTC uses the initial particles per cell (reference,
+                           include/gpu_dsmc.inl:250); 1: uses N_c - 1 (Bird) */
+  int rng;              /* DSMC_RNG_TAUS (reference per-cell HybridTaus) or DSMC_RNG_PHILOX */
+  uint64_t seed;
+  int face_mode;        /* 0: reference functors from `periodic`; 1: face_kind[] */
+  int face_kind[6];     /* -x,+x,-y,+y,-z,+z */
+  float face_temp[6];   /* wall temperature of diffuse faces, K */
+  int wall_diffuse;     /* mesh wall: 0 specular (reference), 1 diffuse */
+  float wall_temp;      /* K */
+  int init_kind;        /* DSMC_INIT_* */
+  float init_temp2;     /* second temperature of the bimodal start, K */
+  int sample_every;     /* sampling interval in steps (reference: 100) */
+  float capacity_factor;/* particle buffer capacity / initial count (>= 1) */
+  uint32_t part_per_cell; /* 0: derive as the reference does, kernels/dsmc.cu:324-330 */
+  int geom_nearest;     /* mesh hits: 0 = the reference's first listed triangle of the start
+                           and end grid cells (kernels/dsmc_kernel.cu:1256-1314,1621-1639);
+                           1 = nearest triangle along the whole path */
+} dsmc_config;
+
+typedef struct dsmc_handle dsmc_handle;
+
+/* Fills the reference defaults (settings_t::settings_t). */
+int dsmc_config_default(dsmc_config* cfg);
+
+/* settings_t::readFromFile (src/sim_settings.cpp:46-132): <grid><min/max/dim>,
+ * <density>, <fnum>, <temp>, <streamvel>, <periodic>, <gas file=...>name</gas>,
+ * plus the extension tags <omega>, <wall kind= T=>, <face ...>, <rng>, <seed>,
+ * <sample every=>.  The gas file is looked up relative to the working
+ * directory first (as the reference does), then to the XML file's directory. */
+int dsmc_config_read_xml(const char* path, dsmc_config* cfg);
+
+/* settings_t::readFromCmdLine (src/sim_settings.cpp:134-186): -f, -benchmark,
+ * -no-geometry, -mt (rejected: not supported), -density, -dt, -run-for. */
+int dsmc_config_from_args(int argc, const char* const* argv, dsmc_config* cfg, float* run_for);
+
+/* CreateSolver(SolverGPU) + DSMCSolver::Init (kernels/dsmc_base.cu:43-47,
+ * 221-233; include/gpu_dsmc.inl:341-378): allocates the particle and per-cell
+ * buffers on the current device. */
+int dsmc_create(const dsmc_config* cfg, dsmc_handle** out);
+int dsmc_destroy(dsmc_handle* h);
+const char* dsmc_last_error(const dsmc_handle* h);
+const char* dsmc_status_string(int status);
+
+/* Orders all of the handle's work on this stream (a cudaStream_t; NULL = legacy default). */
+int dsmc_set_stream(dsmc_handle* h, void* stream);
+/* Synchronises the stream and reports device-side error flags. */
+int dsmc_sync(dsmc_handle* h);
+
+/* Derived quantities (settings_t/main, kernels/dsmc.cu:324-330; InitSimulationProperties,
+ * kernels/dsmc_kernel.cu:309-348). */
+typedef struct dsmc_info {
+  uint32_t part_per_cell;
+  uint32_t cells;
+  uint32_t capacity;
+  uint32_t num_particles;
+  float cell_size[3];
+  float cell_volume;
+  float cross_section;
+  float max_rel_vel;
+  uint64_t step;
+  uint32_t samples;
+  double sim_time;
+  uint64_t particle_steps; /* sum over steps of the particles in cells */
+  uint32_t injected;       /* particles injected by inflow faces (total) */
+  uint32_t removed;        /* particles removed through outflow faces (total) */
+  uint32_t giant_cells;    /* cells processed outside the shared-memory tiles (total) */
+} dsmc_info;
+int dsmc_get_info(dsmc_handle* h, dsmc_info* info);
+
+/* Per-kernel timing with CUDA events recorded around every launch of
+ * dsmc_step on the handle's stream (no equivalent in the reference, which
+ * times the whole loop only, kernels/dsmc.cu:440-449).  dsmc_profile(h, 1)
+ * starts a window, dsmc_profile_read returns per kernel the summed
+ * milliseconds and launch counts since then (kernels: 0 scan, 1 scatter,
+ * 2 cell, 3 inflow injection) and closes the window. */
+int dsmc_profile(dsmc_handle* h, int enable);
+int dsmc_profile_read(dsmc_handle* h, double ms[4], uint32_t launches[4]);
+
+/* DSMCSolver::SetModel -> Model::CreateGrid + InitRegularGrid
+ * (kernels/dsmc_base.cu:49-55, src/model.cpp:733-769,
+ * kernels/dsmc_kernel.cu:350-376): bins the triangle mesh into a uniform grid
+ * of grid_dim cells over the mesh's bounding box and uploads it.  tris holds
+ * 3 vertex ids per triangle; face normals are computed as
+ * normalize(cross(v1-v0, v2-v0)) unless normals (3 floats per triangle) is
+ * given. */
+int dsmc_set_mesh(dsmc_handle* h, const float* verts, uint32_t nverts, const uint32_t* tris,
+                  uint32_t ntris, const float* normals, const int grid_dim[3]);
+
+/* Uploads a prebuilt geometry grid as the reference stores it in .raw files
+ * and reg_grid_t (include/reggrid.h:32-56): bbox, cell size, dims, per-cell
+ * triangle count, triangle ids in bin order, per-cell flag (after the
+ * enclose fill). */
+int dsmc_set_geometry_grid(dsmc_handle* h, const float bbox[6], const float cell[3],
+                           const int dim[3], const uint32_t* cell_count, const uint32_t* tri_ids,
+                           const uint8_t* flags, const float* verts, uint32_t nverts,
+                           const uint32_t* tris, uint32_t ntris, const float* normals);
+
+/* The geometry-grid builder on its own (host; same binning as dsmc_set_mesh).
+ * Returns the number of bin entries through *n_entries (tri_ids holds at most
+ * cap of them). */
+int dsmc_build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tris,
+                             uint32_t ntris, const int grid_dim[3], float bbox[6], float cell[3],
+                             uint32_t* cell_count, uint32_t* tri_ids, uint64_t cap,
+                             uint8_t* flags, uint64_t* n_entries);
+
+/* Model::LoadRaw (src/model.cpp:348-401): reads the reference's .raw mesh
+ * (vertices, indices, face normals).  With verts == NULL only the counts are
+ * returned. */
+int dsmc_read_raw_mesh(const char* path, float* verts, uint32_t* nverts, uint32_t* tris,
+                       uint32_t* ntris, float* face_normals);
+
+/* Triangulated test bodies: an icosphere (subdivision level, 20*4^level
+ * triangles) and a blunt capsule (spherical nose + cone + flat base, ~ntarget
+ * triangles, seeded jitter of the azimuthal start).  With verts == NULL only
+ * the counts are returned. */
+int dsmc_mesh_icosphere(int level, float radius, const float center[3], float* verts,
+                        uint32_t* nverts, uint32_t* tris, uint32_t* ntris);
+int dsmc_mesh_capsule(float nose_radius, float cone_half_angle_deg, float length,
+                      const float nose_center[3], uint32_t ntarget, uint64_t seed, float* verts,
+                      uint32_t* nverts, uint32_t* tris, uint32_t* ntris);
+
+/* GPUDSMCSolver::InitSystemState (include/gpu_dsmc.inl:68-92): fills the
+ * domain with part_per_cell particles per cell (skipping cells flagged as
+ * geometry) and runs a zero-length move.  Returns the particle count. */
+int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out);
+
+/* Host <-> device particle state.  soa != 0: six arrays of n floats
+ * (x,y,z,u,v,w) back to back; soa == 0: pos4 and vel4 float4 AoS as the
+ * reference's particles_state_t.  Upload resets the cell order. */
+int dsmc_upload_state(dsmc_handle* h, const float* pos, const float* vel, uint32_t n, int soa);
+int dsmc_download_state(dsmc_handle* h, float* pos, float* vel, uint32_t* n, int soa);
+/* Per-cell collision state: (sigma*g)max and remainder (float2 per cell,
+ * kernels/dsmc_kernel.cu:131) and HybridTaus seeds (uint4 per cell, :124). */
+int dsmc_set_cell_state(dsmc_handle* h, const float* maxrem, const uint32_t* seeds);
+int dsmc_get_cell_state(dsmc_handle* h, float* maxrem, uint32_t* seeds);
+
+/* RunSimulationStep / DoBenchmark (include/gpu_dsmc.inl:128-274,
+ * kernels/dsmc_base.cu:64-84): nsteps timesteps of length dt, sampling every
+ * sample_every steps.  Asynchronous on the handle's stream. */
+int dsmc_step(dsmc_handle* h, float dt, int nsteps);
+/* Same as dsmc_step but replays a captured CUDA graph of the step. */
+int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps);
+
+/* SampleCellStatistics (kernels/dsmc_kernel.cu:892-910): adds the current
+ * velocities to the FP64 per-cell accumulators now. */
+int dsmc_sample(dsmc_handle* h);
+int dsmc_reset_samples(dsmc_handle* h);
+
+/* Per-cell FP64 accumulators: 5 doubles per cell (count, sum u, sum v, sum w,
+ * sum |v|^2) and the number of sampling passes. */
+int dsmc_read_cell_sums(dsmc_handle* h, double* sums5, uint32_t* nsamples);
+/* ProcessAndOutputStatistics' per-cell fields (kernels/dsmc_base.cu:104-163):
+ * n = fnum N/(V samples), u = sum v / N, T = m (sum|v|^2/N - |u|^2)/(3k);
+ * 5 doubles per cell (n, ux, uy, uz, T). */
+int dsmc_read_fields(dsmc_handle* h, double* fields5);
+/* GetStatistics (kernels/dsmc_kernel.cu:840-854): selections, collisions,
+ * sum of relative speeds of collisions (all steps so far). */
+int dsmc_get_totals(dsmc_handle* h, double totals[3]);
+/* DSMCSolver::DumpStatistics (kernels/dsmc_base.cu:165-174) as text. */
+int dsmc_dump_statistics(dsmc_handle* h, const char* path);
+
+/* Binary snapshot of the whole handle state (particles, per-cell state,
+ * accumulators, counters) and its restore. */
+int dsmc_snapshot(dsmc_handle* h, const char* path);
+int dsmc_restore(dsmc_handle* h, const char* path);
+
+/* ---------------------------------------------------------------------
+ * Stage API: the individual stages of one timestep on caller-owned device
+ * pointers, ordered on `stream` (cudaStream_t).  These run the same device
+ * code as dsmc_step.  Cell grids are described by dsmc_grid.
+ * ------------------------------------------------------------------- */
+typedef struct dsmc_grid {
+  float gmin[3];
+  float gmax[3];
+  float cell[3];
+  uint32_t dim[3];
+} dsmc_grid;
+
+/* CalculateCellIDs (kernels/dsmc_kernel.cu:1712-1732): keys[i] = cell id of
+ * (x[i],y[i],z[i]), idx[i] = i. */
+int dsmc_stage_cell_index(const dsmc_grid* g, const float* x, const float* y, const float* z,
+                          uint32_t n, uint32_t* keys, uint32_t* idx, void* stream);
+
+/* SortParticlesIndices (kernels/dsmc_kernel.cu:2033-2051): stable sort of
+ * (keys, vals) by key, keys < nkeys; also writes the exclusive cell starts
+ * (nkeys+1 entries) when cell_start != NULL.  workspace may be NULL (the call
+ * then allocates on the stream); dsmc_stage_sort_workspace gives its size. */
+int dsmc_stage_sort_workspace(uint32_t n, uint32_t nkeys, size_t* bytes);
+int dsmc_stage_sort(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t nkeys,
+                    uint32_t* cell_start, void* workspace, size_t workspace_bytes, void* stream);
+
+/* FindCellBoundaries (kernels/dsmc_kernel.cu:1734-1808): cell start/end
+ * (uint2 per cell, (0,0) for empty cells) from sorted keys, and the gather of
+ * the six state arrays into sorted order (src -> dst). */
+int dsmc_stage_bounds_reorder(const uint32_t* sorted_keys, const uint32_t* sorted_idx, uint32_t n,
+                              uint32_t ncells, uint32_t* cell_start_end, const float* const src[6],
+                              float* const dst[6], void* stream);
+
+/* Collision constants for the collide stage (gpu_sim_settings_t fields,
+ * kernels/dsmc_kernel.cu:79-101). */
+typedef struct dsmc_collide_params {
+  uint32_t ncells;
+  float cell_volume;
+  float cross_section;
+  float fnum;
+  float avg_conc;
+  float dt;
+  float omega;
+  float vhs_gref;
+  int ntc_local;
+  int rng;
+  uint64_t seed;
+  uint32_t step;
+} dsmc_collide_params;
+
+/* ComputeBirdCollisionsNoMTDev (kernels/dsmc_kernel.cu:912-1102): NTC
+ * collisions in every cell of the sorted velocity arrays (u,v,w in place),
+ * cells given by cell_start (ncells+1 exclusive starts).  maxrem (float2 per
+ * cell) and seeds (uint4 per cell, HybridTaus) are updated; stat4 (float4 per
+ * cell: selections, collisions, sum g) is accumulated when non-NULL. */
+int dsmc_stage_collide(const dsmc_collide_params* p, float* u, float* v, float* w,
+                       const uint32_t* cell_start, float* maxrem, uint32_t* seeds, float* stat4,
+                       void* stream);
+
+/* Move constants: the simulation grid and the boundary treatment. */
+typedef struct dsmc_move_params {
+  dsmc_grid grid;
+  float dt;
+  char periodic;
+  int face_mode;
+  int face_kind[6];
+  float face_vstd[6];
+  uint64_t seed;
+  uint32_t step;
+} dsmc_move_params;
+
+/* IntegrateDev / ProcessCollisionsDev (kernels/dsmc_kernel.cu:1557-1699):
+ * free flight, mesh collisions (with the handle's geometry when h != NULL and
+ * it has one) and the boundary functor, in place on the six arrays. */
+int dsmc_stage_move(dsmc_handle* h, const dsmc_move_params* p, float* x, float* y, float* z,
+                    float* u, float* v, float* w, uint32_t n, void* stream);
+
+/* SampleCellStatisticsDev (kernels/dsmc_kernel.cu:856-910) in FP64: adds
+ * count, sums of u,v,w and |v|^2 per cell into sums5 (5 doubles per cell). */
+int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint32_t* cell_start,
+                      uint32_t ncells, double* sums5, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
