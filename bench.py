@@ -229,13 +229,26 @@ def cpu_oracle_sample(wl, budget_s=12.0, max_threads=None):
 
 # ---------------------------------------------------------------- our arm ---
 
+def reduce_over_ranks(elapsed, count, world, device):
+    """Whole-job timing of independent replicas: the slowest rank's elapsed
+    time and the units all ranks processed.  The only cross-rank traffic of
+    the benchmark."""
+    import torch
+    t = torch.tensor([float(elapsed)], dtype=torch.float64, device=device)
+    c = torch.tensor([float(count)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def algorithmic_bytes(kernel, n_particles, cells, rng_taus, sample_frac):
     """Bytes a kernel must move per launch (SoA FP32 state, 24 B/particle)."""
     if kernel == "scatter":
-        return n_particles * (8 + 24 + 24 + 4)
+        return n_particles * (4 + 24 + 24 + 4)
     if kernel == "cell":
         per_cell = 4 + 16 + (32 if rng_taus else 0) + sample_frac * 80
-        return n_particles * (24 + 4 + 24 + 8) + cells * per_cell
+        return n_particles * (24 + 4 + 24 + 4) + cells * per_cell
     if kernel == "scan":
         return cells * 12
     return 0
@@ -271,13 +284,7 @@ def run_ours(args, rank, world):
     sol.Sync()
     info1 = sol.Info()
     pst = int(info1.particle_steps - info0.particle_steps)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    c = torch.tensor([float(pst)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
-    ms_max = float(t.item())
-    total_ps = float(c.item())
+    ms_max, total_ps = reduce_over_ranks(ms, pst, world, dev)
     value = total_ps / (ms_max * 1e-3)
     launches = sum(v[1] for v in prof.values())
     n_avg = pst / args.steps
@@ -363,13 +370,9 @@ def run_e2e(args, wl, rank, world, dev):
     fields = sol.Fields()
     t1 = time.perf_counter()
     pst = sol.Info().particle_steps - i0
-    el = torch.tensor([t1 - t0], dtype=torch.float64, device=dev)
-    c = torch.tensor([float(pst)], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(el, op=torch.distributed.ReduceOp.MAX)
-        torch.distributed.all_reduce(c, op=torch.distributed.ReduceOp.SUM)
+    el, tot = reduce_over_ranks(t1 - t0, pst, world, dev)
     sol.close()
-    return {"value": float(c.item()) / float(el.item()), "unit": "particle-timesteps/s",
+    return {"value": tot / el, "unit": "particle-timesteps/s",
             "h2d_bytes_per_step": int(state.nbytes / k),
             "d2h_bytes_per_step": int(24 + fields.nbytes / k), "steps": k,
             "note": "upload of the initial pinned state + one C-ABI dsmc_step and a totals read per step "

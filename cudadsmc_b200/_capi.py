@@ -113,6 +113,9 @@ SIGNATURES = [
     ("dsmc_get_cell_state", _I, [_P, _P, _P]),
     ("dsmc_step", _I, [_P, ctypes.c_float, _I]),
     ("dsmc_step_graph", _I, [_P, ctypes.c_float, _I]),
+    ("dsmc_set_kernel_variant", _I, [_P, _I]),
+    ("dsmc_get_kernel_variant", _I, [_P, _P, _P]),
+    ("dsmc_autotune", _I, [_P, ctypes.c_float, _I, _P, _P]),
     ("dsmc_sample", _I, [_P]),
     ("dsmc_reset_samples", _I, [_P]),
     ("dsmc_read_cell_sums", _I, [_P, _P, ctypes.POINTER(_U32)]),

@@ -20,6 +20,7 @@ struct dsmc_handle {
   cudaStream_t stream = nullptr;
 
   uint32_t ppc = 0, cells = 0, capacity = 0, n_scan_tiles = 0, n_tiles = 0, cells_per_tile = 0;
+  int variant = 2;  // cell-kernel variant (dsmc_set_kernel_variant)
   float cell_size[3]{}, cell_volume = 0.f, cross_section = 0.f, max_rel_vel = 0.f;
   float vhs_gref = 0.f;
   GridGeom grid{};
@@ -27,7 +28,8 @@ struct dsmc_handle {
   float* A[6]{};
   float* B[6]{};
   uint32_t* orig = nullptr;
-  uint2* kt = nullptr;
+  uint32_t* keys = nullptr;    // next-step cell key per particle
+  uint32_t* cursor = nullptr;  // per-cell ticket counters of the scatter
   uint32_t* count = nullptr;
   uint32_t* start = nullptr;
   uint32_t* tile_sum = nullptr;
@@ -41,6 +43,7 @@ struct dsmc_handle {
   bool has_geom = false;
   dsmcb::GeomGrid ggrid;
   uint32_t* gflags = nullptr;
+  float* gclear = nullptr;
   uint2* gse = nullptr;
   float4* gtri = nullptr;
 
@@ -86,6 +89,26 @@ int cuda_fail(dsmc_handle* h, cudaError_t e, const char* where) {
     if (e_ != cudaSuccess) return cuda_fail(h, e_, where); \
   } while (0)
 
+void drop_graph(dsmc_handle* h) {
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->graph_exec = nullptr;
+  h->graph = nullptr;
+  h->graph_dt = -1.f;
+}
+
+// Cell-kernel variant and the tile size that goes with it: tiles of about one
+// shared-memory chunk of particles (32..256 cells).
+void apply_variant(dsmc_handle* h, int v) {
+  h->variant = v;
+  const uint64_t cap = (uint64_t)dsmcb::cell_kernel_chunk_capacity(v);
+  uint32_t ct = dsmcb::kMaxCellsPerTile;
+  while (ct > 32 && (uint64_t)ct * std::max<uint32_t>(h->ppc, 1) > cap) ct >>= 1;
+  h->cells_per_tile = ct;
+  h->n_tiles = (h->cells + ct - 1) / ct;
+  drop_graph(h);
+}
+
 uint64_t splitmix64(uint64_t& s) {
   uint64_t z = (s += 0x9E3779B97F4A7C15ull);
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -110,8 +133,8 @@ void free_all(dsmc_handle* h) {
     cudaFree(h->B[i]);
     h->A[i] = h->B[i] = nullptr;
   }
-  void* ps[] = {h->orig, h->kt, h->count, h->start, h->tile_sum, h->maxrem, h->seeds, h->acc,
-                h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gse, h->gtri};
+  void* ps[] = {h->orig, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
+                h->acc, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse, h->gtri};
   for (void* p : ps) cudaFree(p);
 }
 
@@ -136,6 +159,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
   p.fnum = h->cfg.fnum;
   p.avg_conc = (float)h->ppc;
   p.dt = dt;
+  p.ntc_coef = (float)(0.5 * (double)h->cfg.fnum * dt / (double)h->cell_volume);
   p.periodic = h->cfg.periodic;
   p.hard_sphere = std::fabs(h->cfg.gas_omega - 0.5f) < 1e-9f;
   p.vhs_exp = 2.f * h->cfg.gas_omega - 1.f;
@@ -158,6 +182,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.flags = h->gflags;
     p.geom.start_end = h->gse;
     p.geom.tri = h->gtri;
+    p.geom.clear = h->gclear;
     p.geom.diffuse = h->cfg.wall_diffuse;
     p.geom.nearest = h->cfg.geom_nearest;
     p.geom.wall_vstd = std::sqrt(1.3806e-23f * h->cfg.wall_temp / h->cfg.gas_mass);
@@ -210,22 +235,24 @@ cudaError_t timed(dsmc_handle* h, int kernel, F launch) {
 cudaError_t enqueue_step(dsmc_handle* h, float dt) {
   cudaError_t e;
   e = timed(h, 0, [&] {
-    return dsmcb::launch_scan(h->count, h->start, h->cells, h->tile_sum, h->n_scan_tiles, h->meta,
-                              1, h->stream);
+    return dsmcb::launch_scan(h->count, h->cursor, h->start, h->cells, h->tile_sum,
+                              h->n_scan_tiles, h->meta, 1, h->stream);
   });
   if (e) return e;
   e = timed(h, 1, [&] {
-    return dsmcb::launch_scatter(soa_of(h->A), soa_of(h->B), h->kt, h->start, h->orig, h->cells,
-                                 h->tile_sum, h->n_scan_tiles, h->meta, h->capacity, h->stream);
+    return dsmcb::launch_scatter(soa_of(h->A), soa_of(h->B), h->keys, h->start, h->cursor, h->orig,
+                                 h->cells, h->tile_sum, h->n_scan_tiles, h->meta, h->capacity,
+                                 h->stream);
   });
   if (e) return e;
   dsmcb::StepParams p = base_params(h, dt);
   p.in = soa_of(h->B);
   p.in_orig = h->orig;
   p.out = soa_of(h->A);
-  p.out_kt = h->kt;
-  p.flags = dsmcb::kDoFixup | dsmcb::kDoCollide | dsmcb::kDoMove | dsmcb::kDoKeys;
+  p.out_key = h->keys;
+  p.flags = dsmcb::kDoFixup | dsmcb::kDoCollide | dsmcb::kDoMove | dsmcb::kDoKeys | dsmcb::kPadded;
   if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
+  p.cell_variant = h->variant;
   e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
   if (e) return e;
   for (const auto& in : h->inflows) {
@@ -238,9 +265,10 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
     ip.capacity = h->capacity;
     ip.remainder = h->inj_rem + in.face;
     ip.st = soa_of(h->A);
-    ip.kt = h->kt;
+    ip.keys = h->keys;
     ip.count = h->count;
     ip.tile_sum = h->tile_sum;
+    ip.n_scan_tiles = h->n_scan_tiles;
     ip.plan = h->inj_plan + 2 * in.face;
     ip.meta = h->meta;
     e = timed(h, 3, [&] { return dsmcb::launch_inject(ip, h->stream); });
@@ -285,6 +313,7 @@ int check_device_flags(dsmc_handle* h) {
     std::string m = "device error flags:";
     if (err & dsmcb::kErrCapacity) m += " particle capacity exceeded (raise capacity_factor);";
     if (err & dsmcb::kErrKeyRange) m += " cell key out of range;";
+    if (err & dsmcb::kErrTimeout) m += " a bulk copy did not complete within a second;";
     return fail(h, DSMC_ERR_DEVICE, m);
   }
   return DSMC_OK;
@@ -293,7 +322,7 @@ int check_device_flags(dsmc_handle* h) {
 int reindex(dsmc_handle* h, uint32_t n) {
   CK(h, cudaMemsetAsync(h->count, 0, (h->cells + 1) * sizeof(uint32_t), h->stream), "memset");
   CK(h, cudaMemsetAsync(h->tile_sum, 0, h->n_scan_tiles * sizeof(uint32_t), h->stream), "memset");
-  CK(h, dsmcb::launch_index(h->grid, h->cells, h->A[0], h->A[1], h->A[2], n, h->kt, h->count,
+  CK(h, dsmcb::launch_index(h->grid, h->cells, h->A[0], h->A[1], h->A[2], n, h->keys, h->count,
                             h->tile_sum, h->n_scan_tiles, h->cfg.face_mode, h->stream),
      "index kernel");
   uint32_t m2[2] = {n, 0u};
@@ -387,11 +416,7 @@ int dsmc_create(const dsmc_config* cfg, dsmc_handle** out) {
   h->grid.cell = make_float3(h->cell_size[0], h->cell_size[1], h->cell_size[2]);
   h->grid.dim = make_uint3(c.grid_dim[0], c.grid_dim[1], c.grid_dim[2]);
   h->n_scan_tiles = (h->cells + dsmcb::kScanTile - 1) / dsmcb::kScanTile;
-  uint32_t target = 2048;
-  uint32_t ct = 256;
-  while (ct > 32 && (uint64_t)ct * std::max<uint32_t>(h->ppc, 1) > target) ct >>= 1;
-  h->cells_per_tile = ct;
-  h->n_tiles = (h->cells + ct - 1) / ct;
+  apply_variant(h, h->variant);
   float capf = c.capacity_factor < 1.f ? 1.f : c.capacity_factor;
   uint64_t cap = (uint64_t)std::ceil((double)h->ppc * h->cells * capf) + 1024;
   if (cap > 0xF0000000ull) {
@@ -407,7 +432,8 @@ int dsmc_create(const dsmc_config* cfg, dsmc_handle** out) {
     if (!e) e = dalloc(&h->B[i], h->capacity);
   }
   if (!e) e = dalloc(&h->orig, h->capacity);
-  if (!e) e = dalloc(&h->kt, h->capacity);
+  if (!e) e = dalloc(&h->keys, h->capacity);
+  if (!e) e = dalloc(&h->cursor, h->cells + 1);
   if (!e) e = dalloc(&h->count, h->cells + 1);
   if (!e) e = dalloc(&h->start, h->cells + 1);
   if (!e) e = dalloc(&h->tile_sum, h->n_scan_tiles);
@@ -465,11 +491,7 @@ int dsmc_destroy(dsmc_handle* h) {
 int dsmc_set_stream(dsmc_handle* h, void* stream) {
   if (!h) return DSMC_ERR_ARG;
   h->stream = (cudaStream_t)stream;
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-  if (h->graph) cudaGraphDestroy(h->graph);
-  h->graph_exec = nullptr;
-  h->graph = nullptr;
-  h->graph_dt = -1.f;
+  drop_graph(h);
   return DSMC_OK;
 }
 
@@ -562,7 +584,8 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
   const uint32_t gc = g.dim[0] * g.dim[1] * g.dim[2];
   std::vector<uint32_t> flags(gc);
   std::vector<uint2> se(gc);
-  std::vector<float4> tri(3 * g.tri_ids.size() + 3);
+  const size_t stride = dsmcb::kTriStride;
+  std::vector<float4> tri(stride * (g.tri_ids.size() + 1));
   size_t off = 0;
   for (uint32_t c = 0; c < gc; c++) {
     flags[c] = g.flags[c];
@@ -574,30 +597,64 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
       const float* b = verts + 3 * (size_t)tris[3 * t + 1];
       const float* cc = verts + 3 * (size_t)tris[3 * t + 2];
       const float* n = normals + 3 * (size_t)t;
-      tri[3 * (off + k)] = make_float4(a[0], a[1], a[2], n[0]);
-      tri[3 * (off + k) + 1] = make_float4(b[0], b[1], b[2], n[1]);
-      tri[3 * (off + k) + 2] = make_float4(cc[0], cc[1], cc[2], n[2]);
+      tri[stride * (off + k)] = make_float4(a[0], a[1], a[2], n[0]);
+      tri[stride * (off + k) + 1] = make_float4(b[0], b[1], b[2], n[1]);
+      tri[stride * (off + k) + 2] = make_float4(cc[0], cc[1], cc[2], n[2]);
+      // plane of the triangle from its vertices (unit normal, offset)
+      double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+      double e2[3] = {(double)cc[0] - a[0], (double)cc[1] - a[1], (double)cc[2] - a[2]};
+      double pn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                      e1[0] * e2[1] - e1[1] * e2[0]};
+      double l = std::sqrt(pn[0] * pn[0] + pn[1] * pn[1] + pn[2] * pn[2]);
+      if (l > 0) { pn[0] /= l; pn[1] /= l; pn[2] /= l; }
+      tri[stride * (off + k) + 3] = make_float4((float)pn[0], (float)pn[1], (float)pn[2],
+                                                (float)(pn[0] * a[0] + pn[1] * a[1] + pn[2] * a[2]));
     }
     off += g.count[c];
   }
+  // clearance: (Chebyshev cell distance to the nearest cell holding triangles
+  // - 1) x the smallest cell size, a lower bound of the distance from any point
+  // of the cell to the surface (multi-source BFS over the 26-neighbourhood)
+  std::vector<int> dist(gc, -1);
+  std::vector<uint32_t> queue;
+  queue.reserve(gc);
+  for (uint32_t c = 0; c < gc; c++)
+    if (g.count[c]) { dist[c] = 0; queue.push_back(c); }
+  for (size_t qi = 0; qi < queue.size(); qi++) {
+    const uint32_t c = queue[qi];
+    const int cx = (int)(c % g.dim[0]), cy = (int)((c / g.dim[0]) % g.dim[1]),
+              cz = (int)(c / (g.dim[0] * g.dim[1]));
+    for (int dz = -1; dz <= 1; dz++)
+      for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) {
+          const int x = cx + dx, y = cy + dy, z = cz + dz;
+          if (x < 0 || y < 0 || z < 0 || x >= (int)g.dim[0] || y >= (int)g.dim[1] || z >= (int)g.dim[2])
+            continue;
+          const uint32_t nc = ((uint32_t)z * g.dim[1] + (uint32_t)y) * g.dim[0] + (uint32_t)x;
+          if (dist[nc] < 0) { dist[nc] = dist[c] + 1; queue.push_back(nc); }
+        }
+  }
+  const float cmin = std::min(g.cell[0], std::min(g.cell[1], g.cell[2]));
+  std::vector<float> clear(gc);
+  for (uint32_t c = 0; c < gc; c++)
+    clear[c] = dist[c] <= 0 ? (dist[c] < 0 ? 3.0e38f : 0.f) : 0.999f * (float)(dist[c] - 1) * cmin;
   cudaFree(h->gflags);
+  cudaFree(h->gclear);
   cudaFree(h->gse);
   cudaFree(h->gtri);
-  h->gflags = nullptr; h->gse = nullptr; h->gtri = nullptr;
+  h->gflags = nullptr; h->gclear = nullptr; h->gse = nullptr; h->gtri = nullptr;
   CK(h, dalloc(&h->gflags, gc), "geometry alloc");
+  CK(h, dalloc(&h->gclear, gc), "geometry alloc");
   CK(h, dalloc(&h->gse, gc), "geometry alloc");
   CK(h, dalloc(&h->gtri, tri.size()), "geometry alloc");
   CK(h, cudaMemcpy(h->gflags, flags.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
+  CK(h, cudaMemcpy(h->gclear, clear.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
   CK(h, cudaMemcpy(h->gse, se.data(), gc * sizeof(uint2), cudaMemcpyHostToDevice), "geometry upload");
   CK(h, cudaMemcpy(h->gtri, tri.data(), tri.size() * sizeof(float4), cudaMemcpyHostToDevice),
      "geometry upload");
   h->has_geom = true;
   h->cfg.geometry = 1;
-  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-  if (h->graph) cudaGraphDestroy(h->graph);
-  h->graph_exec = nullptr;
-  h->graph = nullptr;
-  h->graph_dt = -1.f;
+  drop_graph(h);
   return DSMC_OK;
 }
 
@@ -838,10 +895,7 @@ int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps) {
   if (!h || nsteps < 0) return DSMC_ERR_ARG;
   if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
   if (!h->graph_exec || h->graph_dt != dt) {
-    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
-    if (h->graph) cudaGraphDestroy(h->graph);
-    h->graph_exec = nullptr;
-    h->graph = nullptr;
+    drop_graph(h);
     cudaStream_t cap = nullptr;
     CK(h, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph stream");
     cudaStream_t saved = h->stream;
@@ -864,6 +918,59 @@ int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps) {
     h->sim_time += dt;
   }
   return DSMC_OK;
+}
+
+int dsmc_set_kernel_variant(dsmc_handle* h, int variant) {
+  if (!h || variant < 0 || variant >= dsmcb::cell_kernel_variants()) return DSMC_ERR_ARG;
+  apply_variant(h, variant);
+  return DSMC_OK;
+}
+
+int dsmc_get_kernel_variant(dsmc_handle* h, int* variant, int* chunk_capacity) {
+  if (!h) return DSMC_ERR_ARG;
+  if (variant) *variant = h->variant;
+  if (chunk_capacity) *chunk_capacity = dsmcb::cell_kernel_chunk_capacity(h->variant);
+  return DSMC_OK;
+}
+
+int dsmc_autotune(dsmc_handle* h, float dt, int steps, int* best, float* ms_per_step) {
+  if (!h || steps < 1) return DSMC_ERR_ARG;
+  if (!h->has_state) return fail(h, DSMC_ERR_STATE, "autotune needs a particle state");
+  const int nv = dsmcb::cell_kernel_variants();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(h, cudaEventCreate(&e0), "event");
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce) {
+    cudaEventDestroy(e0);
+    return cuda_fail(h, ce, "event");
+  }
+  int st = DSMC_OK, pick = h->variant;
+  float best_ms = 0.f;
+  for (int v = 0; v < nv && st == DSMC_OK; v++) {
+    apply_variant(h, v);
+    st = dsmc_step_graph(h, dt, 2);  // capture + warm-up
+    if (st) break;
+    ce = cudaEventRecord(e0, h->stream);
+    if (!ce) st = dsmc_step_graph(h, dt, steps);
+    if (!ce && !st) ce = cudaEventRecord(e1, h->stream);
+    if (!ce && !st) ce = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (!ce && !st) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (ce) st = cuda_fail(h, ce, "autotune timing");
+    if (st) break;
+    ms /= (float)steps;
+    if (ms_per_step) ms_per_step[v] = ms;
+    if (v == 0 || ms < best_ms) {
+      best_ms = ms;
+      pick = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  apply_variant(h, pick);
+  if (best) *best = pick;
+  if (st) return st;
+  return check_device_flags(h);
 }
 
 int dsmc_sample(dsmc_handle* h) {
@@ -1128,7 +1235,7 @@ int dsmc_stage_sort(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t nkeys,
   if (!e) e = cudaMemsetAsync(tsum, 0, 4ull * tiles, s);
   if (!e) e = cudaMemsetAsync(meta, 0, sizeof(Meta), s);
   if (!e && n) e = dsmcb::launch_count_keys(keys, n, nkeys, ticket, count, tsum, tiles, s);
-  if (!e) e = dsmcb::launch_scan(count, start, nkeys, tsum, tiles, meta, 0, s);
+  if (!e) e = dsmcb::launch_scan(count, nullptr, start, nkeys, tsum, tiles, meta, 0, s);
   if (!e && n) e = dsmcb::launch_scatter_kv(keys, vals, ticket, start, n, nkeys, tval, tpos, s);
   if (!e && n) e = dsmcb::launch_segment_fixup(start, nkeys, tval, tpos, keys, vals, s);
   if (!e && cell_start) e = cudaMemcpyAsync(cell_start, start, 4ull * (nkeys + 1), cudaMemcpyDeviceToDevice, s);
@@ -1152,6 +1259,10 @@ int dsmc_stage_collide(const dsmc_collide_params* cp, float* u, float* v, float*
                        void* stream) {
   if (!cp || !u || !v || !w || !cell_start || !maxrem) return DSMC_ERR_ARG;
   if (cp->rng == DSMC_RNG_TAUS && !seeds) return DSMC_ERR_ARG;
+  // the bulk copies of the kernel start on 16-byte boundaries of each array
+  for (const void* a : {(const void*)u, (const void*)v, (const void*)w, (const void*)cell_start,
+                        (const void*)maxrem, (const void*)seeds})
+    if ((uintptr_t)a & 15u) return DSMC_ERR_ARG;
   dsmcb::StepParams p{};
   p.cells = cp->ncells;
   p.cell_volume = cp->cell_volume;
@@ -1159,6 +1270,7 @@ int dsmc_stage_collide(const dsmc_collide_params* cp, float* u, float* v, float*
   p.fnum = cp->fnum;
   p.avg_conc = cp->avg_conc;
   p.dt = cp->dt;
+  p.ntc_coef = (float)(0.5 * (double)cp->fnum * cp->dt / (double)cp->cell_volume);
   p.hard_sphere = std::fabs(cp->omega - 0.5f) < 1e-9f;
   p.vhs_exp = 2.f * cp->omega - 1.f;
   p.vhs_gref = cp->vhs_gref;
@@ -1176,6 +1288,7 @@ int dsmc_stage_collide(const dsmc_collide_params* cp, float* u, float* v, float*
   p.cells_per_tile = 256;
   p.n_tiles = (cp->ncells + 255) / 256;
   p.step_override = cp->step ? cp->step : 1u;
+  p.cell_variant = 0;
   cudaError_t e = dsmcb::launch_cell(p, (cudaStream_t)stream);
   return e ? DSMC_ERR_CUDA : DSMC_OK;
 }

@@ -171,11 +171,17 @@ struct GeomView {
   GridGeom grid;
   const uint32_t* flags;
   const uint2* start_end;
-  const float4* tri;  // 3 float4 per bin entry: (v0, n.x), (v1, n.y), (v2, n.z)
+  // kTriStride float4 per bin entry: (v0, n.x), (v1, n.y), (v2, n.z), (plane normal, offset)
+  const float4* tri;
+  // per cell, a lower bound of the distance from any point of the cell to the
+  // surface (0 in cells holding triangles)
+  const float* clear;
   int diffuse;        // 0: specular (reference); 1: diffuse at wall_temp
   float wall_vstd;    // sqrt(k T_wall / m)
   int nearest;        // 0: reference first-hit in start/end cells; 1: nearest hit along the path
 };
+
+constexpr int kTriStride = 4;
 
 // Ray/triangle test with a determinant threshold relative to the triangle's
 // size (the reference's absolute 1e-6 rejects near-grazing rays on small
@@ -251,9 +257,15 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
     if (__ldg(&G.flags[c]) != 0) {
       uint2 se = __ldg(&G.start_end[c]);
       for (uint32_t i = se.x; i < se.y; i++) {
-        float4 A = __ldg(&G.tri[3 * (size_t)i]);
-        float4 B = __ldg(&G.tri[3 * (size_t)i + 1]);
-        float4 C = __ldg(&G.tri[3 * (size_t)i + 2]);
+        // plane pre-test: both ends of the segment on one side -> no crossing
+        const float4 P = __ldg(&G.tri[kTriStride * (size_t)i + 3]);
+        const float s0 = P.x * o.x + P.y * o.y + P.z * o.z - P.w;
+        const float s1 = s0 + dist * (P.x * d.x + P.y * d.y + P.z * d.z);
+        const float tol = 1e-7f * (fabsf(P.w) + 1.f);
+        if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
+        float4 A = __ldg(&G.tri[kTriStride * (size_t)i]);
+        float4 B = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
+        float4 C = __ldg(&G.tri[kTriStride * (size_t)i + 2]);
         float t;
         if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
                                    make_float3(C.x, C.y, C.z), &t) &&
@@ -308,9 +320,9 @@ __device__ __forceinline__ bool collide_with_geometry(const GeomView& G, float3*
   float dist = distance3(*old_pos, *pos);
   if (dist < kPathEps) return false;
   for (uint32_t i = idx_stend.x; i < idx_stend.y; i++) {
-    float4 a = __ldg(&G.tri[3 * (size_t)i]);
-    float4 b = __ldg(&G.tri[3 * (size_t)i + 1]);
-    float4 c = __ldg(&G.tri[3 * (size_t)i + 2]);
+    float4 a = __ldg(&G.tri[kTriStride * (size_t)i]);
+    float4 b = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
+    float4 c = __ldg(&G.tri[kTriStride * (size_t)i + 2]);
     float3 v1 = make_float3(a.x, a.y, a.z), v2 = make_float3(b.x, b.y, b.z),
            v3 = make_float3(c.x, c.y, c.z);
     if (intersect_triangle(*old_pos, dir, v1, v2, v3, &t, &u, &v)) {

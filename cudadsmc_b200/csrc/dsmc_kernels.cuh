@@ -2,12 +2,12 @@
 //
 // One timestep (dsmc_step) is three launches on the handle's stream:
 //   scan     per-cell particle counts -> exclusive cell starts (counts reset)
-//   scatter  each particle to start[key] + ticket of the sorted array, with its
-//            position in the unsorted array (`orig`)
-//   cell     per tile of cells, staged in shared memory: restore the stable
-//            (key, orig) order inside each cell, NTC collisions, free flight
-//            with mesh and boundary collisions, optional FP64 sampling, the
-//            next step's cell key and a ticket from the per-cell counter.
+//   scatter  each particle to start[key] + a per-cell ticket in the sorted
+//            array, with its position in the unsorted array (`orig`)
+//   cell     per tile of cells, staged in shared memory by bulk copies: the
+//            stable (key, orig) order restored inside each cell, NTC
+//            collisions, free flight with mesh and boundary collisions,
+//            optional FP64 sampling, and the next step's cell key (+ count).
 // The cell kernel writes the state back in sorted order, which is the array the
 // next step's scatter reads: the reference's sort + reorder + collide + move
 // sequence (include/gpu_dsmc.inl:220-274) with two passes over particle memory.
@@ -20,8 +20,6 @@
 
 namespace dsmcb {
 
-constexpr int kCellThreads = 256;     // threads of the cell kernel
-constexpr int kTileCapacity = 3072;   // particles staged per chunk of a tile
 constexpr int kMaxCellsPerTile = 256;
 constexpr int kScanTile = 2048;       // cells per scan block (256 threads x 8)
 constexpr int kScanShift = 11;
@@ -48,6 +46,7 @@ struct Meta {
 enum : uint32_t {
   kErrCapacity = 1u,   // injection would exceed the buffer capacity
   kErrKeyRange = 2u,   // a key >= cells reached the scatter
+  kErrTimeout = 4u,    // a bounded wait on a tile copy ran out
 };
 
 struct SoA {
@@ -58,10 +57,11 @@ enum : int {
   kDoFixup = 1,    // restore (key, orig) order inside each cell
   kDoCollide = 2,
   kDoMove = 4,
-  kDoKeys = 8,     // next-step key + ticket + tile histogram
+  kDoKeys = 8,     // next-step key + count + tile histogram
   kDoSample = 16,  // FP64 sampling after the move (every sample_every steps)
   kSampleForce = 32,  // sample regardless of the step counter
   kVelOnly = 64,      // stage only velocities (collide stage)
+  kPadded = 128,      // buffers carry 16 bytes of slack: whole aligned copies
 };
 
 // Inflow description for a face that injects (extension).
@@ -81,12 +81,13 @@ struct StepParams {
   float fnum;
   float avg_conc;
   float dt;
+  float ntc_coef;  // 0.5 fnum dt / V_c (FP32 selection count of the Philox mode)
   int periodic;
   int hard_sphere;
   float vhs_exp;   // 2*omega - 1
   float vhs_gref;
   int ntc_local;
-  int rng_kind;    // 0 HybridTaus per cell, 1 Philox
+  int rng_kind;    // 0 HybridTaus per cell (reference), 1 Philox
   uint2 seed;
   int face_mode;
   int face_kind[6];
@@ -98,7 +99,7 @@ struct StepParams {
   SoA in;             // state the cell kernel reads (sorted by scatter)
   const uint32_t* in_orig;
   SoA out;            // state the cell kernel writes (sorted order)
-  uint2* out_kt;      // next-step (key, ticket)
+  uint32_t* out_key;  // next-step cell key (kDeadKey: left the domain)
   const uint32_t* start;   // cells+1 exclusive starts
   uint32_t* count;         // per-cell counters for the next step
   uint32_t* tile_sum;      // per scan tile counters for the next step
@@ -113,21 +114,27 @@ struct StepParams {
   int cells_per_tile;
   uint32_t n_tiles;
   uint32_t step_override;  // 0: use meta->step
+  int cell_variant;        // (threads, chunk capacity) of the cell kernel
 };
 
 // Launchers (all asynchronous on `stream`).
 cudaError_t launch_index(const GridGeom& g, uint32_t cells, const float* x, const float* y,
-                         const float* z, uint32_t n, uint2* kt, uint32_t* count,
+                         const float* z, uint32_t n, uint32_t* keys, uint32_t* count,
                          uint32_t* tile_sum, uint32_t n_scan_tiles, int face_mode,
                          cudaStream_t stream);
-cudaError_t launch_scan(uint32_t* count, uint32_t* start, uint32_t cells, const uint32_t* tile_sum,
-                        uint32_t n_scan_tiles, Meta* meta, int bump_step, cudaStream_t stream);
-cudaError_t launch_scatter(const SoA& src, SoA dst, const uint2* kt, const uint32_t* start,
-                           uint32_t* orig, uint32_t cells, uint32_t* tile_sum,
+cudaError_t launch_scan(uint32_t* count, uint32_t* cursor, uint32_t* start, uint32_t cells,
+                        const uint32_t* tile_sum, uint32_t n_scan_tiles, Meta* meta, int bump_step,
+                        cudaStream_t stream);
+cudaError_t launch_scatter(const SoA& src, SoA dst, const uint32_t* keys, const uint32_t* start,
+                           uint32_t* cursor, uint32_t* orig, uint32_t cells, uint32_t* tile_sum,
                            uint32_t n_scan_tiles, Meta* meta, uint32_t capacity,
                            cudaStream_t stream);
+// The timestep's fused cell kernel (also the collide stage with kVelOnly).
 cudaError_t launch_cell(const StepParams& p, cudaStream_t stream);
-int cell_kernel_smem_bytes();
+// Variants of the cell kernel: 0 (512 threads, 2048 particles per chunk,
+// 1 CTA/SM), 1 (256, 1024, 2), 2 (128, 512, 4), 3 (64, 256, up to 8).
+int cell_kernel_variants();
+int cell_kernel_chunk_capacity(int variant);
 // Free flight + boundaries in place on p.out for n particles (move stage);
 // particles that leave through an outflow face get x = NaN.
 cudaError_t launch_move(const StepParams& p, uint32_t n, uint32_t step, cudaStream_t stream);
@@ -146,8 +153,8 @@ cudaError_t launch_segment_fixup(const uint32_t* start, uint32_t nkeys, const ui
                                  const uint32_t* tmp_pos, uint32_t* keys_out, uint32_t* vals_out,
                                  cudaStream_t stream);
 cudaError_t launch_bounds_reorder(const uint32_t* keys, const uint32_t* idx, uint32_t n,
-                                  uint32_t ncells, uint32_t* cse, const float* const src[6], float* const dst[6],
-                                  cudaStream_t stream);
+                                  uint32_t ncells, uint32_t* cse, const float* const src[6],
+                                  float* const dst[6], cudaStream_t stream);
 // acc[field * fstride + cell * cstride] += sums (field 0..4: n, u, v, w, |v|^2)
 cudaError_t launch_sample_cells(const float* u, const float* v, const float* w,
                                 const uint32_t* start, uint32_t cells, double* acc,
@@ -169,7 +176,8 @@ struct InitParams {
 };
 cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);
 
-// Inflow injection: appends particles after meta->n_alive and sets n_total.
+// Inflow injection: appends particles after the ones in cells and counts them
+// for the next scan.
 struct InjectParams {
   GridGeom grid;
   uint32_t cells;
@@ -179,12 +187,16 @@ struct InjectParams {
   uint32_t capacity;
   float* remainder;  // device float carrying the fractional particle count
   SoA st;            // the array the next scatter reads
-  uint2* kt;
+  uint32_t* keys;
   uint32_t* count;
   uint32_t* tile_sum;
+  uint32_t n_scan_tiles;
   uint32_t* plan;    // 2 words of device scratch: first slot, count
   Meta* meta;
 };
 cudaError_t launch_inject(const InjectParams& p, cudaStream_t stream);
+
+int num_sms();
+uint32_t grid_for(uint64_t work, int threads, int per_sm);
 
 }  // namespace dsmcb

@@ -1,0 +1,503 @@
+// Device code shared by the timestep's kernels: warp helpers, RNG views,
+// the NTC collision routines, boundaries and the per-particle flight.
+#pragma once
+
+#include "dsmc_kernels.cuh"
+
+namespace dsmcb {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// Adds the lanes of `mask` holding `key` to count[key] (one atomic per
+// distinct key per warp, no return value) and to the block's histogram of scan
+// tiles.
+__device__ __forceinline__ void warp_count_key(uint32_t* count, uint32_t key, unsigned mask,
+                                               uint32_t* s_tile) {
+  const unsigned peers = __match_any_sync(mask, key);
+  if ((int)lane_id() == __ffs(peers) - 1) {
+    const uint32_t cnt = __popc(peers);
+    atomicAdd(&count[key], cnt);
+    atomicAdd(&s_tile[key >> kScanShift], cnt);
+  }
+}
+
+// Ticket from a per-key counter, aggregated over the lanes of `mask` holding
+// the same key.
+__device__ __forceinline__ uint32_t warp_ticket(uint32_t* counter, uint32_t key, unsigned mask) {
+  const unsigned peers = __match_any_sync(mask, key);
+  const int leader = __ffs(peers) - 1;
+  const unsigned lane = lane_id();
+  uint32_t base = 0;
+  if ((int)lane == leader) base = atomicAdd(&counter[key], (uint32_t)__popc(peers));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void flush_tile_hist(uint32_t* s_tile, uint32_t* tile_sum, uint32_t n) {
+  for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+    const uint32_t v = s_tile[t];
+    if (v) atomicAdd(&tile_sum[t], v);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// ------------------------------------------------------------ RNG views ----
+
+struct TausRng {
+  uint4 s;
+  __device__ __forceinline__ uint32_t u32() { return hybrid_taus_int(s); }
+  __device__ __forceinline__ float f32() { return hybrid_taus_float(s); }
+};
+struct PhiloxRng {
+  PhiloxStream s;
+  __device__ __forceinline__ uint32_t u32() { return s.next(); }
+  __device__ __forceinline__ float f32() { return s.uniform(); }
+};
+
+// Stream purposes in Philox counter word 3.
+constexpr uint32_t kPurposeCollide = 0x636f6c6cu;
+constexpr uint32_t kPurposeWall = 0x77616c6cu;
+constexpr uint32_t kPurposeInit = 0x696e6974u;
+constexpr uint32_t kPurposeInject = 0x696e6a65u;
+constexpr uint32_t kPurposeHeavy = 0x68650000u;  // + lane
+
+// ------------------------------------------------------ velocity access ----
+
+struct SmemVel {
+  float* u; float* v; float* w;
+  const uint16_t* slot;
+  uint32_t off;
+  __device__ __forceinline__ float3 get(uint32_t k) const {
+    const uint32_t j = slot[off + k];
+    return make_float3(u[j], v[j], w[j]);
+  }
+  __device__ __forceinline__ void set(uint32_t k, float3 a) const {
+    const uint32_t j = slot[off + k];
+    u[j] = a.x; v[j] = a.y; w[j] = a.z;
+  }
+};
+
+struct GlobalVel {
+  float* u; float* v; float* w;
+  uint32_t off;
+  __device__ __forceinline__ float3 get(uint32_t k) const {
+    return make_float3(u[off + k], v[off + k], w[off + k]);
+  }
+  __device__ __forceinline__ void set(uint32_t k, float3 a) const {
+    u[off + k] = a.x; v[off + k] = a.y; w[off + k] = a.z;
+  }
+};
+
+// Per-cell collision state of one cell, wherever it is staged.
+struct CellState {
+  float2* maxrem;  // (sigma*g)max, remainder
+  uint4* seed;     // HybridTaus state (reference RNG mode)
+  float4* stat4;   // optional per-cell (selections, collisions, sum g)
+};
+
+// ------------------------------------------------------------- collide ----
+
+__device__ __forceinline__ float sigma_g(const StepParams& p, float mag) {
+  if (p.hard_sphere) return mag * p.cross_section;
+  return mag > 0.f ? mag * (p.cross_section * powf(p.vhs_gref / mag, p.vhs_exp)) : 0.f;
+}
+
+// NTC collisions of one cell with the reference's arithmetic:
+// ComputeBirdCollisionsNoMTDev, kernels/dsmc_kernel.cu:912-1000.  Particles of
+// the cell are acc.get(0..n-1) in sorted order; pair members are
+// start + rand % n; the pair count is evaluated in double.
+template <class Rng, class Acc>
+__device__ __forceinline__ void ntc_reference(const StepParams& p, int partCount, Acc acc, Rng& rng,
+                                              CellState cs, uint32_t& sel, uint32_t& col,
+                                              double& sum_g) {
+  float4 stat = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (cs.stat4) stat = *cs.stat4;
+  float2 vmax = *cs.maxrem;
+  const float avgConc = p.ntc_local ? (float)(partCount - 1) : p.avg_conc;
+  float fpc = (0.5 * partCount * avgConc * p.fnum * vmax.x * p.dt) / p.cell_volume + vmax.y;
+  uint32_t pairsCount = fpc;
+  stat.x += pairsCount;
+  vmax.y = fpc - pairsCount;
+  sel += pairsCount;
+  for (uint32_t i = 0; i < pairsCount; i++) {
+    uint32_t px = rng.u32() % (uint32_t)partCount;
+    float3 v1 = acc.get(px);
+    uint32_t py = rng.u32() % (uint32_t)partCount;
+    float3 v2 = acc.get(py);
+    float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
+    float v = sigma_g(p, mag);
+    if (v / vmax.x > rng.f32()) {
+      stat.y++;
+      stat.z += mag;
+      col++;
+      sum_g += mag;
+      float b = 2.0f * rng.f32() - 1.0f;
+      float a = sqrtf(1 - b * b);
+      float c = 2 * kPiF * rng.f32();
+      float3 angles = make_float3(b * mag / 2.0f, a * mag * __cosf(c) / 2.0f,
+                                  a * mag * __sinf(c) / 2.0f);
+      float3 v11, v22;
+      v11.x = (v1.x + v2.x) / 2.0f + angles.x;
+      v11.y = (v1.y + v2.y) / 2.0f + angles.y;
+      v11.z = (v1.z + v2.z) / 2.0f + angles.z;
+      acc.set(px, v11);
+      v22.x = (v1.x + v2.x) / 2.0f - angles.x;
+      v22.y = (v1.y + v2.y) / 2.0f - angles.y;
+      v22.z = (v1.z + v2.z) / 2.0f - angles.z;
+      acc.set(py, v22);
+    }
+    if (v > vmax.x) vmax.x = v;
+  }
+  *cs.maxrem = vmax;
+  if (cs.stat4) *cs.stat4 = stat;
+}
+
+// Selections of a cell in the Philox mode: FP32, with the host-folded
+// coefficient 0.5 fnum dt / V_c.
+__device__ __forceinline__ float ntc_fpc_fast(const StepParams& p, uint32_t n, float2 vm) {
+  const float avg = p.ntc_local ? (float)(n - 1) : p.avg_conc;
+  return p.ntc_coef * (float)n * avg * vm.x + vm.y;
+}
+
+// Isotropic post-collision velocities (hard sphere / VHS), accurate angles.
+__device__ __forceinline__ void scatter_pair(float3 v1, float3 v2, float mag, float r_cos,
+                                             float r_phi, float3& o1, float3& o2) {
+  const float b = 2.0f * r_cos - 1.0f;
+  const float a = sqrtf(fmaxf(0.f, 1.f - b * b));
+  float sn, cn;
+  sincospif(2.0f * r_phi, &sn, &cn);
+  const float h = 0.5f * mag;
+  const float3 ang = make_float3(b * h, a * h * cn, a * h * sn);
+  const float3 cm = make_float3(0.5f * (v1.x + v2.x), 0.5f * (v1.y + v2.y), 0.5f * (v1.z + v2.z));
+  o1 = make_float3(cm.x + ang.x, cm.y + ang.y, cm.z + ang.z);
+  o2 = make_float3(cm.x - ang.x, cm.y - ang.y, cm.z - ang.z);
+}
+
+// NTC of one cell in the Philox mode (one lane): distinct pairs, acceptance
+// sigma*g > R (sigma*g)max.
+template <class Acc>
+__device__ __forceinline__ void ntc_fast(const StepParams& p, uint32_t cell, uint32_t n, Acc acc,
+                                         uint32_t step, CellState cs, uint32_t& sel, uint32_t& col,
+                                         double& sum_g) {
+  float2 vm = *cs.maxrem;
+  const float fpc = ntc_fpc_fast(p, n, vm);
+  const uint32_t M = (uint32_t)fpc;
+  vm.y = fpc - (float)M;
+  sel += M;
+  PhiloxStream r;
+  r.init(p.seed, cell, step, kPurposeCollide);
+  uint32_t ncol = 0;
+  for (uint32_t i = 0; i < M; i++) {
+    const uint32_t pi = __umulhi(r.next(), n);
+    uint32_t pj = pi + 1u + __umulhi(r.next(), n - 1u);
+    if (pj >= n) pj -= n;
+    const float3 v1 = acc.get(pi), v2 = acc.get(pj);
+    const float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
+    const float v = sigma_g(p, mag);
+    if (v > r.uniform() * vm.x) {
+      ncol++;
+      sum_g += mag;
+      float3 o1, o2;
+      const float rc = r.uniform(), rp = r.uniform();
+      scatter_pair(v1, v2, mag, rc, rp, o1, o2);
+      acc.set(pi, o1);
+      acc.set(pj, o2);
+    }
+    if (v > vm.x) vm.x = v;
+  }
+  col += ncol;
+  *cs.maxrem = vm;
+  if (cs.stat4) {
+    float4 s = *cs.stat4;
+    s.x += M;
+    s.y += ncol;
+    *cs.stat4 = s;
+  }
+}
+
+// One cell's collisions in the configured mode (one lane).
+template <class Acc>
+__device__ __forceinline__ void collide_cell(const StepParams& p, uint32_t cell, int partCount,
+                                             Acc acc, uint32_t step, CellState cs, uint32_t& sel,
+                                             uint32_t& col, double& sum_g) {
+  if (partCount < 2) return;
+  if (p.rng_kind == 0) {
+    TausRng r;
+    r.s = *cs.seed;
+    ntc_reference(p, partCount, acc, r, cs, sel, col, sum_g);
+    *cs.seed = r.s;
+  } else {
+    ntc_fast(p, cell, (uint32_t)partCount, acc, step, cs, sel, col, sum_g);
+  }
+}
+
+// NTC selections of one dense cell by a whole warp (Philox mode).  Pairs are
+// distinct particles drawn uniformly; each round processes every pair whose
+// two particles are not claimed by a lower lane, the others retry with the
+// same pair.  Acceptance uses (sigma*g)max as of the round's start.
+__device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cell, uint32_t n,
+                                               SmemVel acc, uint32_t* claim, uint32_t step,
+                                               CellState cs, uint32_t& sel, uint32_t& col,
+                                               double& sum_g) {
+  const unsigned lane = lane_id();
+  const float2 vm = *cs.maxrem;
+  const float fpc = ntc_fpc_fast(p, n, vm);
+  const uint32_t M = (uint32_t)fpc;
+  float vmax = vm.x;
+  PhiloxStream rng;
+  rng.init(p.seed, cell, step, kPurposeHeavy + lane);
+  uint32_t drawn = 0, done = 0, pi = 0, pj = 0, ncol = 0;
+  bool pend = false;
+  while (done < M) {
+    const unsigned idle = __ballot_sync(kFull, !pend);
+    const uint32_t want = min((uint32_t)__popc(idle), M - drawn);
+    const uint32_t r = __popc(idle & ((1u << lane) - 1u));
+    if (!pend && r < want) {
+      pi = __umulhi(rng.next(), n);
+      pj = pi + 1u + __umulhi(rng.next(), n - 1u);
+      if (pj >= n) pj -= n;
+      pend = true;
+    }
+    drawn += want;
+    uint32_t ji = 0, jj = 0;
+    if (pend) {
+      ji = acc.slot[acc.off + pi];
+      jj = acc.slot[acc.off + pj];
+      atomicMin(&claim[ji], lane);
+      atomicMin(&claim[jj], lane);
+    }
+    __syncwarp();
+    const bool win = pend && claim[ji] == lane && claim[jj] == lane;
+    float vv = 0.f;
+    if (win) {
+      const float3 v1 = acc.get(pi), v2 = acc.get(pj);
+      const float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
+      vv = sigma_g(p, mag);
+      if (vv > rng.uniform() * vmax) {
+        ncol++;
+        sum_g += mag;
+        float3 o1, o2;
+        const float rc = rng.uniform(), rp = rng.uniform();
+        scatter_pair(v1, v2, mag, rc, rp, o1, o2);
+        acc.set(pi, o1);
+        acc.set(pj, o2);
+      }
+    }
+    __syncwarp();
+    if (pend) {
+      claim[ji] = 0xffffffffu;
+      claim[jj] = 0xffffffffu;
+    }
+    if (win) pend = false;
+    done += __popc(__ballot_sync(kFull, win));
+    float mx = vv;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+    vmax = fmaxf(vmax, mx);
+    __syncwarp();
+  }
+  col += ncol;
+  const uint32_t wcol = warp_sum(ncol);
+  if (lane == 0) {
+    sel += M;
+    *cs.maxrem = make_float2(vmax, fpc - (float)M);
+    if (cs.stat4) {
+      float4 s = *cs.stat4;
+      s.x += M;
+      s.y += wcol;
+      *cs.stat4 = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- move ----
+
+// The reference's four boundary functors, kernels/dsmc_kernel.cu:1316-1555,
+// with their order of face checks and their double-precision wrap.
+__device__ __forceinline__ void ref_bc(int periodic, const GridGeom& g, float3& pos, float3& vel) {
+  switch (periodic) {
+    case 'z':
+      if (pos.z > g.gmax.z) pos.z = g.gmin.z + kBounceDelta + pos.z - g.gmax.z;
+      if (pos.y > g.gmax.y) { pos.y = g.gmax.y - kBounceDelta; vel.y *= -1; }
+      if (pos.z < g.gmin.z) pos.z = g.gmax.z - kBounceDelta + pos.z - g.gmin.z;
+      if (pos.y < g.gmin.y) { pos.y = g.gmin.y + kBounceDelta; vel.y *= -1; }
+      if (pos.x < g.gmin.x) { pos.x = g.gmin.x + kBounceDelta; vel.x *= -1; }
+      if (pos.x > g.gmax.x) { pos.x = g.gmax.x - kBounceDelta; vel.x *= -1; }
+      break;
+    case 'x':
+      if (pos.x > g.gmax.x) pos.x = g.gmin.x + kBounceDelta + pos.x - g.gmax.x;
+      if (pos.y > g.gmax.y) { pos.y = g.gmax.y - kBounceDelta; vel.y *= -1; }
+      if (pos.x < g.gmin.x) pos.x = g.gmax.x - kBounceDelta + pos.x - g.gmin.x;
+      if (pos.y < g.gmin.y) { pos.y = g.gmin.y + kBounceDelta; vel.y *= -1; }
+      if (pos.z < g.gmin.z) { pos.z = g.gmin.z + kBounceDelta; vel.z *= -1; }
+      if (pos.z > g.gmax.z) { pos.z = g.gmax.z - kBounceDelta; vel.z *= -1; }
+      break;
+    case 'y':
+      if (pos.y > g.gmax.y) pos.y = g.gmin.y + kBounceDelta + pos.y - g.gmax.y;
+      if (pos.x > g.gmax.x) { pos.x = g.gmax.x - kBounceDelta; vel.x *= -1; }
+      if (pos.y < g.gmin.y) pos.y = g.gmax.y - kBounceDelta + pos.y - g.gmin.y;
+      if (pos.x < g.gmin.x) { pos.x = g.gmin.x + kBounceDelta; vel.x *= -1; }
+      if (pos.z < g.gmin.z) { pos.z = g.gmin.z + kBounceDelta; vel.z *= -1; }
+      if (pos.z > g.gmax.z) { pos.z = g.gmax.z - kBounceDelta; vel.z *= -1; }
+      break;
+    default:
+      if (pos.y > g.gmax.y) { pos.y = g.gmax.y - kBounceDelta; vel.y *= -1; }
+      if (pos.x > g.gmax.x) { pos.x = g.gmax.x - kBounceDelta; vel.x *= -1; }
+      if (pos.y < g.gmin.y) { pos.y = g.gmin.y + kBounceDelta; vel.y *= -1; }
+      if (pos.x < g.gmin.x) { pos.x = g.gmin.x + kBounceDelta; vel.x *= -1; }
+      if (pos.z < g.gmin.z) { pos.z = g.gmin.z + kBounceDelta; vel.z *= -1; }
+      if (pos.z > g.gmax.z) { pos.z = g.gmax.z - kBounceDelta; vel.z *= -1; }
+      break;
+  }
+}
+
+// One domain face (extension): specular and diffuse walls with the exact
+// crossing point, outflow (particle removed), periodic wrap.  Returns false
+// when the particle left the domain.
+__device__ __forceinline__ bool face_axis(const StepParams& p, float& x, float& vx, float lo,
+                                          float hi, int face_lo, float3& pos, float3& vel,
+                                          int axis, PhiloxStream& rng) {
+  int face = -1;
+  float bound = 0.f;
+  if (x < lo) { face = face_lo; bound = lo; }
+  else if (x > hi) { face = face_lo + 1; bound = hi; }
+  if (face < 0) return true;
+  const int kind = p.face_kind[face];
+  if (kind == 2 || kind == 4) return false;  // outflow / inflow face: leaves
+  if (kind == 3) {
+    x = (face & 1) ? x - (hi - lo) : x + (hi - lo);
+    return true;
+  }
+  if (kind == 0) {
+    x = 2.f * bound - x;
+    vx = -vx;
+    return true;
+  }
+  // diffuse wall: back to the crossing point, re-emit, fly the rest
+  const float tau = vx != 0.f ? (x - bound) / vx : 0.f;
+  pos.x -= vel.x * tau; pos.y -= vel.y * tau; pos.z -= vel.z * tau;
+  float3 n_in = make_float3(0.f, 0.f, 0.f);
+  const float s = (face & 1) ? -1.f : 1.f;
+  if (axis == 0) { pos.x = bound; n_in.x = s; }
+  else if (axis == 1) { pos.y = bound; n_in.y = s; }
+  else { pos.z = bound; n_in.z = s; }
+  vel = diffuse_emit(n_in, p.face_vstd[face], rng);
+  pos.x += vel.x * tau; pos.y += vel.y * tau; pos.z += vel.z * tau;
+  return true;
+}
+
+__device__ __forceinline__ bool face_bc(const StepParams& p, float3& pos, float3& vel,
+                                        PhiloxStream& rng) {
+  const GridGeom& g = p.grid;
+  if (!face_axis(p, pos.x, vel.x, g.gmin.x, g.gmax.x, 0, pos, vel, 0, rng)) return false;
+  if (!face_axis(p, pos.y, vel.y, g.gmin.y, g.gmax.y, 2, pos, vel, 1, rng)) return false;
+  if (!face_axis(p, pos.z, vel.z, g.gmin.z, g.gmax.z, 4, pos, vel, 2, rng)) return false;
+  // a re-emitted particle that crossed another face in the rest of its
+  // flight is kept inside
+  pos.x = fminf(fmaxf(pos.x, g.gmin.x), g.gmax.x);
+  pos.y = fminf(fmaxf(pos.y, g.gmin.y), g.gmax.y);
+  pos.z = fminf(fmaxf(pos.z, g.gmin.z), g.gmax.z);
+  return true;
+}
+
+// One particle's flight: IntegrateDev / ProcessCollisionsDev,
+// kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.
+__device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, float3& vel,
+                                              uint32_t gidx, uint32_t step) {
+  float3 old_pos = pos;
+  pos.x = old_pos.x + vel.x * p.dt;
+  pos.y = old_pos.y + vel.y * p.dt;
+  pos.z = old_pos.z + vel.z * p.dt;
+  PhiloxStream rng;
+  rng.init(p.seed, gidx, step, kPurposeWall);
+  if (p.has_geom && p.geom.nearest) {
+    // nearest wall crossing along the path, repeated for the rest of the
+    // flight after each re-emission (extension for bodies with diffuse walls)
+    const GeomView& G = p.geom;
+    for (uint32_t b = 0; b < kCollisionLimit; b++) {
+      const float3 seg = make_float3(pos.x - old_pos.x, pos.y - old_pos.y, pos.z - old_pos.z);
+      const float dist = length3(seg);
+      if (!(dist > 1e-12f)) break;
+      // a path shorter than the start cell's clearance cannot reach the body
+      const uint32_t sc = coll_cell_id(G.grid, old_pos);
+      if (sc != kNone && dist < __ldg(&G.clear[sc])) break;
+      const float3 d = make_float3(seg.x / dist, seg.y / dist, seg.z / dist);
+      float t;
+      uint32_t e;
+      if (!nearest_wall_hit(G, old_pos, d, dist, &t, &e)) break;
+      const float4 P = __ldg(&G.tri[kTriStride * (size_t)e + 3]);
+      const float3 n = make_float3(P.x, P.y, P.z);
+      const float side = (d.x * n.x + d.y * n.y + d.z * n.z) > 0.f ? -1.f : 1.f;
+      const float3 n_out = make_float3(side * n.x, side * n.y, side * n.z);
+      const float3 hp = make_float3(old_pos.x + d.x * t + n_out.x * 1e-6f,
+                                    old_pos.y + d.y * t + n_out.y * 1e-6f,
+                                    old_pos.z + d.z * t + n_out.z * 1e-6f);
+      const float rest = dist - t;
+      if (G.diffuse) {
+        const float speed = length3(vel);
+        vel = diffuse_emit(n_out, G.wall_vstd, rng);
+        const float tau = speed > 0.f ? rest / speed : 0.f;
+        pos = make_float3(hp.x + vel.x * tau, hp.y + vel.y * tau, hp.z + vel.z * tau);
+      } else {
+        vel = reflect3(vel, n);
+        const float3 r = normalize3(vel);
+        pos = make_float3(hp.x + r.x * rest, hp.y + r.y * rest, hp.z + r.z * rest);
+      }
+      old_pos = hp;
+    }
+  } else if (p.has_geom) {
+    const GeomView& G = p.geom;
+    uint32_t st_cubid = kNone, end_cubid = kNone;
+    bool collProcessed = false;
+    uint32_t i = 0;
+    do {
+      st_cubid = coll_cell_id(G.grid, old_pos);
+      end_cubid = coll_cell_id(G.grid, pos);
+      if (st_cubid != kNone) {
+        if (__ldg(&G.flags[st_cubid]) != 0)
+          collProcessed = collide_with_geometry(G, &pos, &vel, &old_pos, st_cubid, &rng);
+      }
+      if (!collProcessed && st_cubid != end_cubid && end_cubid != kNone) {
+        if (__ldg(&G.flags[end_cubid]) != 0)
+          collProcessed = collide_with_geometry(G, &pos, &vel, &old_pos, end_cubid, &rng);
+      }
+    } while (collProcessed && i++ < kCollisionLimit);
+  }
+  if (p.face_mode == 0) {
+    ref_bc(p.periodic, p.grid, pos, vel);
+    return true;
+  }
+  return face_bc(p, pos, vel, rng);
+}
+
+// Sampling of one cell from sorted velocities (SampleCellStatisticsDev,
+// kernels/dsmc_kernel.cu:856-890) into the FP64 accumulators (SoA, 5 fields).
+template <class Acc>
+__device__ __forceinline__ void sample_cell(double* acc, uint32_t cells, uint32_t cell, int n,
+                                            const Acc& a) {
+  if (n <= 0) return;
+  double su = 0, sv = 0, sw = 0, se = 0;
+  for (int k = 0; k < n; k++) {
+    const float3 q = a.get(k);
+    const double x = q.x, y = q.y, z = q.z;
+    su += x; sv += y; sw += z;
+    se += x * x + y * y + z * z;
+  }
+  acc[cell] += (double)n;
+  acc[(size_t)cells + cell] += su;
+  acc[2 * (size_t)cells + cell] += sv;
+  acc[3 * (size_t)cells + cell] += sw;
+  acc[4 * (size_t)cells + cell] += se;
+}
+
+}  // namespace dev
+}  // namespace dsmcb

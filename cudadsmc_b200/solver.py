@@ -120,6 +120,26 @@ class DSMCSolver:
     def StepGraph(self, dt, nsteps=1):
         self._check(lib().dsmc_step_graph(self.h, dt, nsteps), "StepGraph")
 
+    def SetKernelVariant(self, variant):
+        self._check(lib().dsmc_set_kernel_variant(self.h, int(variant)), "SetKernelVariant")
+
+    def KernelVariant(self):
+        """(variant, particles per shared-memory chunk) of the cell kernel."""
+        v, cap = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().dsmc_get_kernel_variant(self.h, ctypes.byref(v), ctypes.byref(cap)),
+                    "KernelVariant")
+        return v.value, cap.value
+
+    def Autotune(self, dt, steps=10):
+        """Times every cell-kernel variant on real timesteps (the run advances
+        by 4 * (steps + 2) steps) and keeps the fastest; returns (best, ms per
+        step of each variant)."""
+        best = ctypes.c_int(0)
+        ms = np.zeros(4, np.float32)
+        self._check(lib().dsmc_autotune(self.h, dt, int(steps), ctypes.byref(best), _ptr(ms)),
+                    "Autotune")
+        return best.value, [float(x) for x in ms]
+
     def Sync(self):
         self._check(lib().dsmc_sync(self.h), "Sync")
 

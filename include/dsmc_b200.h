@@ -216,6 +216,21 @@ int dsmc_step(dsmc_handle* h, float dt, int nsteps);
 /* Same as dsmc_step but replays a captured CUDA graph of the step. */
 int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps);
 
+/* Launch shape of the step's cell kernel (no counterpart in the reference,
+ * whose kernels use fixed block sizes): variant 0 = 512 threads per CTA and
+ * up to 2048 particles per shared-memory chunk, 1 = 256/1024, 2 = 128/512
+ * (default), 3 = 64/256.  Results do not depend on the variant, except in
+ * the Philox mode for a cell holding more particles than the chunk (it is
+ * then collided by one thread instead of one warp, a different but
+ * equivalent stream of draws).  Changing it drops the captured graph. */
+int dsmc_set_kernel_variant(dsmc_handle* h, int variant);
+int dsmc_get_kernel_variant(dsmc_handle* h, int* variant, int* chunk_capacity);
+/* Times `steps` graph-replayed timesteps (after 2 warm-up steps) of every
+ * variant and keeps the fastest.  These are real timesteps of the run: the
+ * simulation advances by 4 * (steps + 2) steps.  ms_per_step (optional)
+ * receives 4 times in milliseconds.  Blocks until done. */
+int dsmc_autotune(dsmc_handle* h, float dt, int steps, int* best, float* ms_per_step);
+
 /* SampleCellStatistics (kernels/dsmc_kernel.cu:892-910): adds the current
  * velocities to the FP64 per-cell accumulators now. */
 int dsmc_sample(dsmc_handle* h);

@@ -180,13 +180,15 @@ def main(out):
     mr_o = np.zeros_like(mr)
     sd_o = np.zeros_like(seeds)
     st4 = np.zeros((128, 4), np.float32)
-    cs7 = np.zeros((128, 7), np.float32)
-    R.ref_get_cell_state(O.p(mr_o), O.p(sd_o), O.p(st4), O.p(cs7))
+    # statistics_t (include/statistics.h:31-37) is 32 bytes: numInSample,
+    # xyzSum, velMag, 4 bytes of alignment padding, the float2 padd
+    cs8 = np.zeros((128, 8), np.float32)
+    R.ref_get_cell_state(O.p(mr_o), O.p(sd_o), O.p(st4), O.p(cs8))
     np.savez_compressed(os.path.join(out, "step3.npz"), gmin=gmin, gmax=gmax, dim=dim, dt=1e-5,
                         ppc=d["ppc"], fnum=1e16, cross_section=d["cross_section"],
                         cell_volume=d["cell_volume"], max_rel_vel=d["max_rel_vel"], pos=pos, vel=vel,
                         maxrem=mr, seeds=seeds, pos_out=pc.cpu().numpy(), vel_out=vc.cpu().numpy(),
-                        maxrem_out=mr_o, seeds_out=sd_o, stat4=st4, cell_stats=cs7,
+                        maxrem_out=mr_o, seeds_out=sd_o, stat4=st4, cell_stats=cs8[:, :5].copy(),
                         cse=cs.cpu().numpy().view(np.uint32).reshape(-1, 2))
     print("golden fixtures written to", out)
 

@@ -162,3 +162,32 @@ def test_steps_vs_reference_kernels(cuda, periodic, steps):
         # a single accept decision decided differently by rounding changes
         # its cell's later history; the bulk stays identical
         assert exact_part > 0.99
+
+
+@pytest.mark.parametrize("rng,density", [("taus", 1e20), ("philox", 1e20), ("philox", 6e20)])
+def test_kernel_variants_give_identical_steps(cuda, rng, density):
+    """Every launch shape of the cell kernel computes the same step (no cell
+    here exceeds the smallest chunk); the autotuner keeps one of them."""
+    out = []
+    for v in range(4):
+        s = make_settings(density=density, rng=rng, init_kind="maxwell", seed=5).set(sample_every=3)
+        solver = DSMCSolver().Init(s)
+        solver.SetKernelVariant(v)
+        assert solver.KernelVariant()[0] == v
+        solver.InitSystemState()
+        solver.RunSimulationStep(1e-5, 4)
+        solver.StepGraph(1e-5, 3)
+        solver.Sync()
+        out.append((solver.DownloadState(), solver.GetCellState(), solver.Fields(),
+                    solver.Info().giant_cells))
+        if v == 3:
+            best, ms = solver.Autotune(1e-5, steps=2)
+            assert 0 <= best < 4 and all(m > 0 for m in ms)
+            assert solver.KernelVariant()[0] == best
+        solver.close()
+    for v in range(1, 4):
+        assert out[v][3] == 0
+        assert np.array_equal(out[0][0], out[v][0])
+        assert np.array_equal(out[0][1][0], out[v][1][0])
+        assert np.array_equal(out[0][1][1], out[v][1][1])
+        assert np.array_equal(out[0][2], out[v][2], equal_nan=True)
