@@ -127,6 +127,7 @@ SIGNATURES = [
     ("dsmc_stage_cell_index", _I, [ctypes.POINTER(Grid), _P, _P, _P, _U32, _P, _P, _P]),
     ("dsmc_stage_sort_workspace", _I, [_U32, _U32, ctypes.POINTER(ctypes.c_size_t)]),
     ("dsmc_stage_sort", _I, [_P, _P, _U32, _U32, _P, _P, ctypes.c_size_t, _P]),
+    ("dsmc_stage_sort_static", _I, [_P, _P, _U32, _U32, _P, _P]),
     ("dsmc_stage_bounds_reorder", _I, [_P, _P, _U32, _U32, _P, _P, _P, _P]),
     ("dsmc_stage_collide", _I, [ctypes.POINTER(CollideParams), _P, _P, _P, _P, _P, _P, _P, _P]),
     ("dsmc_stage_move", _I, [_P, ctypes.POINTER(MoveParams), _P, _P, _P, _P, _P, _P, _U32, _P]),

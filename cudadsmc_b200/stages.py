@@ -55,6 +55,18 @@ def sort(keys, vals, nkeys, cell_start=None, workspace=None):
                                 _p(workspace), wb, _stream()), "stage_sort")
 
 
+def sort_static(keys, vals, nkeys, cell_start=None):
+    """The stable sort of sort() with the library's static scratch: allocates
+    nothing; n <= SORT_STATIC_MAX_N, nkeys <= SORT_STATIC_MAX_KEYS.  Calls that
+    may overlap on one device race on the shared scratch."""
+    check(lib().dsmc_stage_sort_static(_p(keys), _p(vals), keys.numel(), nkeys, _p(cell_start),
+                                       _stream()), "stage_sort_static")
+
+
+SORT_STATIC_MAX_N = 1048576
+SORT_STATIC_MAX_KEYS = 131072
+
+
 def bounds_reorder(keys, idx, ncells, cse, src=None, dst=None):
     """FindCellBoundaries (kernels/dsmc_kernel.cu:1734-1808).  cse: uint2 per
     cell as an int32 tensor of 2*ncells; src/dst: six float tensors each."""

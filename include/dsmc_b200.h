@@ -279,6 +279,26 @@ int dsmc_stage_sort_workspace(uint32_t n, uint32_t nkeys, size_t* bytes);
 int dsmc_stage_sort(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t nkeys,
                     uint32_t* cell_start, void* workspace, size_t workspace_bytes, void* stream);
 
+/* dsmc_stage_sort without any allocation (no counterpart in the reference):
+ * for callers that may not allocate device memory while they run, such as
+ * code recording work into a memory-constrained pool or running next to a
+ * caching allocator that owns the device.  The scratch is a fixed static
+ * device array of about 13.6 MB, reserved on each device when the library's
+ * kernels are loaded there; this call never calls cudaMalloc, cudaFree or an
+ * allocating library function.
+ * Limits: n <= DSMC_SORT_STATIC_MAX_N and nkeys <= DSMC_SORT_STATIC_MAX_KEYS;
+ * larger sizes return DSMC_ERR_CAPACITY before any device work.
+ * The scratch address is looked up once per device on the first call there;
+ * make that first call outside any stream capture.  Every call zeroes the
+ * scratch counters it needs on `stream` itself, so nothing has to be cleared
+ * beforehand.  All calls on one device share the scratch: calls that may
+ * overlap (different streams or host threads without ordering between them)
+ * race and corrupt each other's results; order them on one stream. */
+#define DSMC_SORT_STATIC_MAX_N 1048576u
+#define DSMC_SORT_STATIC_MAX_KEYS 131072u
+int dsmc_stage_sort_static(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t nkeys,
+                           uint32_t* cell_start, void* stream);
+
 /* FindCellBoundaries (kernels/dsmc_kernel.cu:1734-1808): cell start/end
  * (uint2 per cell, (0,0) for empty cells) from sorted keys, and the gather of
  * the six state arrays into sorted order (src -> dst). */
