@@ -264,8 +264,10 @@ def run_ours(args, rank, world):
     sol.SetStream(torch.cuda.current_stream().cuda_stream)
     n0 = sol.InitSystemState()
     dt = wl["settings"]["dt"]
-    # warm-up (also develops the flow a little)
+    # warm-up (also develops the flow a little), then the launch-shape
+    # autotuner of the cell kernel on real steps of the run
     sol.RunSimulationStep(dt, args.warmup)
+    variant, tune_ms = sol.Autotune(dt, steps=args.tune_steps)
     sol.Sync()
     info0 = sol.Info()
     if world > 1:
@@ -315,7 +317,7 @@ def run_ours(args, rank, world):
     # whole-step roofline at 128 B per particle-timestep (algorithmic)
     step_frac = value / max(world, 1) * 128 / (peak * 1e9)
     # end-to-end through the C ABI with host buffers
-    e2e = run_e2e(args, wl, rank, world, dev)
+    e2e = run_e2e(args, wl, rank, world, dev, variant)
     out = {
         "metric": "particle-timesteps/s", "value": value, "unit": "particle-timesteps/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -325,7 +327,8 @@ def run_ours(args, rank, world):
                    "particles_avg_timed": n_avg, "cells": sol.Info().cells, "dt": dt,
                    "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
                    "l2_policy": "working set (2 x 24 B x N state + 12 B x N keys) > 126 MB L2",
-                   "rng": wl["settings"].get("rng")},
+                   "rng": wl["settings"].get("rng"),
+                   "cell_kernel_variant": {"chosen": variant, "autotune_ms_per_step": tune_ms}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg, "ms_per_launch": dom_ms,
@@ -343,13 +346,14 @@ def run_ours(args, rank, world):
     return out
 
 
-def run_e2e(args, wl, rank, world, dev):
+def run_e2e(args, wl, rank, world, dev, variant):
     """The same metric through the C ABI with host buffers: per run the
     pinned initial state is uploaded (h2d), then every step is one dsmc_step
     call followed by a device->host read of that step's collision totals, and
     the sampled fields are read back at the end (d2h)."""
     import torch
     sol = build_solver(wl, seed_offset=rank)
+    sol.SetKernelVariant(variant)
     n0 = sol.InitSystemState()
     state = sol.DownloadState()  # the initial state, as a host would provide it
     host = torch.from_numpy(state).pin_memory()
@@ -407,6 +411,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--tune-steps", type=int, default=10)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

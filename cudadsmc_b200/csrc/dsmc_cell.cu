@@ -34,6 +34,21 @@ struct Chunk {
   int buf;    // staging buffer
   int giant;  // one cell above the chunk capacity
   int valid;
+  uint32_t ntile;  // the tile the CTA processes after this chunk's tile
+};
+
+// Hands out the CTA's tiles after its first (blockIdx.x): from the step's
+// dynamic tile counter (tiles past the first wave go to whichever CTA asks
+// first), or round robin when the launch has no counter.  Used by thread 0,
+// which asks one tile ahead of need so that the atomic's latency is hidden.
+struct TileSource {
+  uint32_t next_static;
+  __device__ __forceinline__ uint32_t grab(const StepParams& p) {
+    if (p.meta) return gridDim.x + atomicAdd(&p.meta->tile_next, 1u);
+    const uint32_t t = next_static;
+    next_static += gridDim.x;
+    return t;
+  }
 };
 
 // Shared memory of one CTA; the scan-tile histogram (n_scan_tiles words)
@@ -43,15 +58,17 @@ struct __align__(128) CellSmem {
   float part[2][7][CAP + 4];
   float2 maxrem[2][kCellArr];
   uint4 seeds[2][kMaxCellsPerTile];
-  uint32_t ls[2][kLsArr];
+  uint32_t ls[3][kLsArr];        // starts of the current, next and following tile
   unsigned long long mbar[2];     // chunk data of buffer b
-  unsigned long long mbar_ls[2];  // starts of ls buffer b
+  unsigned long long mbar_ls[3];  // starts of ls buffer b
   Chunk cur, next;
   uint32_t nheavy;
+  uint32_t nhard;
   uint32_t claim[CAP + 4];
   uint32_t cellm[kMaxCellsPerTile];
   uint16_t heavy[kMaxCellsPerTile];
   uint16_t slot[CAP];
+  uint16_t hardq[CAP];  // staged particles whose flight may meet the body
   uint8_t cellof[CAP];
 };
 
@@ -366,11 +383,14 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
   for (uint32_t t = tid; t < (uint32_t)(CAP + 4); t += blockDim.x) S.claim[t] = 0xffffffffu;
   // mbarrier phase bits: bit b for chunk buffer b, bit 2+b for ls buffer b
   uint32_t phase = 0u;
+  TileSource tiles{blockIdx.x + gridDim.x};
+  uint32_t pending = 0;  // thread 0: the tile after the next one
   if (tid == 0) {
     mbar_init(&S.mbar[0], 1);
     mbar_init(&S.mbar[1], 1);
     mbar_init(&S.mbar_ls[0], 1);
     mbar_init(&S.mbar_ls[1], 1);
+    mbar_init(&S.mbar_ls[2], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     S.cur.valid = 0;
     if (blockIdx.x < p.n_tiles) issue_ls(p, S, blockIdx.x, 0);
@@ -391,6 +411,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
     if (tid == 0) {
       finish_ls(p, S, blockIdx.x, 0);
       S.cur = make_chunk(S, blockIdx.x, 0, 0, ct, p.cells, 0);
+      S.cur.ntile = tiles.grab(p);
+      pending = tiles.grab(p);
+      if (S.cur.ntile < p.n_tiles) issue_ls(p, S, S.cur.ntile, 1);
     }
     __syncwarp();
     if (chunk_has_data(S.cur)) issue_chunk(p, S, S.cur);
@@ -399,10 +422,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
 
   while (S.cur.valid) {
     const Chunk c = S.cur;
-    // the CTA's next tile: its starts are fetched while this tile runs
-    const uint32_t nt = c.tile + gridDim.x;
-    if (c.cur == 0 && tid == 0 && nt < p.n_tiles) issue_ls(p, S, nt, 1 - c.lsb);
-    if (tid == 0) S.nheavy = 0;
+    // the CTA's next tile; its starts were fetched into ls buffer nb when
+    // this tile's first chunk was made
+    const uint32_t nt = c.ntile;
+    const int nb = c.lsb == 2 ? 0 : c.lsb + 1;
+    const uint32_t phase0 = phase;
+    if (tid == 0) {
+      S.nheavy = 0;
+      S.nhard = 0;
+    }
     if (chunk_has_data(c)) {
       ok = mbar_wait_bounded(&S.mbar[c.buf], (phase >> c.buf) & 1u);
       phase ^= 1u << c.buf;
@@ -410,16 +438,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
     // the next chunk; it may lie in the next tile, whose starts must be in
     const bool last_of_tile = c.cur + c.k >= c.nct;
     if (last_of_tile && nt < p.n_tiles) {
-      ok = ok && mbar_wait_bounded(&S.mbar_ls[1 - c.lsb], (phase >> (3 - c.lsb)) & 1u);
-      phase ^= 1u << (3 - c.lsb);
+      ok = ok && mbar_wait_bounded(&S.mbar_ls[nb], (phase >> (2 + nb)) & 1u);
+      phase ^= 1u << (2 + nb);
     }
     if (!__syncthreads_and(ok)) {
       if (tid == 0 && p.meta) atomicOr(&p.meta->error, kErrTimeout);
-      // let copies still in flight land before the CTA's shared memory goes
-      // away (each wait bounded; a buffer with nothing in flight times out)
-      mbar_wait_bounded(&S.mbar[0], phase & 1u);
-      mbar_wait_bounded(&S.mbar[1], (phase >> 1) & 1u);
-      mbar_wait_bounded(&S.mbar_ls[1 - c.lsb], (phase >> (3 - c.lsb)) & 1u);
+      // let the copies that may still be in flight (this chunk's data, the
+      // next tile's starts) land before the CTA's shared memory goes away
+      if (chunk_has_data(c)) mbar_wait_bounded(&S.mbar[c.buf], (phase0 >> c.buf) & 1u);
+      if (nt < p.n_tiles) mbar_wait_bounded(&S.mbar_ls[nb], (phase0 >> (2 + nb)) & 1u);
       return;
     }
     if (warp == 0) {
@@ -428,9 +455,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
         nx.valid = 0;
         if (!last_of_tile) {
           nx = make_chunk(S, c.tile, c.lsb, c.cur + c.k, ct, p.cells, 1 - c.buf);
+          nx.ntile = nt;
         } else if (nt < p.n_tiles) {
-          finish_ls(p, S, nt, 1 - c.lsb);
-          nx = make_chunk(S, nt, 1 - c.lsb, 0, ct, p.cells, 1 - c.buf);
+          finish_ls(p, S, nt, nb);
+          nx = make_chunk(S, nt, nb, 0, ct, p.cells, 1 - c.buf);
+          nx.ntile = pending;
+          pending = tiles.grab(p);
+          // the following tile's starts go into the buffer this tile's
+          // predecessor used
+          if (nx.ntile < p.n_tiles) issue_ls(p, S, nx.ntile, nb == 2 ? 0 : nb + 1);
         }
         S.next = nx;
       }
@@ -515,34 +548,58 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
           if (taus) p.seeds[cs + lc] = SD[lc];
         }
       }
-      // C: flight, next-step keys, stores in sorted order
-      for (uint32_t qb = 0; qb < n; qb += blockDim.x) {
-        const uint32_t q = qb + tid;
-        const bool active = q < n;
-        float3 pos = make_float3(0.f, 0.f, 0.f), vel = pos;
-        bool live = true;
-        const uint32_t g = base + q;
-        if (active) {
-          const uint32_t j = S.slot[q];
-          if (!vel_only) pos = make_float3(X[j], Y[j], Z[j]);
-          vel = make_float3(U[j], V[j], W[j]);
-          if (p.flags & kDoMove) live = move_particle(p, pos, vel, g, step);
-          if (do_sample) { U[j] = vel.x; V[j] = vel.y; W[j] = vel.z; }
-          if (!vel_only) { p.out.x[g] = pos.x; p.out.y[g] = pos.y; p.out.z[g] = pos.z; }
-          p.out.u[g] = vel.x; p.out.v[g] = vel.y; p.out.w[g] = vel.z;
-        }
-        if (do_keys) {
-          const bool has_key = active && live;
-          const unsigned m = __ballot_sync(kFull, has_key);
-          if (active && !live) removed++;
-          if (has_key) {
-            const uint32_t key = cell_id3d(p.grid, pos.x, pos.y, pos.z);
-            warp_count_key(p.count, key, m, s_tile);
-            p.out_key[g] = key;
-          } else if (active) {
-            p.out_key[g] = kDeadKey;
+      // C: flight, next-step keys, stores in sorted order.  With a body,
+      // particles whose path may reach it are queued in the first pass and
+      // flown in a second pass by whole warps, so that the mesh traversal of
+      // a few lanes does not hold up the cheap flights of the rest.
+      const bool split = p.has_geom && (p.flags & kDoMove);
+      const uint32_t lane = lane_id();
+      for (uint32_t pass = 0; pass < (split ? 2u : 1u); pass++) {
+        const uint32_t cnt = pass == 0 ? n : S.nhard;
+        for (uint32_t qb = 0; qb < cnt; qb += blockDim.x) {
+          const uint32_t i = qb + tid;
+          const bool active = i < cnt;
+          float3 pos = make_float3(0.f, 0.f, 0.f), vel = pos;
+          uint32_t q = 0, j = 0;
+          bool defer = false;
+          if (active) {
+            q = pass == 0 ? i : (uint32_t)S.hardq[i];
+            j = S.slot[q];
+            if (!vel_only) pos = make_float3(X[j], Y[j], Z[j]);
+            vel = make_float3(U[j], V[j], W[j]);
+            if (pass == 0 && split) defer = flight_may_meet_body(p, pos, vel);
+          }
+          const unsigned dm = __ballot_sync(kFull, defer);
+          if (dm) {
+            const int leader = __ffs(dm) - 1;
+            uint32_t at = 0;
+            if ((int)lane == leader) at = atomicAdd(&S.nhard, (uint32_t)__popc(dm));
+            at = __shfl_sync(kFull, at, leader);
+            if (defer) S.hardq[at + __popc(dm & ((1u << lane) - 1u))] = (uint16_t)q;
+          }
+          const bool go = active && !defer;
+          const uint32_t g = base + q;
+          bool live = true;
+          if (go) {
+            if (p.flags & kDoMove) live = move_particle(p, pos, vel, g, step);
+            if (do_sample) { U[j] = vel.x; V[j] = vel.y; W[j] = vel.z; }
+            if (!vel_only) { p.out.x[g] = pos.x; p.out.y[g] = pos.y; p.out.z[g] = pos.z; }
+            p.out.u[g] = vel.x; p.out.v[g] = vel.y; p.out.w[g] = vel.z;
+          }
+          if (do_keys) {
+            const bool has_key = go && live;
+            const unsigned m = __ballot_sync(kFull, has_key);
+            if (go && !live) removed++;
+            if (has_key) {
+              const uint32_t key = cell_id3d(p.grid, pos.x, pos.y, pos.z);
+              warp_count_key(p.count, key, m, s_tile);
+              p.out_key[g] = key;
+            } else if (go) {
+              p.out_key[g] = kDeadKey;
+            }
           }
         }
+        if (split && pass == 0) __syncthreads();  // the queue is complete
       }
       // D: sampling
       if (do_sample) {

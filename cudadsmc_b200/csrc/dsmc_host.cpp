@@ -468,8 +468,11 @@ void mesh_icosphere(int level, float radius, const float* center, std::vector<fl
 
 // Sphere-cone capsule around the +x axis: spherical nose of radius rn facing
 // -x, a cone of half-angle theta tangent to it, a flat base closing the body
-// at total length `length` from the nose tip.  Profile and azimuth counts are
-// chosen for about ntarget triangles; the seed rotates the azimuthal start.
+// at total length `length` from the nose tip.  Rings along the profile are
+// about one edge length h apart and each ring has about 2 pi r / h vertices,
+// so the triangles are near-equilateral of similar size everywhere (no fan of
+// slivers at the nose tip or the base centre); h is chosen for about
+// ntarget triangles.  The seed rotates the azimuthal start of the rings.
 void mesh_capsule(float rn, float theta_deg, float length, const float* c, uint32_t ntarget,
                   uint64_t seed, std::vector<float>& verts, std::vector<uint32_t>& tris) {
   const double th = theta_deg * M_PI / 180.0;
@@ -478,35 +481,36 @@ void mesh_capsule(float rn, float theta_deg, float length, const float* c, uint3
   const double x_t = c[0] - rn * std::cos(phi_t), r_t = rn * std::sin(phi_t);
   const double x_base = x_tip + length;
   const double r_base = r_t + (x_base - x_t) * std::tan(th);
-  // azimuth segments and profile rings: 2*naz triangles per ring band
-  uint32_t naz = 64;
-  while (2ull * naz * (naz / 2) < ntarget && naz < 4096) naz += 8;
-  uint32_t nprof = ntarget / (2 * naz);
-  if (nprof < 6) nprof = 6;
-  uint32_t n_nose = std::max<uint32_t>(3, (uint32_t)(nprof * 0.45));
-  uint32_t n_cone = std::max<uint32_t>(2, (uint32_t)(nprof * 0.40));
-  uint32_t n_base = std::max<uint32_t>(1, nprof - n_nose - n_cone);
+  const double L1 = rn * phi_t;
+  const double L2 = std::hypot(x_base - x_t, r_base - r_t);
+  const double L3 = r_base;
+  const double area = 2 * M_PI * rn * rn * (1 - std::cos(phi_t)) + M_PI * (r_t + r_base) * L2 +
+                      M_PI * r_base * r_base;
+  const double h = std::sqrt(4.0 * area / (std::sqrt(3.0) * std::max<uint32_t>(ntarget, 64)));
+  const double ds = h * std::sqrt(3.0) / 2;  // ring spacing along the profile
+  const uint32_t n1 = std::max<uint32_t>(2, (uint32_t)std::lround(L1 / ds));
+  const uint32_t n2 = std::max<uint32_t>(1, (uint32_t)std::lround(L2 / ds));
+  const uint32_t n3 = std::max<uint32_t>(2, (uint32_t)std::lround(L3 / ds));
   // splitmix64 of the seed -> azimuthal phase
   uint64_t z = seed + 0x9E3779B97F4A7C15ull;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   z ^= z >> 31;
-  const double phase = (double)(z >> 11) / 9007199254740992.0 * (2 * M_PI / naz);
+  const double phase = (double)(z >> 11) / 9007199254740992.0 * 2 * M_PI;
   std::vector<double> rx, rr;  // profile rings (x, radius), excluding the two poles
-  for (uint32_t i = 1; i <= n_nose; i++) {
-    double ph = phi_t * i / n_nose;
+  for (uint32_t i = 1; i <= n1; i++) {
+    const double ph = phi_t * i / n1;
     rx.push_back(c[0] - rn * std::cos(ph));
     rr.push_back(rn * std::sin(ph));
   }
-  for (uint32_t i = 1; i <= n_cone; i++) {
-    double x = x_t + (x_base - x_t) * i / n_cone;
+  for (uint32_t i = 1; i <= n2; i++) {
+    const double x = x_t + (x_base - x_t) * i / n2;
     rx.push_back(x);
     rr.push_back(r_t + (x - x_t) * std::tan(th));
   }
-  for (uint32_t i = 1; i < n_base + 1; i++) {
-    double r = r_base * (1.0 - (double)i / (n_base + 1));
+  for (uint32_t i = 1; i < n3; i++) {
     rx.push_back(x_base);
-    rr.push_back(r);
+    rr.push_back(r_base * (1.0 - (double)i / n3));
   }
   verts.clear();
   tris.clear();
@@ -514,29 +518,41 @@ void mesh_capsule(float rn, float theta_deg, float length, const float* c, uint3
     verts.push_back((float)x); verts.push_back((float)y); verts.push_back((float)zz);
     return (uint32_t)(verts.size() / 3 - 1);
   };
-  uint32_t tip = push(x_tip, c[1], c[2]);
-  std::vector<uint32_t> ring0;
+  const uint32_t tip = push(x_tip, c[1], c[2]);
+  std::vector<uint32_t> first(rx.size()), count(rx.size());
   for (size_t k = 0; k < rx.size(); k++) {
-    for (uint32_t a = 0; a < naz; a++) {
-      double ang = phase + 2 * M_PI * a / naz;
+    const uint32_t m = std::max<uint32_t>(3, (uint32_t)std::lround(2 * M_PI * rr[k] / h));
+    first[k] = (uint32_t)(verts.size() / 3);
+    count[k] = m;
+    for (uint32_t a = 0; a < m; a++) {
+      const double ang = phase + 2 * M_PI * a / m;
       push(rx[k], c[1] + rr[k] * std::cos(ang), c[2] + rr[k] * std::sin(ang));
     }
   }
-  uint32_t tail = push(x_base, c[1], c[2]);
-  auto rid = [&](size_t k, uint32_t a) { return (uint32_t)(1 + k * naz + (a % naz)); };
+  const uint32_t tail = push(x_base, c[1], c[2]);
+  auto rid = [&](size_t k, uint32_t a) { return first[k] + a % count[k]; };
   // outward winding: looking from outside, counter-clockwise
-  for (uint32_t a = 0; a < naz; a++) {
+  for (uint32_t a = 0; a < count[0]; a++) {
     tris.push_back(tip); tris.push_back(rid(0, a + 1)); tris.push_back(rid(0, a));
   }
+  // band between ring k and k+1: advance along whichever ring's next vertex
+  // comes first in angle (all rings start at the same phase)
   for (size_t k = 0; k + 1 < rx.size(); k++) {
-    for (uint32_t a = 0; a < naz; a++) {
-      uint32_t p0 = rid(k, a), p1 = rid(k, a + 1), q0 = rid(k + 1, a), q1 = rid(k + 1, a + 1);
-      tris.push_back(p0); tris.push_back(p1); tris.push_back(q1);
-      tris.push_back(p0); tris.push_back(q1); tris.push_back(q0);
+    const uint32_t ma = count[k], mb = count[k + 1];
+    uint32_t i = 0, j = 0;
+    while (i < ma || j < mb) {
+      const bool step_a = j == mb || (i < ma && (double)(i + 1) / ma < (double)(j + 1) / mb);
+      if (step_a) {
+        tris.push_back(rid(k, i)); tris.push_back(rid(k, i + 1)); tris.push_back(rid(k + 1, j));
+        i++;
+      } else {
+        tris.push_back(rid(k, i)); tris.push_back(rid(k + 1, j + 1)); tris.push_back(rid(k + 1, j));
+        j++;
+      }
     }
   }
-  size_t last = rx.size() - 1;
-  for (uint32_t a = 0; a < naz; a++) {
+  const size_t last = rx.size() - 1;
+  for (uint32_t a = 0; a < count[last]; a++) {
     tris.push_back(tail); tris.push_back(rid(last, a)); tris.push_back(rid(last, a + 1));
   }
 }

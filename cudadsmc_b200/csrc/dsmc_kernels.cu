@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
     meta->n_scatter = meta->n_alive + meta->n_pending;
     meta->n_pending = 0;
     meta->n_alive = run;
+    meta->tile_next = 0;
     if (bump) {
       meta->step += 1;
       meta->particle_steps += run;

@@ -39,7 +39,7 @@ struct Meta {
   uint32_t samples;      // sampling passes
   uint32_t injected;     // particles injected by the inflow faces (total)
   uint32_t removed;      // particles removed through outflow faces (total)
-  uint32_t pad;
+  uint32_t tile_next;    // the cell kernel's dynamic tile counter (reset by the scan)
   unsigned long long particle_steps;  // sum over steps of the particles placed by the scan
 };
 

@@ -409,6 +409,28 @@ __device__ __forceinline__ bool face_bc(const StepParams& p, float3& pos, float3
   return true;
 }
 
+// Whether this step's flight from pos may reach the body: the path is at
+// least the start cell's clearance (nearest mode) or starts or ends in a
+// geometry cell holding triangles (first-hit mode); a start outside the
+// geometry grid counts when the path's box overlaps the grid's box.  Only
+// decides which pass of the cell kernel flies the particle, never the result.
+__device__ __forceinline__ bool flight_may_meet_body(const StepParams& p, float3 pos, float3 vel) {
+  const GeomView& G = p.geom;
+  const float3 e = make_float3(pos.x + vel.x * p.dt, pos.y + vel.y * p.dt, pos.z + vel.z * p.dt);
+  const uint32_t sc = coll_cell_id(G.grid, pos);
+  if (G.nearest) {
+    if (sc != kNone) {
+      const float dist = length3(make_float3(e.x - pos.x, e.y - pos.y, e.z - pos.z));
+      return !(dist < __ldg(&G.clear[sc]));
+    }
+    return fminf(pos.x, e.x) <= G.grid.gmax.x && fmaxf(pos.x, e.x) >= G.grid.gmin.x &&
+           fminf(pos.y, e.y) <= G.grid.gmax.y && fmaxf(pos.y, e.y) >= G.grid.gmin.y &&
+           fminf(pos.z, e.z) <= G.grid.gmax.z && fmaxf(pos.z, e.z) >= G.grid.gmin.z;
+  }
+  const uint32_t ec = coll_cell_id(G.grid, e);
+  return (sc != kNone && __ldg(&G.flags[sc]) != 0) || (ec != kNone && __ldg(&G.flags[ec]) != 0);
+}
+
 // One particle's flight: IntegrateDev / ProcessCollisionsDev,
 // kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.
 __device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, float3& vel,
