@@ -86,7 +86,53 @@ def wl_box_100k():
                      "equal mix of 200 K and 600 K Maxwellians")
 
 
-WORKLOADS = {"capsule4m": wl_capsule_4m, "sphere500k": wl_sphere_500k, "box100k": wl_box_100k}
+def batch_members(count=64, seed=20261203):
+    """The batched ensemble: `count` sphere flows (icosphere level 3, r=0.1 m,
+    1.2x0.6x0.6 m, 64x32x32 cells, inflow -x, outflow elsewhere, diffuse wall)
+    with particle counts log-uniform in 50k-2M, Mach uniform in 2-10, Knudsen
+    number (sphere diameter) log-uniform in 0.01-1 through the density, and
+    T_wall/T_inf uniform in 1-3; seeded."""
+    rng = np.random.default_rng(seed)
+    dom, dim = (1.2, 0.6, 0.6), (64, 32, 32)
+    cells = dim[0] * dim[1] * dim[2]
+    cell = [dom[k] / dim[k] for k in range(3)]
+    cell_v = cell[0] * cell[1] * cell[2]
+    T, L, m, d = 200.0, 0.2, ARGON["gas_mass"], ARGON["gas_diam"]
+    a = math.sqrt(5.0 / 3.0 * KB * T / m)
+    cmp = math.sqrt(2 * KB * T / m)
+    cbar = math.sqrt(8 * KB * T / (math.pi * m))
+    out = []
+    for i in range(count):
+        n_part = math.exp(rng.uniform(math.log(5e4), math.log(2e6)))
+        mach = rng.uniform(2.0, 10.0)
+        kn = math.exp(rng.uniform(math.log(0.01), math.log(1.0)))
+        tw = rng.uniform(1.0, 3.0)
+        nd = 1.0 / (math.sqrt(2.0) * math.pi * d * d * kn * L)
+        u = mach * a
+        fnum = nd * cell_v / (n_part / cells)
+        dt = min(0.2 * min(cell) / (u + 3 * cmp), 0.2 * kn * L / cbar)
+        st = dict(grid_min=(0, 0, 0), grid_max=dom, grid_dim=dim, density=nd, fnum=fnum, temp=T,
+                  stream_vel=(u, 0.0, 0.0), dt=dt, rng="philox", ntc_local=1, sample_every=100,
+                  init_kind="maxwell", wall_diffuse=1, wall_temp=tw * T, capacity_factor=1.6,
+                  seed=seed + i, geom_nearest=1,
+                  face_kind={"-x": "inflow", "+x": "outflow", "-y": "outflow", "+y": "outflow",
+                             "-z": "outflow", "+z": "outflow"}, **ARGON)
+        out.append(dict(settings=st, particles=n_part, mach=mach, kn=kn, tw_ratio=tw))
+    return out
+
+
+def wl_batch64():
+    return dict(name="batch64_sphere_flows", settings=None,
+                mesh=dict(kind="icosphere", level=3, radius=0.1, center=(0.4, 0.3, 0.3),
+                          grid=(16, 16, 16)),
+                members=batch_members(64),
+                desc="64 independent sphere flows (64x32x32 cells each) in one graph-launched "
+                     "step: particles log-U[50k, 2M], Mach U[2, 10], Kn log-U[0.01, 1], "
+                     "T_wall/T_inf U[1, 3]")
+
+
+WORKLOADS = {"capsule4m": wl_capsule_4m, "sphere500k": wl_sphere_500k, "box100k": wl_box_100k,
+             "batch64": wl_batch64}
 DEFAULT_WORKLOAD = "capsule4m"
 
 
@@ -346,6 +392,89 @@ def run_ours(args, rank, world):
     return out
 
 
+def run_batch(args, rank, world):
+    """Aggregate particle-timesteps/s of the batched ensemble: one graph launch
+    per timestep advances every member; also the same members stepped one
+    after another (each with its own graph) for comparison."""
+    import torch
+    import cudadsmc_b200 as cb
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    wl = WORKLOADS[args.workload]()
+    m = wl["mesh"]
+    v, t = cb.mesh_icosphere(m["level"], m["radius"], m["center"])
+    sols = []
+    for mem in wl["members"]:
+        st = dict(mem["settings"])
+        st["seed"] += rank * 1000
+        sol = cb.DSMCSolver().Init(cb.settings_t().set(**st))
+        sol.SetModel(v, t, m["grid"])
+        sol.InitSystemState()
+        sols.append(sol)
+    batch = cb.DSMCBatch(sols)
+    stream = torch.cuda.Stream()  # a real stream: the batch's branches fork from it
+    batch.SetStream(stream.cuda_stream)
+    batch.Step(args.warmup)
+    variants = batch.Autotune(steps=2) if args.tune_steps > 0 else None
+    batch.Step(2)
+    batch.Sync()
+
+    def particle_steps():
+        return sum(s.Info().particle_steps for s in sols)
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0 = particle_steps()
+    gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0) if world == 1 else dev.index
+    with ClockSampler(gpu_index) as clk:
+        ev0.record(stream)
+        batch.Step(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    batch.Sync()
+    ms = ev0.elapsed_time(ev1)
+    pst = particle_steps() - p0
+    ms_max, total = reduce_over_ranks(ms, pst, world, dev)
+    value = total / (ms_max * 1e-3)
+    # the same members stepped one after another on one stream
+    for s in sols:
+        s.SetStream(stream.cuda_stream)
+        s.StepGraph(s.settings.cfg.dt, 1)
+    torch.cuda.synchronize()
+    k2 = max(3, args.steps // 4)
+    p1 = particle_steps()
+    ev0.record(stream)
+    for _ in range(k2):
+        for s in sols:
+            s.StepGraph(s.settings.cfg.dt, 1)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = ev0.elapsed_time(ev1)
+    seq_value = (particle_steps() - p1) / (seq_ms * 1e-3)
+    n_now = [s.Info().num_particles for s in sols]
+    out = {
+        "metric": "particle-timesteps/s", "value": value, "unit": "particle-timesteps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded members, generated mesh)",
+        "config": {"workload": wl["name"], "description": wl["desc"], "members": len(sols),
+                   "particles_now_total": int(sum(n_now)), "particles_now_min": int(min(n_now)),
+                   "particles_now_max": int(max(n_now)), "cell_kernel_variants": variants,
+                   "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
+                   "l2_policy": "working set of all members (several GB) > 126 MB L2"},
+        "sequential": {"value": seq_value, "ms_per_step": seq_ms / k2,
+                       "note": "same members, one graph launch per member per step, one stream"},
+        "gpu_launches": args.steps * 4 * len(sols),  # scan, scatter, cell, inflow per member
+        "clocks": clk.summary(),
+    }
+    batch.close()
+    for s in sols:
+        s.close()
+    return out
+
+
 def run_e2e(args, wl, rank, world, dev, variant):
     """The same metric through the C ABI with host buffers: per run the
     pinned initial state is uploaded (h2d), then every step is one dsmc_step
@@ -387,6 +516,8 @@ def run_e2e(args, wl, rank, world, dev, variant):
 
 def run_reference(args):
     wl = WORKLOADS[args.workload]()
+    if wl.get("members"):
+        wl = dict(wl, settings=wl["members"][0]["settings"])
     budget = max(10.0, min(120.0, 4.0 * (args.steps + args.warmup)))
     from oracle import oracle as O
     O.set_threads(os.cpu_count() or 1)
@@ -428,7 +559,7 @@ def main():
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    out = run_ours(args, rank, world)
+    out = run_batch(args, rank, world) if args.workload == "batch64" else run_ours(args, rank, world)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -116,6 +116,13 @@ SIGNATURES = [
     ("dsmc_set_kernel_variant", _I, [_P, _I]),
     ("dsmc_get_kernel_variant", _I, [_P, _P, _P]),
     ("dsmc_autotune", _I, [_P, ctypes.c_float, _I, _P, _P]),
+    ("dsmc_batch_create", _I, [_P, _U32, _P]),
+    ("dsmc_batch_destroy", _I, [_P]),
+    ("dsmc_batch_last_error", ctypes.c_char_p, [_P]),
+    ("dsmc_batch_set_stream", _I, [_P, _P]),
+    ("dsmc_batch_step", _I, [_P, _P, _I]),
+    ("dsmc_batch_sync", _I, [_P]),
+    ("dsmc_batch_autotune", _I, [_P, _P, _I, _P]),
     ("dsmc_sample", _I, [_P]),
     ("dsmc_reset_samples", _I, [_P]),
     ("dsmc_read_cell_sums", _I, [_P, _P, ctypes.POINTER(_U32)]),

@@ -50,6 +50,7 @@ struct dsmc_handle {
   bool has_state = false;
   uint64_t step = 0;
   double sim_time = 0.0;
+  uint64_t gen = 0;  // bumped whenever captured launches of this handle go stale
 
   std::vector<dsmcb::Inflow> inflows;
 
@@ -90,6 +91,7 @@ int cuda_fail(dsmc_handle* h, cudaError_t e, const char* where) {
   } while (0)
 
 void drop_graph(dsmc_handle* h) {
+  h->gen++;
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->graph_exec = nullptr;
@@ -418,7 +420,10 @@ int dsmc_create(const dsmc_config* cfg, dsmc_handle** out) {
   h->n_scan_tiles = (h->cells + dsmcb::kScanTile - 1) / dsmcb::kScanTile;
   apply_variant(h, h->variant);
   float capf = c.capacity_factor < 1.f ? 1.f : c.capacity_factor;
-  uint64_t cap = (uint64_t)std::ceil((double)h->ppc * h->cells * capf) + 1024;
+  // the Maxwellian and bimodal starts fill the fractional part of n V_c / F_N too
+  const double ppc_f = c.part_per_cell ? (double)c.part_per_cell
+                                       : (double)c.density * h->cell_volume / c.fnum;
+  uint64_t cap = (uint64_t)std::ceil(std::max(ppc_f, (double)h->ppc + 1.0) * h->cells * capf) + 1024;
   if (cap > 0xF0000000ull) {
     delete h;
     return fail(nullptr, DSMC_ERR_CONFIG, "particle capacity exceeds 32-bit indexing");
@@ -769,10 +774,18 @@ static bool geometry_in_cell(const dsmcb::GeomGrid& g, const float cmin[3], cons
 int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) {
   if (!h) return DSMC_ERR_ARG;
   const dsmc_config& c = h->cfg;
-  std::vector<uint32_t> slot(h->cells + 1);
+  std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
   uint64_t n = 0;
   const bool geo = h->has_geom && c.geometry;
+  // the reference fills ppc = floor(n V_c / F_N) particles per cell; the
+  // Maxwellian and bimodal starts also honour the fraction (ppc + 1 in a
+  // seeded share of the cells), which matters below a few particles per cell
+  const double ppc_f = c.part_per_cell ? (double)c.part_per_cell
+                                       : (double)c.density * h->cell_volume / c.fnum;
+  const double frac = c.init_kind == DSMC_INIT_REFERENCE ? 0.0 : ppc_f - (double)h->ppc;
+  uint64_t mix = c.seed ^ 0x5DEECE66Dull;
   for (uint32_t cell = 0; cell < h->cells; cell++) {
+    const double u = (double)(splitmix64(mix) >> 11) / 9007199254740992.0;
     uint32_t cx = cell % c.grid_dim[0], cy = (cell / c.grid_dim[0]) % c.grid_dim[1],
              cz = cell / (c.grid_dim[0] * c.grid_dim[1]);
     float cmin[3] = {c.grid_min[0] + cx * h->cell_size[0], c.grid_min[1] + cy * h->cell_size[1],
@@ -782,15 +795,19 @@ int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) 
       continue;
     }
     slot[cell] = (uint32_t)n;
-    n += h->ppc;
+    count[cell] = h->ppc + (u < frac ? 1u : 0u);
+    n += count[cell];
   }
   if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "initial particles exceed capacity");
   CK(h, cudaMemcpyAsync(h->start, slot.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
      "init upload");
+  CK(h, cudaMemcpyAsync(h->count, count.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
+     "init upload");
   dsmcb::InitParams ip{};
   ip.grid = h->grid;
   ip.cells = h->cells;
-  ip.ppc = h->ppc;
+  ip.ppc = h->ppc + (frac > 0.0 ? 1u : 0u);
+  ip.cell_count = h->count;
   ip.kind = c.init_kind;
   ip.vstd = std::sqrt(1.3806e-23f * c.temp / c.gas_mass);
   ip.vstd2 = std::sqrt(1.3806e-23f * (c.init_temp2 > 0 ? c.init_temp2 : c.temp) / c.gas_mass);
@@ -1319,6 +1336,208 @@ int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint
   cudaError_t e = dsmcb::launch_sample_cells(u, v, w, cell_start, ncells, sums5, 1, 5,
                                              (cudaStream_t)stream);
   return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+// ------------------------------------------------------------- batches ----
+
+// Several handles advanced by one CUDA graph per timestep: a fork from the
+// batch stream to one stream per member, each member's step on its branch,
+// and a join back (no counterpart in the reference, which has one solver per
+// process).
+struct dsmc_batch {
+  std::vector<dsmc_handle*> members;
+  std::vector<float> dt;
+  std::vector<uint64_t> gen;
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> ev;  // fork + one join per member
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int batch_fail(dsmc_batch* b, int code, const std::string& msg) {
+  b->err = msg;
+  return code;
+}
+
+void batch_drop_graph(dsmc_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+void batch_free(dsmc_batch* b) {
+  batch_drop_graph(b);
+  for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+  for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
+  if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+bool batch_graph_current(const dsmc_batch* b, const std::vector<float>& dt) {
+  if (!b->exec || dt != b->dt) return false;
+  for (size_t i = 0; i < b->members.size(); i++)
+    if (b->members[i]->gen != b->gen[i]) return false;
+  return true;
+}
+
+int batch_capture(dsmc_batch* b, const std::vector<float>& dt) {
+  batch_drop_graph(b);
+  const size_t n = b->members.size();
+  std::vector<cudaStream_t> saved(n);
+  std::vector<bool> prof(n);
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (!e) e = cudaEventRecord(b->ev[0], b->stream);
+  for (size_t i = 0; i < n && !e; i++) {
+    dsmc_handle* h = b->members[i];
+    saved[i] = h->stream;
+    prof[i] = h->profiling;
+    h->profiling = false;
+    h->stream = b->branch[i];
+    e = cudaStreamWaitEvent(b->branch[i], b->ev[0], 0);
+    if (!e) e = enqueue_step(h, dt[i]);
+    if (!e) e = cudaEventRecord(b->ev[i + 1], b->branch[i]);
+    if (!e) e = cudaStreamWaitEvent(b->stream, b->ev[i + 1], 0);
+    h->stream = saved[i];
+    h->profiling = prof[i];
+  }
+  cudaError_t e2 = cudaStreamEndCapture(b->stream, &b->graph);
+  if (e || e2) {
+    batch_drop_graph(b);
+    return batch_fail(b, DSMC_ERR_CUDA,
+                      std::string("batch graph capture: ") + cudaGetErrorString(e ? e : e2));
+  }
+  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e) {
+    batch_drop_graph(b);
+    return batch_fail(b, DSMC_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(e));
+  }
+  b->dt = dt;
+  for (size_t i = 0; i < n; i++) b->gen[i] = b->members[i]->gen;
+  return DSMC_OK;
+}
+
+}  // namespace
+
+int dsmc_batch_create(dsmc_handle* const* members, uint32_t n, dsmc_batch** out) {
+  if (!members || !n || !out) return DSMC_ERR_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return DSMC_ERR_CUDA;
+  dsmc_batch* b = new dsmc_batch();
+  for (uint32_t i = 0; i < n; i++) {
+    if (!members[i] || members[i]->device != dev) {
+      delete b;
+      g_create_error = "batch members must be handles created on the current device";
+      return DSMC_ERR_ARG;
+    }
+    for (uint32_t j = 0; j < i; j++)
+      if (members[j] == members[i]) {
+        delete b;
+        g_create_error = "a handle appears twice in the batch";
+        return DSMC_ERR_ARG;
+      }
+    b->members.push_back(members[i]);
+  }
+  b->gen.assign(n, 0);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  for (uint32_t i = 0; i < n && !e; i++) {
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (!e) b->branch.push_back(s);
+  }
+  for (uint32_t i = 0; i <= n && !e; i++) {
+    cudaEvent_t ev = nullptr;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (!e) b->ev.push_back(ev);
+  }
+  if (e) {
+    g_create_error = std::string("batch streams: ") + cudaGetErrorString(e);
+    batch_free(b);
+    return DSMC_ERR_CUDA;
+  }
+  *out = b;
+  return DSMC_OK;
+}
+
+int dsmc_batch_destroy(dsmc_batch* b) {
+  if (!b) return DSMC_ERR_ARG;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_free(b);
+  return DSMC_OK;
+}
+
+const char* dsmc_batch_last_error(const dsmc_batch* b) { return b ? b->err.c_str() : ""; }
+
+int dsmc_batch_set_stream(dsmc_batch* b, void* stream) {
+  if (!b) return DSMC_ERR_ARG;
+  if (b->own_stream && b->stream) {
+    cudaStreamSynchronize(b->stream);
+    cudaStreamDestroy(b->stream);
+  }
+  if (stream) {
+    b->stream = (cudaStream_t)stream;
+    b->own_stream = false;
+  } else {
+    b->own_stream = true;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return batch_fail(b, DSMC_ERR_CUDA, "batch stream");
+  }
+  batch_drop_graph(b);
+  return DSMC_OK;
+}
+
+int dsmc_batch_step(dsmc_batch* b, const float* dt, int nsteps) {
+  if (!b || nsteps < 0) return DSMC_ERR_ARG;
+  const size_t n = b->members.size();
+  std::vector<float> d(n);
+  for (size_t i = 0; i < n; i++) {
+    dsmc_handle* h = b->members[i];
+    if (!h->has_state) return batch_fail(b, DSMC_ERR_STATE, "a member has no particle state");
+    d[i] = dt ? dt[i] : h->cfg.dt;
+  }
+  if (!batch_graph_current(b, d)) {
+    const int st = batch_capture(b, d);
+    if (st) return st;
+  }
+  for (int k = 0; k < nsteps; k++) {
+    const cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+    if (e) return batch_fail(b, DSMC_ERR_CUDA, std::string("batch graph launch: ") + cudaGetErrorString(e));
+    for (size_t i = 0; i < n; i++) {
+      b->members[i]->step++;
+      b->members[i]->sim_time += d[i];
+    }
+  }
+  return DSMC_OK;
+}
+
+int dsmc_batch_sync(dsmc_batch* b) {
+  if (!b) return DSMC_ERR_ARG;
+  const cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e) return batch_fail(b, DSMC_ERR_CUDA, std::string("batch sync: ") + cudaGetErrorString(e));
+  for (dsmc_handle* h : b->members) {
+    const int st = check_device_flags(h);
+    if (st) return batch_fail(b, st, h->err);
+  }
+  return DSMC_OK;
+}
+
+int dsmc_batch_autotune(dsmc_batch* b, const float* dt, int steps, int* variants) {
+  if (!b || steps < 1) return DSMC_ERR_ARG;
+  int st = dsmc_batch_sync(b);
+  if (st) return st;
+  for (size_t i = 0; i < b->members.size(); i++) {
+    dsmc_handle* h = b->members[i];
+    int best = 0;
+    st = dsmc_autotune(h, dt ? dt[i] : h->cfg.dt, steps, &best, nullptr);
+    if (st) return batch_fail(b, st, h->err);
+    if (variants) variants[i] = best;
+  }
+  return DSMC_OK;
 }
 
 }  // extern "C"

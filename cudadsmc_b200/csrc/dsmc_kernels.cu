@@ -313,7 +313,7 @@ __global__ void k_init_fill(const InitParams p) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
     const uint32_t cell = i / p.ppc, k = i - cell * p.ppc;
     const uint32_t dst0 = p.cell_slot[cell];
-    if (dst0 == kNone) continue;
+    if (dst0 == kNone || k >= p.cell_count[cell]) continue;
     const uint32_t d = dst0 + k;
     const uint32_t cx = cell % p.grid.dim.x;
     const uint32_t cy = (cell / p.grid.dim.x) % p.grid.dim.y;

@@ -172,6 +172,7 @@ struct InitParams {
   float3 stream;
   uint2 seed;
   const uint32_t* cell_slot;  // per cell: first particle index, kNone = skipped cell
+  const uint32_t* cell_count; // per cell: particles to fill (<= ppc)
   SoA out;
 };
 cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);

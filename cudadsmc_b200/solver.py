@@ -241,6 +241,54 @@ class DSMCSolver:
         self._check(lib().dsmc_restore(self.h, str(path).encode()), "Restore")
 
 
+class DSMCBatch:
+    """Independent solvers advanced together by one CUDA graph launch per
+    timestep (dsmc_batch_*).  The solvers stay owned by the caller; close the
+    batch before them."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        hs = (ctypes.c_void_p * len(self.solvers))(*[s.h for s in self.solvers])
+        b = ctypes.c_void_p()
+        check(lib().dsmc_batch_create(hs, len(self.solvers), ctypes.byref(b)), "DSMCBatch")
+        self.b = b.value
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        if getattr(self, "b", None):
+            lib().dsmc_batch_destroy(self.b)
+            self.b = None
+
+    def _check(self, st, where):
+        if st != _capi.DSMC_OK:
+            detail = lib().dsmc_batch_last_error(self.b)
+            raise _capi.DsmcError(st, where, detail.decode() if detail else "")
+
+    def _dt(self, dt):
+        if dt is None:
+            return None
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float32), (len(self.solvers),)))
+        return d
+
+    def SetStream(self, stream):
+        self._check(lib().dsmc_batch_set_stream(self.b, ctypes.c_void_p(stream)), "SetStream")
+
+    def Step(self, nsteps=1, dt=None):
+        d = self._dt(dt)
+        self._check(lib().dsmc_batch_step(self.b, _ptr(d), int(nsteps)), "Step")
+
+    def Sync(self):
+        self._check(lib().dsmc_batch_sync(self.b), "Sync")
+
+    def Autotune(self, steps=5, dt=None):
+        d = self._dt(dt)
+        v = np.zeros(len(self.solvers), np.int32)
+        self._check(lib().dsmc_batch_autotune(self.b, _ptr(d), int(steps), _ptr(v)), "Autotune")
+        return [int(x) for x in v]
+
+
 def CreateSolver(kind="gpu"):
     """CreateSolver(SolverGPU).  The reference's CPU solver type returns None
     there as well (kernels/dsmc_base.cu:225-226)."""

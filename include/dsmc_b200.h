@@ -231,6 +231,30 @@ int dsmc_get_kernel_variant(dsmc_handle* h, int* variant, int* chunk_capacity);
  * receives 4 times in milliseconds.  Blocks until done. */
 int dsmc_autotune(dsmc_handle* h, float dt, int steps, int* best, float* ms_per_step);
 
+/* Batches (no counterpart in the reference, which runs one solver per
+ * process): independent handles of uneven size advanced together, one CUDA
+ * graph launch per timestep with one branch per member, so small instances
+ * run concurrently.  Members must live on the current device and appear once;
+ * the batch does not own them (destroy the batch first).  Batch work is
+ * ordered on the batch stream, not on the members' streams: call
+ * dsmc_batch_sync before using a member on its own.  The graph is captured on
+ * the first step and again whenever a dt or a member's launch set changes
+ * (kernel variant, mesh, stream).  Results equal stepping each member alone. */
+typedef struct dsmc_batch dsmc_batch;
+int dsmc_batch_create(dsmc_handle* const* members, uint32_t n, dsmc_batch** out);
+int dsmc_batch_destroy(dsmc_batch* b);
+const char* dsmc_batch_last_error(const dsmc_batch* b);
+/* Orders the batch's launches on this stream (NULL: a stream of its own). */
+int dsmc_batch_set_stream(dsmc_batch* b, void* stream);
+/* nsteps timesteps of every member; dt holds one step length per member
+ * (NULL: each member's configured dt).  Asynchronous on the batch stream. */
+int dsmc_batch_step(dsmc_batch* b, const float* dt, int nsteps);
+/* Synchronises the batch stream and reports the members' device error flags. */
+int dsmc_batch_sync(dsmc_batch* b);
+/* dsmc_autotune for every member (each advances by 4 * (steps + 2) steps);
+ * variants (optional) receives the chosen variant per member. */
+int dsmc_batch_autotune(dsmc_batch* b, const float* dt, int steps, int* variants);
+
 /* SampleCellStatistics (kernels/dsmc_kernel.cu:892-910): adds the current
  * velocities to the FP64 per-cell accumulators now. */
 int dsmc_sample(dsmc_handle* h);
