@@ -113,6 +113,15 @@ SIGNATURES = [
     ("dsmc_get_cell_state", _I, [_P, _P, _P]),
     ("dsmc_step", _I, [_P, ctypes.c_float, _I]),
     ("dsmc_step_graph", _I, [_P, ctypes.c_float, _I]),
+    ("dsmc_init_from_fields", _I, [_P, _P, _P]),
+    ("dsmc_gemm_bf16", _I, [_I, _I, _I, _P, _I, _I, _P, _I, _I, _P, _I, ctypes.c_float, _P, _I, _P,
+                            _I, _I, _P]),
+    ("dsmc_gelu_backward", _I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),
+    ("dsmc_colsum", _I, [_P, _I, _I, _I, _P, _P]),
+    ("dsmc_mse_grad", _I, [_P, _P, ctypes.c_size_t, ctypes.c_float, _P, _P, _P, _P, _P]),
+    ("dsmc_adam_step", _I, [_P, _P, _P, _P, _P, ctypes.c_size_t, ctypes.c_float, ctypes.c_float,
+                            ctypes.c_float, ctypes.c_float, _I, ctypes.c_float, _P]),
+    ("dsmc_to_bf16", _I, [_P, _P, ctypes.c_size_t, _P]),
     ("dsmc_set_kernel_variant", _I, [_P, _I]),
     ("dsmc_get_kernel_variant", _I, [_P, _P, _P]),
     ("dsmc_autotune", _I, [_P, ctypes.c_float, _I, _P, _P]),

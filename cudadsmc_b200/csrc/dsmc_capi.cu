@@ -824,6 +824,73 @@ int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) 
   return DSMC_OK;
 }
 
+int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out) {
+  if (!h || !fields5) return fail(h, DSMC_ERR_ARG, "null argument");
+  const dsmc_config& c = h->cfg;
+  std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
+  std::vector<float4> state(h->cells);
+  const bool geo = h->has_geom && c.geometry;
+  const float kb_m = 1.3806e-23f / c.gas_mass;
+  uint64_t mix = c.seed ^ 0x2545F4914F6CDD1Dull;
+  uint64_t n = 0;
+  uint32_t kmax = 0;
+  for (uint32_t cell = 0; cell < h->cells; cell++) {
+    const double u01 = (double)(splitmix64(mix) >> 11) / 9007199254740992.0;
+    const float* f = fields5 + 5 * (size_t)cell;
+    uint32_t cx = cell % c.grid_dim[0], cy = (cell / c.grid_dim[0]) % c.grid_dim[1],
+             cz = cell / (c.grid_dim[0] * c.grid_dim[1]);
+    float cmin[3] = {c.grid_min[0] + cx * h->cell_size[0], c.grid_min[1] + cy * h->cell_size[1],
+                     c.grid_min[2] + cz * h->cell_size[2]};
+    if (geo && geometry_in_cell(h->ggrid, cmin, h->cell_size)) {
+      slot[cell] = 0xffffffffu;
+      continue;
+    }
+    // expected simulator particles n V_c / F_N, rounded stochastically
+    const double expect = (std::isfinite(f[0]) && f[0] > 0.f) ? (double)f[0] * h->cell_volume / c.fnum : 0.0;
+    const double fl = std::floor(expect);
+    const uint32_t k = (uint32_t)fl + (u01 < expect - fl ? 1u : 0u);
+    slot[cell] = (uint32_t)n;
+    count[cell] = k;
+    kmax = std::max(kmax, k);
+    n += k;
+    const float T = (std::isfinite(f[4]) && f[4] > 0.f) ? f[4] : c.temp;
+    state[cell] = make_float4(std::isfinite(f[1]) ? f[1] : 0.f, std::isfinite(f[2]) ? f[2] : 0.f,
+                              std::isfinite(f[3]) ? f[3] : 0.f, std::sqrt(kb_m * T));
+  }
+  if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "seeded particles exceed capacity");
+  // the per-cell drift and spread travel in the sampling accumulators, which
+  // a new state resets anyway
+  static_assert(sizeof(float4) <= 5 * sizeof(double), "cell state must fit the accumulators");
+  float4* dstate = reinterpret_cast<float4*>(h->acc);
+  CK(h, cudaMemcpyAsync(h->start, slot.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
+     "seed upload");
+  CK(h, cudaMemcpyAsync(h->count, count.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
+     "seed upload");
+  CK(h, cudaMemcpyAsync(dstate, state.data(), h->cells * sizeof(float4), cudaMemcpyHostToDevice,
+                        h->stream), "seed upload");
+  dsmcb::InitParams ip{};
+  ip.grid = h->grid;
+  ip.cells = h->cells;
+  ip.ppc = kmax;
+  ip.kind = DSMC_INIT_MAXWELL;
+  ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
+  ip.cell_slot = h->start;
+  ip.cell_count = h->count;
+  ip.cell_state = dstate;
+  ip.out = soa_of(h->A);
+  CK(h, dsmcb::launch_init_fill(ip, h->stream), "seed fill");
+  CK(h, cudaMemsetAsync(h->acc, 0, 5 * (size_t)h->cells * sizeof(double), h->stream), "reset samples");
+  int st = reindex(h, (uint32_t)n);
+  if (st) return st;
+  Meta m{};
+  st = read_meta(h, m);
+  if (st) return st;
+  m.samples = 0;
+  CK(h, cudaMemcpy(&h->meta->samples, &m.samples, 4, cudaMemcpyHostToDevice), "meta");
+  if (n_out) *n_out = (uint32_t)n;
+  return DSMC_OK;
+}
+
 int dsmc_upload_state(dsmc_handle* h, const float* pos, const float* vel, uint32_t n, int soa) {
   if (!h || (n && (!pos || (!vel && !soa)))) return fail(h, DSMC_ERR_ARG, "null state");
   if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "state exceeds particle capacity");

@@ -328,13 +328,19 @@ __global__ void k_init_fill(const InitParams p) {
       vel.y = vv * sinf(r.uniform() * tetha) + p.stream.y;
       vel.z = vv * sinf(r.uniform() * tetha) + p.stream.z;
     } else {
-      const float sd = (p.kind == 2 && (i & 1u)) ? p.vstd2 : p.vstd;
+      float sd = (p.kind == 2 && (i & 1u)) ? p.vstd2 : p.vstd;
+      float3 drift = p.stream;
+      if (p.cell_state) {
+        const float4 cs = p.cell_state[cell];
+        drift = make_float3(cs.x, cs.y, cs.z);
+        sd = cs.w;
+      }
       const float r1 = r.uniform(), r2 = r.uniform(), r3 = r.uniform(), r4 = r.uniform();
       const float m1 = sd * sqrtf(-2.f * logf(r1)), m2 = sd * sqrtf(-2.f * logf(r3));
       float s1, c1, s2, c2;
       sincospif(2.0f * r2, &s1, &c1);
       sincospif(2.0f * r4, &s2, &c2);
-      vel = make_float3(m1 * c1 + p.stream.x, m1 * s1 + p.stream.y, m2 * c2 + p.stream.z);
+      vel = make_float3(m1 * c1 + drift.x, m1 * s1 + drift.y, m2 * c2 + drift.z);
     }
     const float3 cellmin = make_float3(p.grid.gmin.x + cx * p.grid.cell.x,
                                        p.grid.gmin.y + cy * p.grid.cell.y,

@@ -173,6 +173,7 @@ struct InitParams {
   uint2 seed;
   const uint32_t* cell_slot;  // per cell: first particle index, kNone = skipped cell
   const uint32_t* cell_count; // per cell: particles to fill (<= ppc)
+  const float4* cell_state;   // optional per cell (u, v, w, sqrt(kT/m)) of the Maxwellian
   SoA out;
 };
 cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);

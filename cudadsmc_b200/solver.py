@@ -110,6 +110,15 @@ class DSMCSolver:
         self._check(lib().dsmc_init_state(self.h, _ptr(sv), ctypes.byref(n)), "InitSystemState")
         return n.value
 
+    def InitFromFields(self, fields):
+        """Seeds the particles from per-cell (n, u, v, w, T) fields [cells, 5]."""
+        f = np.ascontiguousarray(fields, np.float32).reshape(-1, 5)
+        if f.shape[0] != self.settings.getCellsCount():
+            raise ValueError("fields must hold one (n, u, v, w, T) row per cell")
+        n = ctypes.c_uint32()
+        self._check(lib().dsmc_init_from_fields(self.h, _ptr(f), ctypes.byref(n)), "InitFromFields")
+        return n.value
+
     def RunSimulationStep(self, dt, nsteps=1):
         self._check(lib().dsmc_step(self.h, dt, nsteps), "RunSimulationStep")
 

@@ -199,6 +199,17 @@ int dsmc_mesh_capsule(float nose_radius, float cone_half_angle_deg, float length
  * geometry) and runs a zero-length move.  Returns the particle count. */
 int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out);
 
+/* Seeds the particle population from per-cell fields instead of the
+ * free-stream fill (extension; the reference only has the uniform fill,
+ * kernels/dsmc_kernel.cu:394-427): fields5 holds per cell (x fastest) the
+ * number density n [m^-3], the mean velocity (u, v, w) [m/s] and the
+ * temperature T [K].  Each cell receives n V_c / F_N particles (rounded
+ * stochastically from the seed) drawn from the Maxwellian at (u, v, w, T);
+ * cells covered by the mesh stay empty, as in dsmc_init_state; non-finite or
+ * non-positive n gives an empty cell, a non-finite or non-positive T the
+ * configured temperature.  Resets the sampling accumulators. */
+int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out);
+
 /* Host <-> device particle state.  soa != 0: six arrays of n floats
  * (x,y,z,u,v,w) back to back; soa == 0: pos4 and vel4 float4 AoS as the
  * reference's particles_state_t.  Upload resets the cell order. */
@@ -378,6 +389,33 @@ int dsmc_stage_move(dsmc_handle* h, const dsmc_move_params* p, float* x, float* 
  * count, sums of u,v,w and |v|^2 per cell into sums5 (5 doubles per cell). */
 int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint32_t* cell_start,
                       uint32_t ncells, double* sums5, void* stream);
+
+/* --- Warm-start surrogate kernels (no counterpart in the reference) ---
+ * Device pointers, asynchronous on `stream`.  BF16 operands, FP32
+ * accumulation.  dsmc_gemm_bf16: c = A B (+ bias) (+ beta c) for an m x n
+ * result; a_trans = 1 reads A stored k x m, b_trans = 1 reads B stored n x k
+ * (row-major, leading dimensions lda/ldb/ldc/ldcb in elements).  act = 1
+ * applies GELU: c keeps the pre-activation, c_bf16 (optional) receives the
+ * activation in BF16.  Requires k, lda, ldb multiples of 8, 16-byte aligned
+ * A and B, m a multiple of 8 when a_trans, n a multiple of 8 unless b_trans.
+ * split_k > 1 splits the reduction and adds into c with atomics (c zeroed by
+ * the caller; no bias, act or c_bf16). */
+int dsmc_gemm_bf16(int m, int n, int k, const void* a, int lda, int a_trans, const void* b, int ldb,
+                   int b_trans, float* c, int ldc, float beta, const float* bias, int act, void* c_bf16,
+                   int ldcb, int split_k, void* stream);
+/* dz = dh * GELU'(z), in FP32 and/or BF16. */
+int dsmc_gelu_backward(const float* z, const float* dh, float* dz, void* dz_bf16, size_t n,
+                       void* stream);
+/* out[col] = sum over rows of x[row * ld + col]. */
+int dsmc_colsum(const float* x, int rows, int cols, int ld, float* out, void* stream);
+/* Masked mean-square error: for every finite BF16 target t, loss += (y - t)^2,
+ * count += 1 and dy = scale * 2 (y - t); NaN targets give dy = 0. */
+int dsmc_mse_grad(const float* y, const void* t_bf16, size_t n, float scale, void* dy_bf16, float* dy,
+                  double* loss, unsigned long long* count, void* stream);
+/* Adam step t (>= 1) with decoupled weight decay; refreshes w_bf16 if given. */
+int dsmc_adam_step(float* w, const float* g, float* m, float* v, void* w_bf16, size_t n, float lr,
+                   float b1, float b2, float eps, int t, float weight_decay, void* stream);
+int dsmc_to_bf16(const float* x, void* y, size_t n, void* stream);
 
 #ifdef __cplusplus
 }
