@@ -771,114 +771,44 @@ static bool geometry_in_cell(const dsmcb::GeomGrid& g, const float cmin[3], cons
          flagged(x0, y0, z1) || flagged(x1, y0, z1);
 }
 
-int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) {
-  if (!h) return DSMC_ERR_ARG;
-  const dsmc_config& c = h->cfg;
-  std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
-  uint64_t n = 0;
-  const bool geo = h->has_geom && c.geometry;
-  // the reference fills ppc = floor(n V_c / F_N) particles per cell; the
-  // Maxwellian and bimodal starts also honour the fraction (ppc + 1 in a
-  // seeded share of the cells), which matters below a few particles per cell
-  const double ppc_f = c.part_per_cell ? (double)c.part_per_cell
-                                       : (double)c.density * h->cell_volume / c.fnum;
-  const double frac = c.init_kind == DSMC_INIT_REFERENCE ? 0.0 : ppc_f - (double)h->ppc;
-  uint64_t mix = c.seed ^ 0x5DEECE66Dull;
-  for (uint32_t cell = 0; cell < h->cells; cell++) {
-    const double u = (double)(splitmix64(mix) >> 11) / 9007199254740992.0;
-    uint32_t cx = cell % c.grid_dim[0], cy = (cell / c.grid_dim[0]) % c.grid_dim[1],
-             cz = cell / (c.grid_dim[0] * c.grid_dim[1]);
-    float cmin[3] = {c.grid_min[0] + cx * h->cell_size[0], c.grid_min[1] + cy * h->cell_size[1],
-                     c.grid_min[2] + cz * h->cell_size[2]};
-    if (geo && geometry_in_cell(h->ggrid, cmin, h->cell_size)) {
-      slot[cell] = 0xffffffffu;
-      continue;
-    }
-    slot[cell] = (uint32_t)n;
-    count[cell] = h->ppc + (u < frac ? 1u : 0u);
-    n += count[cell];
-  }
+namespace {
+
+// Scratch of the extension fills inside the sampling accumulators (40 bytes
+// per cell, reset after the fill): per-cell Maxwellian state, an outside
+// point and the outside fraction.
+float4* fill_state(dsmc_handle* h) { return reinterpret_cast<float4*>(h->acc); }
+float4* fill_point(dsmc_handle* h) { return reinterpret_cast<float4*>(h->acc) + h->cells; }
+float* fill_frac(dsmc_handle* h) { return reinterpret_cast<float*>(fill_point(h) + h->cells); }
+static_assert(2 * sizeof(float4) + sizeof(float) <= 5 * sizeof(double),
+              "fill scratch must fit the accumulators");
+
+// Fraction of every cell outside the mesh (all ones without one).
+int outside_fractions(dsmc_handle* h, std::vector<float>& frac) {
+  frac.assign(h->cells, 1.f);
+  if (!(h->has_geom && h->cfg.geometry)) return DSMC_OK;
+  CK(h, dsmcb::launch_outside_fraction(h->grid, base_params(h, h->cfg.dt).geom, h->cells,
+                                       fill_frac(h), fill_point(h), h->stream), "outside fraction");
+  CK(h, cudaMemcpyAsync(frac.data(), fill_frac(h), h->cells * sizeof(float), cudaMemcpyDeviceToHost,
+                        h->stream), "outside fraction");
+  CK(h, cudaStreamSynchronize(h->stream), "outside fraction");
+  return DSMC_OK;
+}
+
+// Uploads the per-cell slots and counts, fills, resets the accumulators and
+// indexes the new state.
+int finish_fill(dsmc_handle* h, dsmcb::InitParams& ip, const std::vector<uint32_t>& slot,
+                const std::vector<uint32_t>& count, uint64_t n, uint32_t* n_out) {
   if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "initial particles exceed capacity");
   CK(h, cudaMemcpyAsync(h->start, slot.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
      "init upload");
   CK(h, cudaMemcpyAsync(h->count, count.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
      "init upload");
-  dsmcb::InitParams ip{};
   ip.grid = h->grid;
   ip.cells = h->cells;
-  ip.ppc = h->ppc + (frac > 0.0 ? 1u : 0u);
-  ip.cell_count = h->count;
-  ip.kind = c.init_kind;
-  ip.vstd = std::sqrt(1.3806e-23f * c.temp / c.gas_mass);
-  ip.vstd2 = std::sqrt(1.3806e-23f * (c.init_temp2 > 0 ? c.init_temp2 : c.temp) / c.gas_mass);
-  ip.vmp = std::sqrt(2 * 1.3806e-23f * c.temp / c.gas_mass);
-  const float* sv = stream_vel ? stream_vel : c.stream_vel;
-  ip.stream = make_float3(sv[0], sv[1], sv[2]);
-  ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
   ip.cell_slot = h->start;
+  ip.cell_count = h->count;
   ip.out = soa_of(h->A);
   CK(h, dsmcb::launch_init_fill(ip, h->stream), "init fill");
-  int st = reindex(h, (uint32_t)n);
-  if (st) return st;
-  if (n_out) *n_out = (uint32_t)n;
-  return DSMC_OK;
-}
-
-int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out) {
-  if (!h || !fields5) return fail(h, DSMC_ERR_ARG, "null argument");
-  const dsmc_config& c = h->cfg;
-  std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
-  std::vector<float4> state(h->cells);
-  const bool geo = h->has_geom && c.geometry;
-  const float kb_m = 1.3806e-23f / c.gas_mass;
-  uint64_t mix = c.seed ^ 0x2545F4914F6CDD1Dull;
-  uint64_t n = 0;
-  uint32_t kmax = 0;
-  for (uint32_t cell = 0; cell < h->cells; cell++) {
-    const double u01 = (double)(splitmix64(mix) >> 11) / 9007199254740992.0;
-    const float* f = fields5 + 5 * (size_t)cell;
-    uint32_t cx = cell % c.grid_dim[0], cy = (cell / c.grid_dim[0]) % c.grid_dim[1],
-             cz = cell / (c.grid_dim[0] * c.grid_dim[1]);
-    float cmin[3] = {c.grid_min[0] + cx * h->cell_size[0], c.grid_min[1] + cy * h->cell_size[1],
-                     c.grid_min[2] + cz * h->cell_size[2]};
-    if (geo && geometry_in_cell(h->ggrid, cmin, h->cell_size)) {
-      slot[cell] = 0xffffffffu;
-      continue;
-    }
-    // expected simulator particles n V_c / F_N, rounded stochastically
-    const double expect = (std::isfinite(f[0]) && f[0] > 0.f) ? (double)f[0] * h->cell_volume / c.fnum : 0.0;
-    const double fl = std::floor(expect);
-    const uint32_t k = (uint32_t)fl + (u01 < expect - fl ? 1u : 0u);
-    slot[cell] = (uint32_t)n;
-    count[cell] = k;
-    kmax = std::max(kmax, k);
-    n += k;
-    const float T = (std::isfinite(f[4]) && f[4] > 0.f) ? f[4] : c.temp;
-    state[cell] = make_float4(std::isfinite(f[1]) ? f[1] : 0.f, std::isfinite(f[2]) ? f[2] : 0.f,
-                              std::isfinite(f[3]) ? f[3] : 0.f, std::sqrt(kb_m * T));
-  }
-  if (n > h->capacity) return fail(h, DSMC_ERR_CAPACITY, "seeded particles exceed capacity");
-  // the per-cell drift and spread travel in the sampling accumulators, which
-  // a new state resets anyway
-  static_assert(sizeof(float4) <= 5 * sizeof(double), "cell state must fit the accumulators");
-  float4* dstate = reinterpret_cast<float4*>(h->acc);
-  CK(h, cudaMemcpyAsync(h->start, slot.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
-     "seed upload");
-  CK(h, cudaMemcpyAsync(h->count, count.data(), (h->cells + 1) * 4, cudaMemcpyHostToDevice, h->stream),
-     "seed upload");
-  CK(h, cudaMemcpyAsync(dstate, state.data(), h->cells * sizeof(float4), cudaMemcpyHostToDevice,
-                        h->stream), "seed upload");
-  dsmcb::InitParams ip{};
-  ip.grid = h->grid;
-  ip.cells = h->cells;
-  ip.ppc = kmax;
-  ip.kind = DSMC_INIT_MAXWELL;
-  ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
-  ip.cell_slot = h->start;
-  ip.cell_count = h->count;
-  ip.cell_state = dstate;
-  ip.out = soa_of(h->A);
-  CK(h, dsmcb::launch_init_fill(ip, h->stream), "seed fill");
   CK(h, cudaMemsetAsync(h->acc, 0, 5 * (size_t)h->cells * sizeof(double), h->stream), "reset samples");
   int st = reindex(h, (uint32_t)n);
   if (st) return st;
@@ -889,6 +819,122 @@ int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out)
   CK(h, cudaMemcpy(&h->meta->samples, &m.samples, 4, cudaMemcpyHostToDevice), "meta");
   if (n_out) *n_out = (uint32_t)n;
   return DSMC_OK;
+}
+
+double unit_draw(uint64_t& mix) { return (double)(splitmix64(mix) >> 11) / 9007199254740992.0; }
+
+}  // namespace
+
+int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) {
+  if (!h) return DSMC_ERR_ARG;
+  const dsmc_config& c = h->cfg;
+  std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
+  uint64_t n = 0;
+  const bool geo = h->has_geom && c.geometry;
+  const bool reference = c.init_kind == DSMC_INIT_REFERENCE;
+  dsmcb::InitParams ip{};
+  uint64_t mix = c.seed ^ 0x5DEECE66Dull;
+  if (reference) {
+    // InitSystemState / GenerateInitialVelocities (kernels/dsmc_kernel.cu:394-427):
+    // ppc = floor(n V_c / F_N) particles in every cell the mesh does not touch
+    for (uint32_t cell = 0; cell < h->cells; cell++) {
+      uint32_t cx = cell % c.grid_dim[0], cy = (cell / c.grid_dim[0]) % c.grid_dim[1],
+               cz = cell / (c.grid_dim[0] * c.grid_dim[1]);
+      float cmin[3] = {c.grid_min[0] + cx * h->cell_size[0], c.grid_min[1] + cy * h->cell_size[1],
+                       c.grid_min[2] + cz * h->cell_size[2]};
+      if (geo && geometry_in_cell(h->ggrid, cmin, h->cell_size)) {
+        slot[cell] = 0xffffffffu;
+        continue;
+      }
+      slot[cell] = (uint32_t)n;
+      count[cell] = h->ppc;
+      n += h->ppc;
+    }
+    ip.ppc = h->ppc;
+  } else {
+    // the Maxwellian and bimodal starts: n V_c / F_N particles times the part
+    // of the cell outside the body, rounded stochastically from the seed;
+    // positions inside the body are drawn again
+    std::vector<float> frac;
+    int st = outside_fractions(h, frac);
+    if (st) return st;
+    const double ppc_f = c.part_per_cell ? (double)c.part_per_cell
+                                         : (double)c.density * h->cell_volume / c.fnum;
+    uint32_t kmax = 0;
+    for (uint32_t cell = 0; cell < h->cells; cell++) {
+      const double expect = ppc_f * frac[cell];
+      const double fl = std::floor(expect);
+      const uint32_t k = (uint32_t)fl + (unit_draw(mix) < expect - fl ? 1u : 0u);
+      slot[cell] = (uint32_t)n;
+      count[cell] = k;
+      kmax = std::max(kmax, k);
+      n += k;
+    }
+    ip.ppc = kmax;
+    ip.reject_inside = geo;
+    if (geo) {
+      ip.geom = base_params(h, c.dt).geom;
+      ip.cell_point = fill_point(h);
+    }
+  }
+  ip.kind = c.init_kind;
+  ip.vstd = std::sqrt(1.3806e-23f * c.temp / c.gas_mass);
+  ip.vstd2 = std::sqrt(1.3806e-23f * (c.init_temp2 > 0 ? c.init_temp2 : c.temp) / c.gas_mass);
+  ip.vmp = std::sqrt(2 * 1.3806e-23f * c.temp / c.gas_mass);
+  const float* sv = stream_vel ? stream_vel : c.stream_vel;
+  ip.stream = make_float3(sv[0], sv[1], sv[2]);
+  ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
+  return finish_fill(h, ip, slot, count, n, n_out);
+}
+
+int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out) {
+  if (!h || !fields5) return fail(h, DSMC_ERR_ARG, "null argument");
+  const dsmc_config& c = h->cfg;
+  std::vector<float> frac;
+  int st = outside_fractions(h, frac);
+  if (st) return st;
+  std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
+  std::vector<float4> state(h->cells);
+  std::vector<float2> maxrem(h->cells);
+  const bool geo = h->has_geom && c.geometry;
+  const float kb_m = 1.3806e-23f / c.gas_mass;
+  uint64_t mix = c.seed ^ 0x2545F4914F6CDD1Dull;
+  uint64_t n = 0;
+  uint32_t kmax = 0;
+  for (uint32_t cell = 0; cell < h->cells; cell++) {
+    const float* f = fields5 + 5 * (size_t)cell;
+    // n V_c / F_N particles in the part of the cell outside the body
+    const double expect = (std::isfinite(f[0]) && f[0] > 0.f)
+                              ? (double)f[0] * h->cell_volume / c.fnum * frac[cell] : 0.0;
+    const double fl = std::floor(expect);
+    const uint32_t k = (uint32_t)fl + (unit_draw(mix) < expect - fl ? 1u : 0u);
+    slot[cell] = (uint32_t)n;
+    count[cell] = k;
+    kmax = std::max(kmax, k);
+    n += k;
+    const float T = (std::isfinite(f[4]) && f[4] > 0.f) ? f[4] : c.temp;
+    state[cell] = make_float4(std::isfinite(f[1]) ? f[1] : 0.f, std::isfinite(f[2]) ? f[2] : 0.f,
+                              std::isfinite(f[3]) ? f[3] : 0.f, std::sqrt(kb_m * T));
+    // (sigma g)max scaled to the cell's temperature like the initial value
+    // (InitSimulationProperties, kernels/dsmc_kernel.cu:329-331)
+    maxrem[cell] = make_float2(h->max_rel_vel * std::sqrt(std::max(T, c.temp) / c.temp),
+                               (float)unit_draw(mix));
+  }
+  CK(h, cudaMemcpyAsync(fill_state(h), state.data(), h->cells * sizeof(float4), cudaMemcpyHostToDevice,
+                        h->stream), "seed upload");
+  CK(h, cudaMemcpyAsync(h->maxrem, maxrem.data(), h->cells * sizeof(float2), cudaMemcpyHostToDevice,
+                        h->stream), "seed upload");
+  dsmcb::InitParams ip{};
+  ip.ppc = kmax;
+  ip.kind = DSMC_INIT_MAXWELL;
+  ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
+  ip.cell_state = fill_state(h);
+  ip.reject_inside = geo;
+  if (geo) {
+    ip.geom = base_params(h, c.dt).geom;
+    ip.cell_point = fill_point(h);
+  }
+  return finish_fill(h, ip, slot, count, n, n_out);
 }
 
 int dsmc_upload_state(dsmc_handle* h, const float* pos, const float* vel, uint32_t n, int soa) {

@@ -288,6 +288,56 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
   return true;
 }
 
+// Whether o lies inside the closed mesh: parity of the triangles crossed by
+// the ray from o along a fixed direction off every axis, up to the grid's
+// boundary.  A crossing counts in the geometry cell whose stretch of the ray
+// holds it, so a triangle binned in several cells counts once.
+__device__ __forceinline__ bool inside_mesh(const GeomView& G, float3 o) {
+  const GridGeom& g = G.grid;
+  if (coll_cell_id(g, o) == kNone) return false;
+  const float da[3] = {0.80178373f, 0.53452248f, 0.26726124f};  // (3, 2, 1) / sqrt(14)
+  const float3 d = make_float3(da[0], da[1], da[2]);
+  const float oa[3] = {o.x, o.y, o.z};
+  const float lo[3] = {g.gmin.x, g.gmin.y, g.gmin.z};
+  const float cs[3] = {g.cell.x, g.cell.y, g.cell.z};
+  const int dm[3] = {(int)g.dim.x, (int)g.dim.y, (int)g.dim.z};
+  int idx[3];
+  float tmax[3], tdel[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int i = (int)floorf((oa[a] - lo[a]) / cs[a]);
+    idx[a] = min(max(i, 0), dm[a] - 1);
+    tmax[a] = (lo[a] + (idx[a] + 1) * cs[a] - oa[a]) / da[a];
+    tdel[a] = cs[a] / da[a];
+  }
+  float tcur = 0.f;
+  uint32_t crossings = 0;
+  const int max_iter = dm[0] + dm[1] + dm[2] + 3;
+  for (int it = 0; it < max_iter; it++) {
+    const uint32_t c = ((uint32_t)idx[2] * g.dim.y + (uint32_t)idx[1]) * g.dim.x + (uint32_t)idx[0];
+    const float texit = fminf(tmax[0], fminf(tmax[1], tmax[2]));
+    if (__ldg(&G.flags[c]) != 0) {
+      const uint2 se = __ldg(&G.start_end[c]);
+      for (uint32_t i = se.x; i < se.y; i++) {
+        const float4 A = __ldg(&G.tri[kTriStride * (size_t)i]);
+        const float4 B = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
+        const float4 C = __ldg(&G.tri[kTriStride * (size_t)i + 2]);
+        float t;
+        if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
+                                   make_float3(C.x, C.y, C.z), &t) &&
+            t > 0.f && t >= tcur && t < texit)
+          crossings++;
+      }
+    }
+    const int a = (tmax[0] <= tmax[1] && tmax[0] <= tmax[2]) ? 0 : (tmax[1] <= tmax[2] ? 1 : 2);
+    idx[a] += 1;
+    if (idx[a] >= dm[a]) break;
+    tcur = texit;
+    tmax[a] += tdel[a];
+  }
+  return (crossings & 1u) != 0;
+}
+
 // Diffuse re-emission about the unit normal n on the side the particle came
 // from (full accommodation at the wall temperature): normal speed from the
 // flux-weighted half-range Maxwellian, tangential components Gaussian.

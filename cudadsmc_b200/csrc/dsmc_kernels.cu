@@ -9,6 +9,8 @@
 // few bytes per particle.  All particle traffic is coalesced except the
 // scatter's writes, which land near-sorted because most particles stay in or
 // next to their cell between steps.
+#include <algorithm>
+
 #include "dsmc_step_dev.cuh"
 
 namespace dsmcb {
@@ -345,9 +347,24 @@ __global__ void k_init_fill(const InitParams p) {
     const float3 cellmin = make_float3(p.grid.gmin.x + cx * p.grid.cell.x,
                                        p.grid.gmin.y + cy * p.grid.cell.y,
                                        p.grid.gmin.z + cz * p.grid.cell.z);
-    const float px = cellmin.x + r.uniform() * p.grid.cell.x;
-    const float py = cellmin.y + r.uniform() * p.grid.cell.y;
-    const float pz = cellmin.z + r.uniform() * p.grid.cell.z;
+    float px = cellmin.x + r.uniform() * p.grid.cell.x;
+    float py = cellmin.y + r.uniform() * p.grid.cell.y;
+    float pz = cellmin.z + r.uniform() * p.grid.cell.z;
+    // a cell the mesh covers in part: positions inside the body are drawn
+    // again (at most 64 times), then the cell's known outside point is used
+    if (p.reject_inside) {
+      bool in = inside_mesh(p.geom, make_float3(px, py, pz));
+      for (int tries = 0; tries < 64 && in; tries++) {
+        px = cellmin.x + r.uniform() * p.grid.cell.x;
+        py = cellmin.y + r.uniform() * p.grid.cell.y;
+        pz = cellmin.z + r.uniform() * p.grid.cell.z;
+        in = inside_mesh(p.geom, make_float3(px, py, pz));
+      }
+      if (in && p.cell_point && p.cell_point[cell].w > 0.f) {
+        const float4 q = p.cell_point[cell];
+        px = q.x; py = q.y; pz = q.z;
+      }
+    }
     p.out.x[d] = px; p.out.y[d] = py; p.out.z[d] = pz;
     p.out.u[d] = vel.x; p.out.v[d] = vel.y; p.out.w[d] = vel.z;
   }
@@ -557,6 +574,60 @@ cudaError_t launch_sample_cells(const float* u, const float* v, const float* w,
                                 size_t fstride, size_t cstride, cudaStream_t stream) {
   const uint32_t grid = grid_for(cells, 256, 8);
   k_sample_cells<<<grid, 256, 0, stream>>>(u, v, w, start, cells, acc, fstride, cstride);
+  return cudaGetLastError();
+}
+
+// One warp per cell, two of the 4x4x4 sub-cell centres per lane.
+__global__ void k_outside_fraction(const GridGeom grid, const GeomView geom, uint32_t cells,
+                                   float* frac, float4* point) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t cell = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); cell < cells;
+       cell += warps) {
+    const uint32_t cx = cell % grid.dim.x, cy = (cell / grid.dim.x) % grid.dim.y,
+                   cz = cell / (grid.dim.x * grid.dim.y);
+    const float3 lo = make_float3(grid.gmin.x + cx * grid.cell.x, grid.gmin.y + cy * grid.cell.y,
+                                  grid.gmin.z + cz * grid.cell.z);
+    const bool near = lo.x <= geom.grid.gmax.x && lo.x + grid.cell.x >= geom.grid.gmin.x &&
+                      lo.y <= geom.grid.gmax.y && lo.y + grid.cell.y >= geom.grid.gmin.y &&
+                      lo.z <= geom.grid.gmax.z && lo.z + grid.cell.z >= geom.grid.gmin.z;
+    if (!near) {
+      if (lane == 0) {
+        frac[cell] = 1.f;
+        point[cell] = make_float4(lo.x + 0.5f * grid.cell.x, lo.y + 0.5f * grid.cell.y,
+                                  lo.z + 0.5f * grid.cell.z, 1.f);
+      }
+      continue;
+    }
+    bool out[2];
+    float3 q[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const uint32_t sidx = lane * 2u + (uint32_t)h;
+      q[h] = make_float3(lo.x + ((sidx & 3u) + 0.5f) * 0.25f * grid.cell.x,
+                         lo.y + (((sidx >> 2) & 3u) + 0.5f) * 0.25f * grid.cell.y,
+                         lo.z + ((sidx >> 4) + 0.5f) * 0.25f * grid.cell.z);
+      out[h] = !inside_mesh(geom, q[h]);
+    }
+    const unsigned m0 = __ballot_sync(0xffffffffu, out[0]);
+    const unsigned m1 = __ballot_sync(0xffffffffu, out[1]);
+    const uint32_t n_out = __popc(m0) + __popc(m1);
+    const int src = m0 ? __ffs(m0) - 1 : (m1 ? __ffs(m1) - 1 : 0);
+    const int which = m0 ? 0 : 1;
+    const float px = __shfl_sync(0xffffffffu, which ? q[1].x : q[0].x, src);
+    const float py = __shfl_sync(0xffffffffu, which ? q[1].y : q[0].y, src);
+    const float pz = __shfl_sync(0xffffffffu, which ? q[1].z : q[0].z, src);
+    if (lane == 0) {
+      frac[cell] = (float)n_out / 64.f;
+      point[cell] = make_float4(px, py, pz, n_out ? 1.f : 0.f);
+    }
+  }
+}
+
+cudaError_t launch_outside_fraction(const GridGeom& grid, const GeomView& geom, uint32_t cells,
+                                    float* frac, float4* point, cudaStream_t stream) {
+  const uint32_t blocks = (uint32_t)std::min<uint64_t>(((uint64_t)cells + 7) / 8, 8u * num_sms());
+  k_outside_fraction<<<blocks, 256, 0, stream>>>(grid, geom, cells, frac, point);
   return cudaGetLastError();
 }
 

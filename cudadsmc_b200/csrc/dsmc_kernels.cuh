@@ -174,9 +174,16 @@ struct InitParams {
   const uint32_t* cell_slot;  // per cell: first particle index, kNone = skipped cell
   const uint32_t* cell_count; // per cell: particles to fill (<= ppc)
   const float4* cell_state;   // optional per cell (u, v, w, sqrt(kT/m)) of the Maxwellian
+  int reject_inside;          // redraw positions that fall inside the mesh
+  GeomView geom;
+  const float4* cell_point;   // optional per cell: a point outside the mesh (w = 1) or none (w = 0)
   SoA out;
 };
 cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);
+// Fraction of every cell outside the mesh (64 stratified points per cell)
+// and one outside point per cell (w = 1; w = 0 if none was found).
+cudaError_t launch_outside_fraction(const GridGeom& grid, const GeomView& geom, uint32_t cells,
+                                    float* frac, float4* point, cudaStream_t stream);
 
 // Inflow injection: appends particles after the ones in cells and counts them
 // for the next scan.

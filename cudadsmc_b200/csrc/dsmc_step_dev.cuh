@@ -458,7 +458,11 @@ __device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, 
       if (!nearest_wall_hit(G, old_pos, d, dist, &t, &e)) break;
       const float4 P = __ldg(&G.tri[kTriStride * (size_t)e + 3]);
       const float3 n = make_float3(P.x, P.y, P.z);
-      const float side = (d.x * n.x + d.y * n.y + d.z * n.z) > 0.f ? -1.f : 1.f;
+      // the mesh is closed with outward normals: a face reached from its
+      // back side holds a particle inside the body (left over from a fill of
+      // a cell the body covers in part), which is removed
+      if ((d.x * n.x + d.y * n.y + d.z * n.z) > 0.f) return false;
+      const float side = 1.f;
       const float3 n_out = make_float3(side * n.x, side * n.y, side * n.z);
       const float3 hp = make_float3(old_pos.x + d.x * t + n_out.x * 1e-6f,
                                     old_pos.y + d.y * t + n_out.y * 1e-6f,

@@ -43,7 +43,8 @@ def test_energy_conserved(cuda, rng, density):
 def test_bimodal_relaxes_to_maxwellian(cuda, rng):
     # configs[0] of the workload list: argon VHS, 200 K + 600 K halves, 16^3 cells
     sol, n = box(1e20, rng=rng, omega=0.81, init="bimodal", temp=200.0, t2=600.0)
-    assert n == 98304
+    # n V / F_N = 24.41 per cell: the extension starts fill the fraction too
+    assert abs(n - 100000) < 300
     u0 = sol.DownloadState()[3:].astype(np.float64)
     k0 = np.mean(u0 ** 4, axis=1) / np.mean(u0 ** 2, axis=1) ** 2
     assert np.all(k0 > 3.5)  # mixture kurtosis 3.75

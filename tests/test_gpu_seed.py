@@ -1,0 +1,71 @@
+"""Initial states: the Maxwellian fill and the field-seeded fill keep
+particles out of the body, and the seeded fill follows the given per-cell
+density, drift and temperature."""
+import numpy as np
+import pytest
+
+from cudadsmc_b200 import DSMCSolver, mesh_icosphere, settings_t
+
+pytestmark = pytest.mark.gpu
+
+M_AR, D_AR, KB = 6.63e-26, 4.17e-10, 1.3806e-23
+C, R = np.array([0.4, 0.3, 0.3]), 0.1
+
+
+def solver(seed=3):
+    s = settings_t().set(grid_min=(0, 0, 0), grid_max=(1.2, 0.6, 0.6), grid_dim=(32, 16, 16),
+                         density=1e20, fnum=1e20 * (1.2 / 32) * (0.6 / 16) ** 2 / 10, temp=200.0,
+                         stream_vel=(1000.0, 0, 0), gas_mass=M_AR, gas_diam=D_AR, gas_tref=273.0,
+                         gas_omega=0.81, rng="philox", ntc_local=1, init_kind="maxwell", seed=seed,
+                         capacity_factor=3.0, wall_diffuse=1, wall_temp=300.0, geom_nearest=1)
+    sol = DSMCSolver().Init(s)
+    v, t = mesh_icosphere(3, R, tuple(C))
+    sol.SetModel(v, t, (16, 16, 16))
+    return sol
+
+
+def test_maxwellian_fill_keeps_out_of_the_body(cuda):
+    sol = solver()
+    n = sol.InitSystemState()
+    a = sol.DownloadState()
+    assert a.shape[1] == n
+    r = np.linalg.norm(a[:3].T - C, axis=1)
+    # the icosphere's facets lie within 1 % of the sphere; redrawn positions
+    # leave at most a few particles inside cells the body covers almost fully
+    assert np.sum(r < R * 0.99) <= 1e-3 * n
+    # a particle reaching a face from inside is removed at that step
+    sol.RunSimulationStep(2e-6, 80)
+    a = sol.DownloadState()
+    r = np.linalg.norm(a[:3].T - C, axis=1)
+    assert np.sum(r < R * 0.99) == 0
+    sol.close()
+
+
+def test_field_seeding(cuda):
+    sol = solver()
+    dims = (32, 16, 16)
+    cells = dims[0] * dims[1] * dims[2]
+    z, y, x = np.meshgrid(np.arange(dims[2]), np.arange(dims[1]), np.arange(dims[0]), indexing="ij")
+    x = x.reshape(-1)
+    f = np.zeros((cells, 5), np.float32)
+    f[:, 0] = 1e20 * (1 + x / 16.0)                     # density rising along x
+    f[:, 1] = 500.0 + 20.0 * x                          # drift along x
+    f[:, 4] = 300.0                                     # temperature
+    n = sol.InitFromFields(f)
+    a = sol.DownloadState()
+    assert a.shape[1] == n
+    info = sol.Info()
+    expect = np.sum(f[:, 0]) * info.cell_volume / sol.settings.cfg.fnum
+    assert abs(n / expect - 1) < 0.02  # the covered cells are left out
+    r = np.linalg.norm(a[:3].T - C, axis=1)
+    assert np.sum(r < R * 0.99) <= 1e-3 * n
+    cx = np.minimum((a[0] / (1.2 / 32)).astype(int), 31)
+    for col in (2, 16, 29):
+        sel = cx == col
+        assert abs(a[3, sel].mean() - (500 + 20 * col)) < 30
+        T = M_AR * np.var(a[4, sel]) / KB
+        assert abs(T / 300 - 1) < 0.1
+    # the seeded state steps
+    sol.RunSimulationStep(2e-6, 5)
+    sol.Sync()
+    sol.close()
