@@ -52,7 +52,7 @@ def wl_capsule_4m():
              face_kind={"-x": "inflow", "+x": "outflow", "-y": "outflow", "+y": "outflow",
                         "-z": "outflow", "+z": "outflow"}, **ARGON)
     mesh = dict(kind="capsule", nose_radius=0.15, cone_deg=20.0, length=0.26,
-                nose_center=(0.35 + 0.15, 0.3, 0.3), ntarget=20000, seed=7, grid=(24, 32, 32))
+                nose_center=(0.35 + 0.15, 0.3, 0.3), ntarget=20000, seed=7, grid=(48, 64, 64))
     return dict(name="capsule_mach7_argon_4M_128x64x64", settings=s, mesh=mesh,
                 desc=f"argon VHS w=0.81, Mach {mach:.0f} (U={U:.0f} m/s), T=200 K, n=1e20, "
                      "diffuse capsule wall 500 K (nose r=0.15 m, 20 deg cone, ~20k tris), "

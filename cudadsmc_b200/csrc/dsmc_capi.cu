@@ -20,7 +20,7 @@ struct dsmc_handle {
   cudaStream_t stream = nullptr;
 
   uint32_t ppc = 0, cells = 0, capacity = 0, n_scan_tiles = 0, n_tiles = 0, cells_per_tile = 0;
-  int variant = 2;  // cell-kernel variant (dsmc_set_kernel_variant)
+  int variant = 5;  // cell-kernel variant (dsmc_set_kernel_variant)
   float cell_size[3]{}, cell_volume = 0.f, cross_section = 0.f, max_rel_vel = 0.f;
   float vhs_gref = 0.f;
   GridGeom grid{};
@@ -46,6 +46,7 @@ struct dsmc_handle {
   float* gclear = nullptr;
   uint2* gse = nullptr;
   float4* gtri = nullptr;
+  float4* gplane = nullptr;
 
   bool has_state = false;
   uint64_t step = 0;
@@ -100,12 +101,14 @@ void drop_graph(dsmc_handle* h) {
 }
 
 // Cell-kernel variant and the tile size that goes with it: tiles of about one
-// shared-memory chunk of particles (32..256 cells).
+// shared-memory chunk of particles (32..256 cells); the warp-autonomous
+// variants use tiles of 32 cells, one per lane.
 void apply_variant(dsmc_handle* h, int v) {
   h->variant = v;
   const uint64_t cap = (uint64_t)dsmcb::cell_kernel_chunk_capacity(v);
   uint32_t ct = dsmcb::kMaxCellsPerTile;
   while (ct > 32 && (uint64_t)ct * std::max<uint32_t>(h->ppc, 1) > cap) ct >>= 1;
+  if (dsmcb::cell_kernel_is_warp(v)) ct = dsmcb::cell_kernel_w_tile();
   h->cells_per_tile = ct;
   h->n_tiles = (h->cells + ct - 1) / ct;
   drop_graph(h);
@@ -136,7 +139,7 @@ void free_all(dsmc_handle* h) {
     h->A[i] = h->B[i] = nullptr;
   }
   void* ps[] = {h->orig, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
-                h->acc, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse, h->gtri};
+                h->acc, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse, h->gtri, h->gplane};
   for (void* p : ps) cudaFree(p);
 }
 
@@ -166,6 +169,11 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
   p.hard_sphere = std::fabs(h->cfg.gas_omega - 0.5f) < 1e-9f;
   p.vhs_exp = 2.f * h->cfg.gas_omega - 1.f;
   p.vhs_gref = h->vhs_gref;
+  if (!p.hard_sphere && h->vhs_gref > 0.f && h->cross_section > 0.f) {
+    const double e = 2.0 * (double)h->cfg.gas_omega - 1.0;
+    p.vhs_c1 = (float)(1.0 - e);
+    p.vhs_c0 = (float)(std::log2((double)h->cross_section) + e * std::log2((double)h->vhs_gref));
+  }
   p.ntc_local = h->cfg.ntc_local;
   p.rng_kind = h->cfg.rng;
   p.seed = make_uint2((uint32_t)h->cfg.seed, (uint32_t)(h->cfg.seed >> 32));
@@ -184,6 +192,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.flags = h->gflags;
     p.geom.start_end = h->gse;
     p.geom.tri = h->gtri;
+    p.geom.plane = h->gplane;
     p.geom.clear = h->gclear;
     p.geom.diffuse = h->cfg.wall_diffuse;
     p.geom.nearest = h->cfg.geom_nearest;
@@ -241,20 +250,25 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
                               h->n_scan_tiles, h->meta, 1, h->stream);
   });
   if (e) return e;
+  // the split cell kernels gather the state through orig themselves; the
+  // fused one reads it scattered into B
+  const bool split = dsmcb::cell_kernel_is_warp(h->variant);
   e = timed(h, 1, [&] {
-    return dsmcb::launch_scatter(soa_of(h->A), soa_of(h->B), h->keys, h->start, h->cursor, h->orig,
-                                 h->cells, h->tile_sum, h->n_scan_tiles, h->meta, h->capacity,
-                                 h->stream);
+    return dsmcb::launch_scatter(!split, soa_of(h->A), soa_of(h->B), h->keys, h->start, h->cursor,
+                                 h->orig, h->cells, h->tile_sum, h->n_scan_tiles, h->meta,
+                                 h->capacity, h->stream);
   });
   if (e) return e;
   dsmcb::StepParams p = base_params(h, dt);
-  p.in = soa_of(h->B);
+  p.in = split ? soa_of(h->A) : soa_of(h->B);
+  p.mid = soa_of(h->B);
   p.in_orig = h->orig;
   p.out = soa_of(h->A);
   p.out_key = h->keys;
   p.flags = dsmcb::kDoFixup | dsmcb::kDoCollide | dsmcb::kDoMove | dsmcb::kDoKeys | dsmcb::kPadded;
   if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
   p.cell_variant = h->variant;
+  p.defer_list = h->orig;
   e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
   if (e) return e;
   for (const auto& in : h->inflows) {
@@ -591,6 +605,7 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
   std::vector<uint2> se(gc);
   const size_t stride = dsmcb::kTriStride;
   std::vector<float4> tri(stride * (g.tri_ids.size() + 1));
+  std::vector<float4> plane(g.tri_ids.size() + 1);
   size_t off = 0;
   for (uint32_t c = 0; c < gc; c++) {
     flags[c] = g.flags[c];
@@ -612,8 +627,8 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
                       e1[0] * e2[1] - e1[1] * e2[0]};
       double l = std::sqrt(pn[0] * pn[0] + pn[1] * pn[1] + pn[2] * pn[2]);
       if (l > 0) { pn[0] /= l; pn[1] /= l; pn[2] /= l; }
-      tri[stride * (off + k) + 3] = make_float4((float)pn[0], (float)pn[1], (float)pn[2],
-                                                (float)(pn[0] * a[0] + pn[1] * a[1] + pn[2] * a[2]));
+      plane[off + k] = make_float4((float)pn[0], (float)pn[1], (float)pn[2],
+                                   (float)(pn[0] * a[0] + pn[1] * a[1] + pn[2] * a[2]));
     }
     off += g.count[c];
   }
@@ -647,15 +662,20 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
   cudaFree(h->gclear);
   cudaFree(h->gse);
   cudaFree(h->gtri);
+  cudaFree(h->gplane);
   h->gflags = nullptr; h->gclear = nullptr; h->gse = nullptr; h->gtri = nullptr;
+  h->gplane = nullptr;
   CK(h, dalloc(&h->gflags, gc), "geometry alloc");
   CK(h, dalloc(&h->gclear, gc), "geometry alloc");
   CK(h, dalloc(&h->gse, gc), "geometry alloc");
   CK(h, dalloc(&h->gtri, tri.size()), "geometry alloc");
+  CK(h, dalloc(&h->gplane, plane.size()), "geometry alloc");
   CK(h, cudaMemcpy(h->gflags, flags.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
   CK(h, cudaMemcpy(h->gclear, clear.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
   CK(h, cudaMemcpy(h->gse, se.data(), gc * sizeof(uint2), cudaMemcpyHostToDevice), "geometry upload");
   CK(h, cudaMemcpy(h->gtri, tri.data(), tri.size() * sizeof(float4), cudaMemcpyHostToDevice),
+     "geometry upload");
+  CK(h, cudaMemcpy(h->gplane, plane.data(), plane.size() * sizeof(float4), cudaMemcpyHostToDevice),
      "geometry upload");
   h->has_geom = true;
   h->cfg.geometry = 1;
@@ -1055,6 +1075,8 @@ int dsmc_set_kernel_variant(dsmc_handle* h, int variant) {
   apply_variant(h, variant);
   return DSMC_OK;
 }
+
+int dsmc_kernel_variant_count(void) { return dsmcb::cell_kernel_variants(); }
 
 int dsmc_get_kernel_variant(dsmc_handle* h, int* variant, int* chunk_capacity) {
   if (!h) return DSMC_ERR_ARG;

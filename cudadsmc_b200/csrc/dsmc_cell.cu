@@ -17,6 +17,7 @@
 // overlap them.  The (threads, capacity) variant is chosen at run time.
 // Algorithmic traffic per particle: 28 B read (state + orig), 28 B written
 // (state + key), plus about 24-56 B per cell of collision state.
+#include "dsmc_bulk.cuh"
 #include "dsmc_step_dev.cuh"
 
 namespace dsmcb {
@@ -26,7 +27,6 @@ using namespace dev;
 
 constexpr int kCellArr = kMaxCellsPerTile + 4;   // float2 per-cell slots (+ slack)
 constexpr int kLsArr = kMaxCellsPerTile + 8;
-constexpr uint32_t kHeavyMin = 8;                // selections that make a cell dense
 
 struct Chunk {
   uint32_t tile, c0, nct, cur, k, base, n;
@@ -75,50 +75,6 @@ struct __align__(128) CellSmem {
 template <int CAP>
 constexpr size_t smem_bytes(uint32_t n_scan_tiles) {
   return ((sizeof(CellSmem<CAP>) + 15) & ~(size_t)15) + 4 * (size_t)n_scan_tiles;
-}
-
-// ------------------------------------------------------ bulk copy / mbar ----
-
-__device__ __forceinline__ uint32_t smem_u32(const void* ptr) {
-  return (uint32_t)__cvta_generic_to_shared(ptr);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* m, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
-                                         unsigned long long* m) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(m))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* m, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(m)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Waits for an mbarrier phase for at most about a second.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* m, uint32_t parity) {
-  if (mbar_try_wait(m, parity)) return true;
-  const uint64_t t0 = global_ns();
-  while (!mbar_try_wait(m, parity)) {
-    if (global_ns() - t0 > 1000000000ull) return false;
-  }
-  return true;
 }
 
 // --------------------------------------------------------------- chunks ----
@@ -200,7 +156,7 @@ __device__ void issue_chunk(const StepParams& p, CellSmem<CAP>& S, const Chunk& 
   unsigned long long* m = &S.mbar[c.buf];
   if (lane == 0) mbar_expect_tx(m, pbytes * narr + mbytes + sbytes);
   __syncwarp();
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  fence_proxy_async();
   const int first = vel_only ? 3 : 0;
   if (lane < narr) {
     const int a = first + (int)lane;
@@ -247,7 +203,7 @@ __device__ void issue_ls(const StepParams& p, CellSmem<CAP>& S, uint32_t tile, i
   const uint32_t ct = (uint32_t)p.cells_per_tile;
   const uint32_t nct = min(ct, p.cells - tile * ct);
   const uint32_t whole = (p.flags & kPadded) ? ((nct + 1u + 3u) & ~3u) : ((nct + 1u) & ~3u);
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  fence_proxy_async();
   mbar_expect_tx(&S.mbar_ls[b], whole * 4u);
   if (whole) bulk_g2s(S.ls[b], p.start + tile * ct, whole * 4u, &S.mbar_ls[b]);
 }
@@ -263,7 +219,7 @@ __device__ void finish_ls(const StepParams& p, CellSmem<CAP>& S, uint32_t tile, 
 
 // A cell too large for the shared-memory chunk: processed by the whole block
 // directly in the output arrays.
-__device__ void giant_cell(const StepParams& p, uint32_t cell, uint32_t s, uint32_t e,
+static __device__ __noinline__ void giant_cell(const StepParams& p, uint32_t cell, uint32_t s, uint32_t e,
                            uint32_t step, bool do_sample, uint32_t* s_tile, uint32_t& sel,
                            uint32_t& col, double& sum_g, uint32_t& removed) {
   __shared__ double red[4][32];
@@ -360,7 +316,7 @@ __device__ void giant_cell(const StepParams& p, uint32_t cell, uint32_t s, uint3
 // ---------------------------------------------------------------- kernel ----
 
 template <int THREADS, int CAP, int MINB>
-__global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
+__global__ void __launch_bounds__(THREADS, MINB) k_cell(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   CellSmem<CAP>& S = *reinterpret_cast<CellSmem<CAP>*>(smem_raw);
   uint32_t* s_tile = reinterpret_cast<uint32_t*>(smem_raw + ((sizeof(CellSmem<CAP>) + 15) & ~(size_t)15));
@@ -391,7 +347,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
     mbar_init(&S.mbar_ls[0], 1);
     mbar_init(&S.mbar_ls[1], 1);
     mbar_init(&S.mbar_ls[2], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_mbar_init();
     S.cur.valid = 0;
     if (blockIdx.x < p.n_tiles) issue_ls(p, S, blockIdx.x, 0);
   }
@@ -581,7 +537,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_cell(const StepParams p) {
           const uint32_t g = base + q;
           bool live = true;
           if (go) {
-            if (p.flags & kDoMove) live = move_particle(p, pos, vel, g, step);
+            // pass 0 flies only paths that cannot reach the body
+            if (p.flags & kDoMove)
+              live = pass == 0 ? move_free(p, pos, vel, g, step) : move_particle(p, pos, vel, g, step);
             if (do_sample) { U[j] = vel.x; V[j] = vel.y; W[j] = vel.z; }
             if (!vel_only) { p.out.x[g] = pos.x; p.out.y[g] = pos.y; p.out.z[g] = pos.z; }
             p.out.u[g] = vel.x; p.out.v[g] = vel.y; p.out.w[g] = vel.z;
@@ -667,14 +625,22 @@ cudaError_t launch_variant(const StepParams& p, cudaStream_t stream) {
 
 }  // namespace
 
-int cell_kernel_variants() { return 4; }
+// Variants 0-3: the CTA-wide kernel above; 4-7: the warp-autonomous kernel
+// (dsmc_cellw.cu), which handles the full step with padded buffers (the
+// collide stage, kVelOnly on caller buffers, always runs the CTA-wide one).
+int cell_kernel_variants() { return 4 + cell_kernel_w_variants(); }
 
 int cell_kernel_chunk_capacity(int variant) {
   static const int caps[4] = {2048, 1024, 512, 256};
-  return caps[variant < 0 || variant > 3 ? 2 : variant];
+  if (variant >= 4) return cell_kernel_w_capacity(variant - 4);
+  return caps[variant < 0 ? 2 : variant];
 }
 
+bool cell_kernel_is_warp(int variant) { return variant >= 4; }
+
 cudaError_t launch_cell(const StepParams& p, cudaStream_t stream) {
+  if (p.cell_variant >= 4 && (p.flags & kPadded) && !(p.flags & kVelOnly))
+    return launch_cell_w(p, p.cell_variant - 4, stream);
   switch (p.cell_variant) {
     case 0: return launch_variant<512, 2048, 1>(p, stream);
     case 1: return launch_variant<256, 1024, 2>(p, stream);

@@ -1,0 +1,633 @@
+// The timestep's cell work as two warp-autonomous kernels (sm_100a).
+//
+// Both kernels hand out tiles of 32 consecutive cells to warps (lane L owns
+// cell L of a tile; tiles past the first wave come from a dynamic counter),
+// and neither has a CTA-wide barrier inside its loop.
+//
+// k_collide_w (order + collisions): a tile is cut into chunks of whole cells
+// holding at most CAPW particles.  The particle arrays of a chunk (x, y, z,
+// u, v, w, orig) are staged in the warp's slice of shared memory by 1-D bulk
+// copies completing on the warp's mbarrier, double buffered (the copy of the
+// next chunk is in flight while the current one is processed):
+//   A  cell of each staged particle; rank by orig inside the cell (the stable
+//      order of the reference's sort)
+//   B  NTC collisions: light cells one lane each, dense cells (Philox mode)
+//      one whole warp each
+//   C  the chunk back to global memory in sorted order
+// k_flight_w (flight + keys): streams the tile's particles, 32 at a time:
+// free flight and boundaries, next-step key and count (warp-aggregated
+// atomics on the per-cell counts and the per scan tile totals, so the kernel
+// has no CTA-wide barrier at all).  Flights that may reach the body are
+// listed instead: they cluster in the tiles next to the body, so
+// k_mesh_w flies them afterwards one per thread over the whole GPU.
+// k_sample_w then samples (FP64) on sampling steps.
+//
+// The per-cell and per-particle arithmetic is that of the fused CTA-wide
+// kernel (dsmc_cell.cu), in the same order, so both compute the same step for
+// every cell that fits a chunk; the split only costs one more pass over the
+// state (24 B written + 24 B read per particle) and lets each kernel run at
+// its own register budget and occupancy.
+//
+// Traffic per particle: k_collide_w 28 B read (state + orig) + 24 B written;
+// k_flight_w 24 B read + 28 B written (state + key).  Per cell: 8 B of starts
+// per kernel, 16 B ((sigma g)max read + write), 32 B more in the reference
+// RNG mode, 80 B on sampling steps.
+#include "dsmc_bulk.cuh"
+#include "dsmc_step_dev.cuh"
+
+namespace dsmcb {
+namespace {
+
+using namespace dev;
+
+constexpr uint32_t kWarpTile = 32;  // cells per warp tile, one per lane
+constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach the body
+
+template <int CAPW>
+struct __align__(16) WarpSmem {
+  float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
+  uint4 seeds[kWarpTile];      // HybridTaus states (reference RNG mode)
+  float2 mr[kWarpTile];        // (sigma g)max, NTC remainder
+  uint32_t claim[CAPW];        // pair claims inside a dense cell
+  uint32_t cs[kWarpTile + 1];  // chunk-relative start of each tile cell
+  unsigned long long mbar[2];
+  uint16_t slot[CAPW];         // sorted position -> staged index
+  uint8_t cellof[CAPW];        // tile cell (lane) of each staged particle
+};
+
+template <int CAPW, int WARPS>
+constexpr size_t collide_smem_bytes() {
+  return WARPS * sizeof(WarpSmem<CAPW>);
+}
+
+// A tile of 32 cells as the lanes see it: lane L holds the start and end of
+// cell 32 t + L (cells past the last one are empty at the total count).
+struct WTile {
+  uint32_t t, nct, s, e;
+};
+
+__device__ __forceinline__ WTile load_tile(const StepParams& p, uint32_t t) {
+  WTile w;
+  w.t = t;
+  w.nct = 0;
+  w.s = w.e = 0;
+  if (t < p.n_tiles) {
+    const uint32_t c0 = t * kWarpTile;
+    const uint32_t c = c0 + lane_id();
+    w.nct = min(kWarpTile, p.cells - c0);
+    w.s = __ldg(&p.start[min(c, p.cells)]);
+    w.e = __ldg(&p.start[min(c + 1u, p.cells)]);
+  }
+  return w;
+}
+
+// Tiles of a warp: tile w first, then from the step's dynamic counter (or
+// round robin without one).  Lane 0 asks ahead of need so that the atomic's
+// latency is hidden.
+struct TileQueue {
+  uint32_t nwarps, next_static;
+  uint32_t* counter;
+  __device__ __forceinline__ uint32_t grab() {
+    if (counter) return nwarps + atomicAdd(counter, 1u);
+    const uint32_t t = next_static;
+    next_static += nwarps;
+    return t;
+  }
+};
+
+// Chunk of a tile: cells [cur, cur + k) holding particles [base, base + n).
+struct WChunk {
+  uint32_t cur, k, base, n;
+  int buf, giant, valid;
+};
+
+// As many whole cells from `cur` as fit CAPW particles (a single cell that
+// does not fit is a giant chunk).  Warp-uniform; cur < T.nct.
+template <int CAPW>
+__device__ __forceinline__ WChunk make_wchunk(const WTile& T, uint32_t cur, int buf) {
+  WChunk c;
+  c.cur = cur;
+  c.buf = buf;
+  c.valid = 1;
+  const uint32_t lane = lane_id();
+  c.base = __shfl_sync(kFull, T.s, cur);
+  // ends grow with the lane: the cells that fit are a prefix from cur
+  const bool fits = lane >= cur && lane < T.nct && T.e - c.base <= (uint32_t)CAPW;
+  const uint32_t k = __popc(__ballot_sync(kFull, fits));
+  c.giant = k == 0;
+  c.k = k == 0 ? 1u : k;
+  c.n = __shfl_sync(kFull, T.e, cur + c.k - 1u) - c.base;
+  return c;
+}
+
+// Bulk copy of a chunk's orig (the pre-scatter index of every sorted slot)
+// into buffer c.buf.  The library's buffers carry 16 bytes of slack, so the
+// whole 16-byte aligned cover of [base, base + n) is copied (at most CAPW + 6
+// elements).
+template <int CAPW>
+__device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>& S, const WChunk& c) {
+  const uint32_t ia = c.base & ~3u, ib = (c.base + c.n + 3u) & ~3u;
+  const uint32_t bytes = (ib - ia) * 4u;
+  const uint32_t lane = lane_id();
+  if (lane == 0) mbar_expect_tx(&S.mbar[c.buf], bytes);
+  __syncwarp();
+  if (lane == 0) {
+    fence_proxy_async();
+    bulk_g2s(S.part[c.buf][6], p.in_orig + ia, bytes, &S.mbar[c.buf]);
+  }
+}
+
+// A cell too large for a chunk: the warp gathers it in sorted order into the
+// mid arrays in global memory and one lane collides it there.
+static __device__ __noinline__ void giant_collide_warp(const StepParams& p, uint32_t cell,
+                                                       uint32_t s, uint32_t e, uint32_t step,
+                                                       uint32_t& sel, uint32_t& col,
+                                                       double& sum_g) {
+  const uint32_t n = e - s;
+  const uint32_t lane = lane_id();
+  if (lane == 0 && p.meta) atomicAdd(&p.meta->giant_cells, 1u);
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t my = p.in_orig[s + i];
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < n; j++) rank += (uint32_t)(p.in_orig[s + j] < my);
+    const uint32_t d = s + rank;
+    p.mid.x[d] = p.in.x[my]; p.mid.y[d] = p.in.y[my]; p.mid.z[d] = p.in.z[my];
+    p.mid.u[d] = p.in.u[my]; p.mid.v[d] = p.in.v[my]; p.mid.w[d] = p.in.w[my];
+  }
+  __syncwarp();
+  if ((p.flags & kDoCollide) && lane == 0) {
+    GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, s};
+    CellState st{p.maxrem + cell, p.seeds ? p.seeds + cell : nullptr,
+                 p.stat4 ? p.stat4 + cell : nullptr};
+    collide_cell(p, cell, (int)n, acc, step, st, sel, col, sum_g);
+  }
+  __syncwarp();
+}
+
+// ------------------------------------------------------ order + collide ----
+
+template <int CAPW, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_constant__ StepParams p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  WarpSmem<CAPW>& S = reinterpret_cast<WarpSmem<CAPW>*>(smem_raw)[warp];
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const bool do_fixup = (p.flags & kDoFixup) != 0;
+  const bool do_collide = (p.flags & kDoCollide) != 0;
+  const bool taus = p.rng_kind == 0;
+  const bool heavy_mode = !taus && do_collide;
+  for (uint32_t t = lane; t < (uint32_t)CAPW; t += 32) S.claim[t] = 0xffffffffu;
+  if (lane == 0) {
+    mbar_init(&S.mbar[0], 1);
+    mbar_init(&S.mbar[1], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+
+  const uint32_t nwarps = gridDim.x * WARPS;
+  const uint32_t gw = blockIdx.x * WARPS + warp;
+  TileQueue tq{nwarps, gw + nwarps, p.meta ? &p.meta->tile_next : nullptr};
+  WTile A = load_tile(p, gw);
+  uint32_t pend = 0, tb = 0;
+  if (lane == 0 && gw < p.n_tiles) {
+    tb = tq.grab();
+    pend = tq.grab();
+  }
+  tb = __shfl_sync(kFull, gw < p.n_tiles ? tb : 0xffffffffu, 0);
+  WTile B = load_tile(p, tb);
+
+  uint32_t phase = 0;  // bit b: parity of the next phase of buffer b
+  uint32_t sel = 0, col = 0;
+  double sum_g = 0.0;
+  WChunk C;
+  C.valid = 0;
+  if (A.t < p.n_tiles) {
+    C = make_wchunk<CAPW>(A, 0, 0);
+    if (!C.giant && C.n) issue_wchunk(p, S, C);
+  }
+
+  while (C.valid) {
+    // the chunk after this one, and its copy into the other buffer
+    WChunk N;
+    N.valid = 0;
+    bool n_in_b = false;
+    if (C.cur + C.k < A.nct) {
+      N = make_wchunk<CAPW>(A, C.cur + C.k, C.buf ^ 1);
+    } else if (B.t < p.n_tiles) {
+      N = make_wchunk<CAPW>(B, 0, C.buf ^ 1);
+      n_in_b = true;
+    }
+    const bool n_copy = N.valid && !N.giant && N.n;
+    if (n_copy) issue_wchunk(p, S, N);
+
+    const uint32_t c0 = A.t * kWarpTile;
+    const uint32_t cell = c0 + lane;
+    const bool mine = lane >= C.cur && lane < C.cur + C.k;
+    const uint32_t s0 = A.s - C.base, nc = A.e - A.s;  // meaningful for `mine`
+    if (!C.giant && C.n) {
+      if (do_collide && mine) {
+        S.mr[lane] = p.maxrem[cell];
+        if (taus) S.seeds[lane] = p.seeds[cell];
+      }
+      S.cs[lane] = s0;
+      if (lane == 31) S.cs[32] = A.e - C.base;
+      const uint32_t par = (phase >> C.buf) & 1u;
+      bool ok = mbar_wait_bounded(&S.mbar[C.buf], par);
+      phase ^= 1u << C.buf;
+      if (!__all_sync(kFull, ok)) {
+        if (lane == 0 && p.meta) atomicOr(&p.meta->error, kErrTimeout);
+        // this chunk's and the next chunk's copies may still be in flight:
+        // let them land (again bounded) before the shared memory goes away
+        mbar_wait_bounded(&S.mbar[C.buf], par);
+        if (n_copy) mbar_wait_bounded(&S.mbar[N.buf], (phase >> N.buf) & 1u);
+        break;
+      }
+    }
+    __syncwarp();
+
+    if (C.giant) {
+      giant_collide_warp(p, c0 + C.cur, C.base, C.base + C.n, step, sel, col, sum_g);
+    } else if (C.n > 0) {
+      const uint32_t off = C.base & 3u;
+      float* X = S.part[C.buf][0] + off;
+      float* Y = S.part[C.buf][1] + off;
+      float* Z = S.part[C.buf][2] + off;
+      float* U = S.part[C.buf][3] + off;
+      float* V = S.part[C.buf][4] + off;
+      float* W = S.part[C.buf][5] + off;
+      const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][6] + off);
+      const uint32_t base = C.base, n = C.n;
+      // A0: gather of the chunk's state through orig (asynchronous 4-byte
+      // copies, in flight while the order is restored)
+      for (uint32_t t = lane; t < n; t += 32) {
+        const uint32_t i = OR[t];
+        cp_async4(X + t, p.in.x + i);
+        cp_async4(Y + t, p.in.y + i);
+        cp_async4(Z + t, p.in.z + i);
+        cp_async4(U + t, p.in.u + i);
+        cp_async4(V + t, p.in.v + i);
+        cp_async4(W + t, p.in.w + i);
+      }
+      // A1: cell of each staged particle; dense cells
+      if (do_fixup && mine)
+        for (uint32_t j = s0; j < s0 + nc; j++) S.cellof[j] = (uint8_t)lane;
+      bool heavy = false;
+      if (heavy_mode && mine && nc >= 2)
+        heavy = (uint32_t)ntc_fpc_fast(p, nc, S.mr[lane]) >= kHeavyMin;
+      const unsigned heavy_mask = __ballot_sync(kFull, heavy);
+      __syncwarp();
+      // A2: slot[sorted position] = staged index, sorted = (cell, orig).  The
+      // origs are distinct, so a particle's rank in its cell is the number of
+      // smaller origs there, counted four at a time from the 16-byte aligned
+      // staging row (element j sits at ORA[j + off]).
+      const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][6]);
+      for (uint32_t t = lane; t < n; t += 32) {
+        if (!do_fixup) {
+          S.slot[t] = (uint16_t)t;
+          continue;
+        }
+        const uint32_t lc = S.cellof[t];
+        const uint32_t a = S.cs[lc], b = S.cs[lc + 1];
+        const uint32_t my = OR[t];
+        const uint32_t lo = a + off, hi = b + off;
+        uint32_t rank = 0;
+        for (uint32_t jj = lo & ~3u; jj < hi; jj += 4) {
+          const uint4 o = *reinterpret_cast<const uint4*>(ORA + jj);
+          if (jj >= lo && jj + 4u <= hi) {
+            rank += (uint32_t)(o.x < my) + (uint32_t)(o.y < my) + (uint32_t)(o.z < my) +
+                    (uint32_t)(o.w < my);
+          } else {
+            rank += (uint32_t)(jj >= lo && o.x < my) +
+                    (uint32_t)(jj + 1u >= lo && jj + 1u < hi && o.y < my) +
+                    (uint32_t)(jj + 2u >= lo && jj + 2u < hi && o.z < my) +
+                    (uint32_t)(jj + 3u < hi && o.w < my);
+          }
+        }
+        S.slot[a + rank] = (uint16_t)t;
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      // B: collisions; light cells one lane each, dense cells one warp each
+      if (do_collide) {
+        if (mine && !heavy) {
+          SmemVel acc{U, V, W, S.slot, s0};
+          CellState st{&S.mr[lane], taus ? &S.seeds[lane] : nullptr,
+                       p.stat4 ? p.stat4 + cell : nullptr};
+          collide_cell(p, cell, (int)nc, acc, step, st, sel, col, sum_g);
+        }
+        __syncwarp();
+        for (unsigned hm = heavy_mask; hm; hm &= hm - 1u) {
+          const uint32_t lc = (uint32_t)__ffs(hm) - 1u;
+          const uint32_t a = S.cs[lc], b = S.cs[lc + 1];
+          SmemVel acc{U, V, W, S.slot, a};
+          CellState st{&S.mr[lc], nullptr, p.stat4 ? p.stat4 + c0 + lc : nullptr};
+          ntc_heavy_warp(p, c0 + lc, b - a, acc, S.claim, step, st, sel, col, sum_g);
+          __syncwarp();
+        }
+        if (mine) {
+          p.maxrem[cell] = S.mr[lane];
+          if (taus) p.seeds[cell] = S.seeds[lane];
+        }
+      }
+      // C: the chunk in sorted order
+      for (uint32_t q = lane; q < n; q += 32) {
+        const uint32_t j = S.slot[q], g = base + q;
+        p.mid.x[g] = X[j]; p.mid.y[g] = Y[j]; p.mid.z[g] = Z[j];
+        p.mid.u[g] = U[j]; p.mid.v[g] = V[j]; p.mid.w[g] = W[j];
+      }
+    }
+    __syncwarp();
+    if (n_in_b) {
+      A = B;
+      const uint32_t t2 = __shfl_sync(kFull, pend, 0);
+      B = load_tile(p, t2);
+      if (lane == 0 && t2 < p.n_tiles) pend = tq.grab();
+    }
+    C = N;
+  }
+  const unsigned long long s64 = warp_sum((unsigned long long)sel);
+  const unsigned long long c64 = warp_sum((unsigned long long)col);
+  const double g = warp_sum(sum_g);
+  if (lane == 0 && p.meta) {
+    if (s64) atomicAdd(&p.meta->selections, s64);
+    if (c64) atomicAdd(&p.meta->collisions, c64);
+    if (g != 0.0) atomicAdd(&p.meta->sum_g, g);
+  }
+}
+
+// ------------------------------------------------ flight + keys + sample ----
+
+// Next-step key and count of a flown particle (all lanes; `go`: this lane
+// flew one), its state stored at g.
+__device__ __forceinline__ void finish_flight(const StepParams& p, bool go, bool live, uint32_t g,
+                                              float3 pos, float3 vel, uint32_t& removed) {
+  if (go) {
+    p.out.x[g] = pos.x; p.out.y[g] = pos.y; p.out.z[g] = pos.z;
+    p.out.u[g] = vel.x; p.out.v[g] = vel.y; p.out.w[g] = vel.z;
+  }
+  if (p.flags & kDoKeys) {
+    const bool has_key = go && live;
+    const unsigned m = __ballot_sync(kFull, has_key);
+    if (go && !live) removed++;
+    if (has_key) {
+      const uint32_t key = cell_id3d(p.grid, pos.x, pos.y, pos.z);
+      warp_count_key_global(p.count, key, m, p.tile_sum);
+      p.out_key[g] = key;
+    } else if (go) {
+      p.out_key[g] = kDeadKey;
+    }
+  }
+}
+
+// Appends q[from, from + cnt) (cnt <= 32) to the step's list of flights that
+// may reach the body (one atomic per call).
+__device__ __forceinline__ void list_deferred(const StepParams& p, const uint32_t* q, uint32_t from,
+                                              uint32_t cnt) {
+  const uint32_t lane = lane_id();
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(&p.meta->n_defer, cnt);
+  base = __shfl_sync(kFull, base, 0);
+  if (lane < cnt) p.defer_list[base + lane] = q[from + lane];
+}
+
+// Free flights, 32 particles at a time per warp, read from p.mid (the sorted
+// state k_collide_w produced) and written to p.out.  Flights that may reach
+// the body are listed for k_mesh_w instead, which spreads them over the whole
+// GPU (they cluster in the tiles next to the body).
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
+  __shared__ uint32_t s_q[WARPS][kFlightQ];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const bool do_move = (p.flags & kDoMove) != 0;
+  const bool split = p.has_geom && do_move;
+  uint32_t* q = s_q[warp];
+
+  const uint32_t nwarps = gridDim.x * WARPS;
+  const uint32_t gw = blockIdx.x * WARPS + warp;
+  TileQueue tq{nwarps, gw + nwarps, p.meta ? &p.meta->tile_next2 : nullptr};
+  uint32_t tnext = 0;
+  if (lane == 0 && gw < p.n_tiles) tnext = tq.grab();
+  uint32_t removed = 0, nq = 0;
+  WTile T = load_tile(p, gw);
+  while (T.t < p.n_tiles) {
+    // the warp's next tile (its starts load while this one is flown); lane 0
+    // asks for the one after it
+    const uint32_t t2 = __shfl_sync(kFull, tnext, 0);
+    if (lane == 0 && t2 < p.n_tiles) tnext = tq.grab();
+    const WTile T2 = load_tile(p, t2);
+    const uint32_t ts = __shfl_sync(kFull, T.s, 0), te = __shfl_sync(kFull, T.e, T.nct - 1u);
+    // the state of the first group of 32; each iteration loads the next
+    // group's while it flies the current one
+    float3 npos = make_float3(0.f, 0.f, 0.f), nvel = npos;
+    if (ts + lane < te) {
+      const uint32_t g = ts + lane;
+      npos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
+      nvel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
+    }
+    for (uint32_t qb = ts; qb < te; qb += 32) {
+      const uint32_t g = qb + lane;
+      const bool active = g < te;
+      const float3 pos0 = npos, vel0 = nvel;
+      if (g + 32u < te) {
+        const uint32_t gn = g + 32u;
+        npos = make_float3(p.mid.x[gn], p.mid.y[gn], p.mid.z[gn]);
+        nvel = make_float3(p.mid.u[gn], p.mid.v[gn], p.mid.w[gn]);
+      }
+      float3 pos = pos0, vel = vel0;
+      bool defer = false;
+      if (active && split) defer = flight_may_meet_body(p, pos, vel);
+      const unsigned dm = __ballot_sync(kFull, defer);
+      if (defer) q[nq + __popc(dm & ((1u << lane) - 1u))] = g;
+      nq += __popc(dm);
+      const bool go = active && !defer;
+      bool live = true;
+      // a path that cannot reach the body
+      if (go && do_move) live = move_free(p, pos, vel, g, step);
+      finish_flight(p, go, live, g, pos, vel, removed);
+      if (nq >= 32) {
+        __syncwarp();
+        nq -= 32;
+        list_deferred(p, q, nq, 32);
+        __syncwarp();
+      }
+    }
+    T = T2;
+  }
+  if (nq) {
+    __syncwarp();
+    list_deferred(p, q, 0, nq);
+  }
+  const uint32_t r = warp_sum(removed);
+  if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+}
+
+// The listed flights, one particle per thread over the whole grid (the list's
+// order does not matter: each particle's flight, key and count are its own).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const uint32_t n = p.meta->n_defer;
+  uint32_t removed = 0;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const bool go = i < n;
+    uint32_t g = 0;
+    float3 pos = make_float3(0.f, 0.f, 0.f), vel = pos;
+    bool live = true;
+    if (go) {
+      g = p.defer_list[i];
+      pos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
+      vel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
+      live = move_particle(p, pos, vel, g, step);
+    }
+    finish_flight(p, go, live, g, pos, vel, removed);
+  }
+  const uint32_t r = warp_sum(removed);
+  if (lane_id() == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+}
+
+// FP64 sampling after the flights, one cell per thread (the reference's
+// SampleCellStatisticsDev order: each cell's particles in sorted order, with
+// their velocities after the move); returns at once on other steps.
+__global__ void __launch_bounds__(256) k_sample_w(const __grid_constant__ StepParams p) {
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const bool do_sample =
+      (p.flags & kDoSample) &&
+      ((p.flags & kSampleForce) || (p.sample_every > 0 && step % (uint32_t)p.sample_every == 0));
+  if (!do_sample) return;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < p.cells; c += gridDim.x * blockDim.x) {
+    const uint32_t s = __ldg(&p.start[c]), e = __ldg(&p.start[c + 1]);
+    GlobalVel a{p.out.u, p.out.v, p.out.w, s};
+    sample_cell(p.acc, p.cells, c, (int)(e - s), a);
+  }
+  if (p.meta && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.meta->samples, 1u);
+}
+
+// ------------------------------------------------------------- launches ----
+
+struct LaunchShapeW {
+  int device = -1;
+  uint32_t n_scan_tiles = 0;
+  int per_sm = 0;
+};
+
+template <int CAPW, int WARPS, int MINB>
+cudaError_t launch_collide_w(const StepParams& p, cudaStream_t stream) {
+  static LaunchShapeW cache[8];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  LaunchShapeW& ls = cache[dev & 7];
+  const size_t smem = collide_smem_bytes<CAPW, WARPS>();
+  if (ls.device != dev) {
+    e = cudaFuncSetAttribute(k_collide_w<CAPW, WARPS, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_collide_w<CAPW, WARPS, MINB>,
+                                                      WARPS * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    ls.device = dev;
+    ls.per_sm = per_sm;
+  }
+  uint32_t grid = (uint32_t)(num_sms() * ls.per_sm);
+  const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
+  if (grid > need) grid = need;
+  if (grid == 0) return cudaSuccess;
+  k_collide_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+constexpr int kFlightWarps = 8;
+
+template <int MINB>
+cudaError_t launch_flight_w(const StepParams& p, cudaStream_t stream) {
+  static LaunchShapeW cache[8];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  LaunchShapeW& ls = cache[dev & 7];
+  if (ls.device != dev) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flight_w<kFlightWarps, MINB>,
+                                                      kFlightWarps * 32, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    ls.device = dev;
+    ls.per_sm = per_sm;
+  }
+  uint32_t grid = (uint32_t)(num_sms() * ls.per_sm);
+  const uint32_t need = (p.n_tiles + kFlightWarps - 1) / kFlightWarps;
+  if (grid > need) grid = need;
+  if (grid == 0) return cudaSuccess;
+  k_flight_w<kFlightWarps, MINB><<<grid, kFlightWarps * 32, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+template <int MINB>
+cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
+  static LaunchShapeW cache[8];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  LaunchShapeW& ls = cache[dev & 7];
+  if (ls.device != dev) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mesh_w<MINB>, 256, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    ls.device = dev;
+    ls.per_sm = per_sm;
+  }
+  k_mesh_w<MINB><<<(uint32_t)(num_sms() * ls.per_sm), 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
+  k_sample_w<<<grid_for(p.cells, 256, 8), 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Split variants (cell_kernel_variants() numbers them after the fused
+// CTA-wide ones): (particles per warp chunk, warps per CTA, register cap) of
+// the order + collide kernel and the register cap of the flight kernel (8
+// warps per CTA): 0 (256, 4, 128; 80), 1 (128, 4, 128; 80), 2 (128, 8, 80;
+// 64), 3 (128, 4, 64; 64).  The mesh kernel runs at 64 registers (more warps
+// to cover its chains of L2 loads).
+int cell_kernel_w_variants() { return 4; }
+
+int cell_kernel_w_capacity(int v) {
+  static const int caps[4] = {256, 128, 128, 128};
+  return caps[v < 0 || v > 3 ? 1 : v];
+}
+
+uint32_t cell_kernel_w_tile() { return kWarpTile; }
+
+cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream) {
+  cudaError_t e;
+  switch (v) {
+    case 0: e = launch_collide_w<256, 4, 4>(p, stream); break;
+    case 2: e = launch_collide_w<128, 8, 3>(p, stream); break;
+    case 3: e = launch_collide_w<128, 4, 8>(p, stream); break;
+    default: e = launch_collide_w<128, 4, 4>(p, stream); break;
+  }
+  if (e != cudaSuccess) return e;
+  switch (v) {
+    case 2: case 3: e = launch_flight_w<4>(p, stream); break;
+    default: e = launch_flight_w<3>(p, stream); break;
+  }
+  if (e != cudaSuccess) return e;
+  // flights that may reach the body (listed only with a body and the move)
+  if (p.has_geom && (p.flags & kDoMove)) {
+    e = launch_mesh_w<4>(p, stream);
+    if (e != cudaSuccess) return e;
+  }
+  if (p.flags & kDoSample) return launch_sample_w(p, stream);
+  return cudaSuccess;
+}
+
+}  // namespace dsmcb

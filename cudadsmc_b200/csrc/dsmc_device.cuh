@@ -58,6 +58,13 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
   return c;
 }
 
+// One Philox block, out of line: the streams below refill from one copy of
+// the ten rounds instead of an inlined copy at every draw site.
+static __device__ __noinline__ uint4 philox_block(uint32_t b, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                  uint2 k) {
+  return philox4x32_10(make_uint4(b, c1, c2, c3), k);
+}
+
 // A Philox stream: (key, counter words 1..3 fixed) and a running block index
 // in word 0; hands out 32-bit words four at a time.
 struct PhiloxStream {
@@ -71,7 +78,7 @@ struct PhiloxStream {
   }
   __device__ __forceinline__ uint32_t next() {
     if (used == 4) {
-      buf = philox4x32_10(make_uint4(block++, c1, c2, c3), key);
+      buf = philox_block(block++, c1, c2, c3, key);
       used = 0;
     }
     uint32_t r = used == 0 ? buf.x : used == 1 ? buf.y : used == 2 ? buf.z : buf.w;
@@ -170,9 +177,12 @@ __device__ __forceinline__ bool intersect_triangle(float3 orig, float3 dir, floa
 struct GeomView {
   GridGeom grid;
   const uint32_t* flags;
-  const uint2* start_end;
-  // kTriStride float4 per bin entry: (v0, n.x), (v1, n.y), (v2, n.z), (plane normal, offset)
+  const uint2* start_end;  // bin entries of each cell; (kNone, kNone) when empty
+  // kTriStride float4 per bin entry: (v0, n.x), (v1, n.y), (v2, n.z)
   const float4* tri;
+  // per bin entry, the triangle's plane (unit normal, offset), packed apart
+  // from the vertices so that a cell's planes share cache lines
+  const float4* plane;
   // per cell, a lower bound of the distance from any point of the cell to the
   // surface (0 in cells holding triangles)
   const float* clear;
@@ -181,7 +191,7 @@ struct GeomView {
   int nearest;        // 0: reference first-hit in start/end cells; 1: nearest hit along the path
 };
 
-constexpr int kTriStride = 4;
+constexpr int kTriStride = 3;
 
 // Ray/triangle test with a determinant threshold relative to the triangle's
 // size (the reference's absolute 1e-6 rejects near-grazing rays on small
@@ -216,12 +226,17 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
   float lo[3] = {g.gmin.x, g.gmin.y, g.gmin.z}, hi[3] = {g.gmax.x, g.gmax.y, g.gmax.z};
   float cs[3] = {g.cell.x, g.cell.y, g.cell.z};
   int dm[3] = {(int)g.dim.x, (int)g.dim.y, (int)g.dim.z};
+  // slab and cell-crossing parameters by reciprocal multiplies (the start
+  // cell below keeps the division)
+  float ida[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) ida[a] = fabsf(da[a]) < 1e-30f ? 0.f : 1.f / da[a];
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     if (fabsf(da[a]) < 1e-30f) {
       if (oa[a] < lo[a] || oa[a] > hi[a]) return false;
     } else {
-      float ta = (lo[a] - oa[a]) / da[a], tb = (hi[a] - oa[a]) / da[a];
+      float ta = (lo[a] - oa[a]) * ida[a], tb = (hi[a] - oa[a]) * ida[a];
       if (ta > tb) { float s = ta; ta = tb; tb = s; }
       t0 = fmaxf(t0, ta);
       t1 = fminf(t1, tb);
@@ -237,12 +252,12 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
     idx[a] = min(max(i, 0), dm[a] - 1);
     if (da[a] > 0.f) {
       stp[a] = 1;
-      tmax[a] = (lo[a] + (idx[a] + 1) * cs[a] - oa[a]) / da[a];
-      tdel[a] = cs[a] / da[a];
+      tmax[a] = (lo[a] + (idx[a] + 1) * cs[a] - oa[a]) * ida[a];
+      tdel[a] = cs[a] * ida[a];
     } else if (da[a] < 0.f) {
       stp[a] = -1;
-      tmax[a] = (lo[a] + idx[a] * cs[a] - oa[a]) / da[a];
-      tdel[a] = -cs[a] / da[a];
+      tmax[a] = (lo[a] + idx[a] * cs[a] - oa[a]) * ida[a];
+      tdel[a] = -cs[a] * ida[a];
     } else {
       stp[a] = 0;
       tmax[a] = 3.0e38f;
@@ -254,14 +269,21 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
   const int max_iter = dm[0] + dm[1] + dm[2] + 3;
   for (int it = 0; it < max_iter; it++) {
     uint32_t c = ((uint32_t)idx[2] * g.dim.y + (uint32_t)idx[1]) * g.dim.x + (uint32_t)idx[0];
-    if (__ldg(&G.flags[c]) != 0) {
-      uint2 se = __ldg(&G.start_end[c]);
-      for (uint32_t i = se.x; i < se.y; i++) {
+    const uint2 se = __ldg(&G.start_end[c]);
+    for (uint32_t i0 = se.x; i0 < se.y; i0 += 8) {
+      // the planes of up to 8 of the cell's triangles in one round of loads
+      float4 P[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        P[k] = i0 + k < se.y ? __ldg(&G.plane[i0 + k]) : make_float4(0.f, 0.f, 0.f, 1.f);
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t i = i0 + k;
+        if (i >= se.y) break;
         // plane pre-test: both ends of the segment on one side -> no crossing
-        const float4 P = __ldg(&G.tri[kTriStride * (size_t)i + 3]);
-        const float s0 = P.x * o.x + P.y * o.y + P.z * o.z - P.w;
-        const float s1 = s0 + dist * (P.x * d.x + P.y * d.y + P.z * d.z);
-        const float tol = 1e-7f * (fabsf(P.w) + 1.f);
+        const float s0 = P[k].x * o.x + P[k].y * o.y + P[k].z * o.z - P[k].w;
+        const float s1 = s0 + dist * (P[k].x * d.x + P[k].y * d.y + P[k].z * d.z);
+        const float tol = 1e-7f * (fabsf(P[k].w) + 1.f);
         if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
         float4 A = __ldg(&G.tri[kTriStride * (size_t)i]);
         float4 B = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
@@ -341,8 +363,9 @@ __device__ __forceinline__ bool inside_mesh(const GeomView& G, float3 o) {
 // Diffuse re-emission about the unit normal n on the side the particle came
 // from (full accommodation at the wall temperature): normal speed from the
 // flux-weighted half-range Maxwellian, tangential components Gaussian.
-__device__ __forceinline__ float3 diffuse_emit(float3 n_out, float vstd, PhiloxStream& rng) {
-  float r1 = rng.uniform(), r2 = rng.uniform(), r3 = rng.uniform();
+// r1, r2, r3: uniforms in (0, 1).  Out of line (walls are the cold path).
+static __device__ __noinline__ float3 diffuse_emit_r(float3 n_out, float vstd, float r1, float r2,
+                                                     float r3) {
   float vn = vstd * sqrtf(-2.0f * logf(r1));
   float rad = vstd * sqrtf(-2.0f * logf(r2));
   float s, c;
@@ -356,6 +379,10 @@ __device__ __forceinline__ float3 diffuse_emit(float3 n_out, float vstd, PhiloxS
                           n_out.x * e1.y - n_out.y * e1.x);
   return make_float3(vn * n_out.x + t1 * e1.x + t2 * e2.x, vn * n_out.y + t1 * e1.y + t2 * e2.y,
                      vn * n_out.z + t1 * e1.z + t2 * e2.z);
+}
+__device__ __forceinline__ float3 diffuse_emit(float3 n_out, float vstd, PhiloxStream& rng) {
+  const float r1 = rng.uniform(), r2 = rng.uniform(), r3 = rng.uniform();
+  return diffuse_emit_r(n_out, vstd, r1, r2, r3);
 }
 
 // CollideWithGeometry, kernels/dsmc_kernel.cu:1256-1314: the first triangle

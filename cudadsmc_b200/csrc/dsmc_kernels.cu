@@ -19,7 +19,7 @@ namespace {
 using namespace dev;
 
 // Move stage: free flight and boundaries for n particles in place.
-__global__ void __launch_bounds__(256) k_move(const StepParams p, uint32_t n, uint32_t step) {
+__global__ void __launch_bounds__(256) k_move(const __grid_constant__ StepParams p, uint32_t n, uint32_t step) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float3 pos = make_float3(p.out.x[i], p.out.y[i], p.out.z[i]);
     float3 vel = make_float3(p.out.u[i], p.out.v[i], p.out.w[i]);
@@ -124,6 +124,8 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
     meta->n_pending = 0;
     meta->n_alive = run;
     meta->tile_next = 0;
+    meta->tile_next2 = 0;
+    meta->n_defer = 0;
     if (bump) {
       meta->step += 1;
       meta->particle_steps += run;
@@ -132,31 +134,76 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
 }
 
 // Scatter into sorted order: dst[start[key] + ticket] = src[i], orig = i.  The
-// tickets come from per-cell cursors (one atomic per distinct key per warp).
-__global__ void __launch_bounds__(256) k_scatter(SoA src, SoA dst, const uint32_t* __restrict__ keys,
-                                                 const uint32_t* __restrict__ start,
-                                                 uint32_t* cursor, uint32_t* __restrict__ orig,
-                                                 uint32_t cells, uint32_t* tile_sum,
-                                                 uint32_t n_scan_tiles, Meta* meta,
-                                                 uint32_t capacity) {
+// tickets come from per-cell cursors (one atomic per distinct key per group of
+// 32).  Each warp takes kScatterU groups of 32 consecutive particles at once,
+// so that their chains of key load -> ticket atomic -> stores overlap.  With
+// STATE false only orig is written: one scattered 4-byte store per particle
+// instead of seven (scattered stores, not the loads or the atomics, bound this
+// kernel), and the split cell kernels gather the state through orig.
+constexpr int kScatterU = 4;
+
+template <bool STATE>
+__global__ void __launch_bounds__(256, 4) k_scatter(SoA src, SoA dst, const uint32_t* __restrict__ keys,
+                                                    const uint32_t* __restrict__ start,
+                                                    uint32_t* cursor, uint32_t* __restrict__ orig,
+                                                    uint32_t cells, uint32_t* tile_sum,
+                                                    uint32_t n_scan_tiles, Meta* meta,
+                                                    uint32_t capacity) {
   if (blockIdx.x == 0)
     for (uint32_t t = threadIdx.x; t < n_scan_tiles; t += blockDim.x) tile_sum[t] = 0;
   const uint32_t n = meta->n_scatter;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    const uint32_t i = base + threadIdx.x;
-    const uint32_t key = i < n ? keys[i] : kDeadKey;
-    const bool live = key < cells;
-    if (i < n && key != kDeadKey && !live) atomicOr(&meta->error, kErrKeyRange);
-    const unsigned m = __ballot_sync(kFull, live);
-    if (!live) continue;
-    const uint32_t d = __ldg(&start[key]) + warp_ticket(cursor, key, m);
-    if (d >= capacity) {
-      atomicOr(&meta->error, kErrKeyRange);
-      continue;
+  const uint32_t lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  constexpr int U = kScatterU;
+  for (uint32_t base = gw * 32u * U; base < n; base += nw * 32u * U) {
+    uint32_t key[U];
+    float x[U], y[U], z[U], u[U], v[U], w[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const uint32_t i = base + 32u * k + lane;
+      key[k] = i < n ? keys[i] : kDeadKey;
+      x[k] = y[k] = z[k] = u[k] = v[k] = w[k] = 0.f;
+      if (STATE && i < n) {
+        x[k] = src.x[i]; y[k] = src.y[i]; z[k] = src.z[i];
+        u[k] = src.u[i]; v[k] = src.v[i]; w[k] = src.w[i];
+      }
     }
-    dst.x[d] = src.x[i]; dst.y[d] = src.y[i]; dst.z[d] = src.z[i];
-    dst.u[d] = src.u[i]; dst.v[d] = src.v[i]; dst.w[d] = src.w[i];
-    orig[d] = i;
+    // the ticket atomics of all groups first, then their broadcasts
+    unsigned msk[U], peers[U];
+    uint32_t st[U], got[U];
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      const uint32_t i = base + 32u * k + lane;
+      const bool live = key[k] < cells;
+      if (i < n && key[k] != kDeadKey && !live) atomicOr(&meta->error, kErrKeyRange);
+      msk[k] = __ballot_sync(kFull, live);
+      st[k] = 0;
+      got[k] = 0;
+      peers[k] = 0;
+      if (live) {
+        st[k] = __ldg(&start[key[k]]);
+        peers[k] = __match_any_sync(msk[k], key[k]);
+        if ((int)lane == __ffs(peers[k]) - 1) got[k] = atomicAdd(&cursor[key[k]], (uint32_t)__popc(peers[k]));
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
+      if (!(key[k] < cells)) continue;
+      const uint32_t i = base + 32u * k + lane;
+      const uint32_t t = __shfl_sync(msk[k], got[k], __ffs(peers[k]) - 1) +
+                         __popc(peers[k] & ((1u << lane) - 1u));
+      const uint32_t d = st[k] + t;
+      if (d >= capacity) {
+        atomicOr(&meta->error, kErrKeyRange);
+        continue;
+      }
+      if (STATE) {
+        dst.x[d] = x[k]; dst.y[d] = y[k]; dst.z[d] = z[k];
+        dst.u[d] = u[k]; dst.v[d] = v[k]; dst.w[d] = w[k];
+      }
+      orig[d] = i;
+    }
   }
 }
 
@@ -310,7 +357,7 @@ __global__ void k_sample_cells(const float* __restrict__ u, const float* __restr
 // reference's speed/angle sampler (GetRandomVelocity, :394-415) or an exact
 // Maxwellian.  Random numbers come from Philox (the reference used its
 // Mersenne-Twister table, which is not reproduced).
-__global__ void k_init_fill(const InitParams p) {
+__global__ void k_init_fill(const __grid_constant__ InitParams p) {
   const uint32_t total = p.cells * p.ppc;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
     const uint32_t cell = i / p.ppc, k = i - cell * p.ppc;
@@ -374,7 +421,7 @@ __global__ void k_init_fill(const InitParams p) {
 
 // Plan: number of particles the face injects this step (carrying the
 // fractional remainder), reserved after the particles already in the array.
-__global__ void k_inject_plan(const InjectParams p, uint32_t* plan) {
+__global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* plan) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const float want = *p.remainder + p.inflow.number_flux * p.inflow.area * p.dt;
   uint32_t k = want > 0.f ? (uint32_t)want : 0u;
@@ -415,7 +462,7 @@ __device__ __forceinline__ float sample_flux_normal(float s, PhiloxStream& r) {
 __device__ __forceinline__ float& comp(float3& a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 __device__ __forceinline__ float compc(const float3& a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 
-__global__ void k_inject_fill(const InjectParams p, const uint32_t* plan) {
+__global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint32_t* plan) {
   extern __shared__ uint32_t s_tile[];
   const uint32_t step = p.meta->step;
   for (uint32_t t = threadIdx.x; t < p.n_scan_tiles; t += blockDim.x) s_tile[t] = 0;
@@ -503,13 +550,18 @@ cudaError_t launch_scan(uint32_t* count, uint32_t* cursor, uint32_t* start, uint
   return cudaGetLastError();
 }
 
-cudaError_t launch_scatter(const SoA& src, SoA dst, const uint32_t* keys, const uint32_t* start,
+cudaError_t launch_scatter(bool with_state, const SoA& src, SoA dst, const uint32_t* keys,
+                           const uint32_t* start,
                            uint32_t* cursor, uint32_t* orig, uint32_t cells, uint32_t* tile_sum,
                            uint32_t n_scan_tiles, Meta* meta, uint32_t capacity,
                            cudaStream_t stream) {
-  const uint32_t grid = (uint32_t)num_sms() * 8;
-  k_scatter<<<grid, 256, 0, stream>>>(src, dst, keys, start, cursor, orig, cells, tile_sum,
-                                      n_scan_tiles, meta, capacity);
+  const uint32_t grid = (uint32_t)num_sms() * 4;
+  if (with_state)
+    k_scatter<true><<<grid, 256, 0, stream>>>(src, dst, keys, start, cursor, orig, cells, tile_sum,
+                                              n_scan_tiles, meta, capacity);
+  else
+    k_scatter<false><<<grid, 256, 0, stream>>>(src, dst, keys, start, cursor, orig, cells,
+                                               tile_sum, n_scan_tiles, meta, capacity);
   return cudaGetLastError();
 }
 
@@ -578,7 +630,7 @@ cudaError_t launch_sample_cells(const float* u, const float* v, const float* w,
 }
 
 // One warp per cell, two of the 4x4x4 sub-cell centres per lane.
-__global__ void k_outside_fraction(const GridGeom grid, const GeomView geom, uint32_t cells,
+__global__ void k_outside_fraction(const GridGeom grid, const __grid_constant__ GeomView geom, uint32_t cells,
                                    float* frac, float4* point) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);

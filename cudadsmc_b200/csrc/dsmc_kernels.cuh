@@ -40,6 +40,8 @@ struct Meta {
   uint32_t injected;     // particles injected by the inflow faces (total)
   uint32_t removed;      // particles removed through outflow faces (total)
   uint32_t tile_next;    // the cell kernel's dynamic tile counter (reset by the scan)
+  uint32_t tile_next2;   // the flight kernel's dynamic tile counter (reset by the scan)
+  uint32_t n_defer;      // flights listed for the mesh kernel this step (reset by the scan)
   unsigned long long particle_steps;  // sum over steps of the particles placed by the scan
 };
 
@@ -86,6 +88,9 @@ struct StepParams {
   int hard_sphere;
   float vhs_exp;   // 2*omega - 1
   float vhs_gref;
+  // Philox mode: sigma(g) g = 2^(vhs_c1 log2 g + vhs_c0), vhs_c1 = 1 - vhs_exp,
+  // vhs_c0 = log2(cross_section) + vhs_exp log2(vhs_gref)
+  float vhs_c0, vhs_c1;
   int ntc_local;
   int rng_kind;    // 0 HybridTaus per cell (reference), 1 Philox
   uint2 seed;
@@ -99,6 +104,9 @@ struct StepParams {
   SoA in;             // state the cell kernel reads (sorted by scatter)
   const uint32_t* in_orig;
   SoA out;            // state the cell kernel writes (sorted order)
+  SoA mid;            // split variants: the sorted post-collision state between
+                      // the collide kernel (which gathers it from `in` through
+                      // in_orig) and the flight kernel (which writes `out`)
   uint32_t* out_key;  // next-step cell key (kDeadKey: left the domain)
   const uint32_t* start;   // cells+1 exclusive starts
   uint32_t* count;         // per-cell counters for the next step
@@ -115,6 +123,9 @@ struct StepParams {
   uint32_t n_tiles;
   uint32_t step_override;  // 0: use meta->step
   int cell_variant;        // (threads, chunk capacity) of the cell kernel
+  uint32_t* defer_list;    // split variants: flights that may reach the body
+                           // (capacity entries; the orig buffer, dead once the
+                           // collide kernel has read it)
 };
 
 // Launchers (all asynchronous on `stream`).
@@ -125,16 +136,27 @@ cudaError_t launch_index(const GridGeom& g, uint32_t cells, const float* x, cons
 cudaError_t launch_scan(uint32_t* count, uint32_t* cursor, uint32_t* start, uint32_t cells,
                         const uint32_t* tile_sum, uint32_t n_scan_tiles, Meta* meta, int bump_step,
                         cudaStream_t stream);
-cudaError_t launch_scatter(const SoA& src, SoA dst, const uint32_t* keys, const uint32_t* start,
+// with_state = false: only orig (the split cell kernels gather the state).
+cudaError_t launch_scatter(bool with_state, const SoA& src, SoA dst, const uint32_t* keys,
+                           const uint32_t* start,
                            uint32_t* cursor, uint32_t* orig, uint32_t cells, uint32_t* tile_sum,
                            uint32_t n_scan_tiles, Meta* meta, uint32_t capacity,
                            cudaStream_t stream);
 // The timestep's fused cell kernel (also the collide stage with kVelOnly).
 cudaError_t launch_cell(const StepParams& p, cudaStream_t stream);
-// Variants of the cell kernel: 0 (512 threads, 2048 particles per chunk,
-// 1 CTA/SM), 1 (256, 1024, 2), 2 (128, 512, 4), 3 (64, 256, up to 8).
+// Variants of the cell kernel.  CTA-wide: 0 (512 threads, 2048 particles per
+// chunk, 1 CTA/SM), 1 (256, 1024, 2), 2 (128, 512, 4), 3 (64, 256, up to 8).
+// Warp-autonomous (particles per warp chunk, warps per CTA): 4 (256, 4),
+// 5 (128, 4), 6 (128, 8), 7 (64, 8).
 int cell_kernel_variants();
 int cell_kernel_chunk_capacity(int variant);
+// Variants at or above 4 use the warp-autonomous kernel, whose tiles are
+// cell_kernel_w_tile() cells (one per lane).
+bool cell_kernel_is_warp(int variant);
+int cell_kernel_w_variants();
+int cell_kernel_w_capacity(int v);
+uint32_t cell_kernel_w_tile();
+cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream);
 // Free flight + boundaries in place on p.out for n particles (move stage);
 // particles that leave through an outflow face get x = NaN.
 cudaError_t launch_move(const StepParams& p, uint32_t n, uint32_t step, cudaStream_t stream);

@@ -8,6 +8,8 @@ namespace dsmcb {
 namespace dev {
 
 constexpr unsigned kFull = 0xffffffffu;
+// NTC selections at which a cell is collided by a whole warp (Philox mode).
+constexpr uint32_t kHeavyMin = 8;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
@@ -22,6 +24,19 @@ __device__ __forceinline__ void warp_count_key(uint32_t* count, uint32_t key, un
     atomicAdd(&count[key], cnt);
     atomicAdd(&s_tile[key >> kScanShift], cnt);
   }
+}
+
+// Adds the lanes of `mask` holding `key` to count[key] and to the per scan
+// tile totals in global memory (one atomic per distinct key and one per
+// distinct scan tile per warp): for kernels without a block-wide histogram.
+__device__ __forceinline__ void warp_count_key_global(uint32_t* count, uint32_t key, unsigned mask,
+                                                      uint32_t* tile_sum) {
+  const unsigned lane = lane_id();
+  const unsigned peers = __match_any_sync(mask, key);
+  if ((int)lane == __ffs(peers) - 1) atomicAdd(&count[key], (uint32_t)__popc(peers));
+  const uint32_t tk = key >> kScanShift;
+  const unsigned tpeers = __match_any_sync(mask, tk);
+  if ((int)lane == __ffs(tpeers) - 1) atomicAdd(&tile_sum[tk], (uint32_t)__popc(tpeers));
 }
 
 // Ticket from a per-key counter, aggregated over the lanes of `mask` holding
@@ -109,6 +124,26 @@ struct CellState {
 __device__ __forceinline__ float sigma_g(const StepParams& p, float mag) {
   if (p.hard_sphere) return mag * p.cross_section;
   return mag > 0.f ? mag * (p.cross_section * powf(p.vhs_gref / mag, p.vhs_exp)) : 0.f;
+}
+
+__device__ __forceinline__ float lg2_approx(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// sigma(g) g of the Philox mode: the VHS power law as
+// 2^((1 - e) log2 g + log2 sigma_ref + e log2 g_ref) with the hardware base-2
+// log and exponential (relative error about 1e-6, far below what an
+// acceptance test R < sigma g / (sigma g)max can resolve).
+__device__ __forceinline__ float sigma_g_fast(const StepParams& p, float mag) {
+  if (p.hard_sphere) return mag * p.cross_section;
+  return mag > 0.f ? ex2_approx(fmaf(p.vhs_c1, lg2_approx(mag), p.vhs_c0)) : 0.f;
 }
 
 // NTC collisions of one cell with the reference's arithmetic:
@@ -202,7 +237,7 @@ __device__ __forceinline__ void ntc_fast(const StepParams& p, uint32_t cell, uin
     if (pj >= n) pj -= n;
     const float3 v1 = acc.get(pi), v2 = acc.get(pj);
     const float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
-    const float v = sigma_g(p, mag);
+    const float v = sigma_g_fast(p, mag);
     if (v > r.uniform() * vm.x) {
       ncol++;
       sum_g += mag;
@@ -281,7 +316,7 @@ __device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cel
     if (win) {
       const float3 v1 = acc.get(pi), v2 = acc.get(pj);
       const float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
-      vv = sigma_g(p, mag);
+      vv = sigma_g_fast(p, mag);
       if (vv > rng.uniform() * vmax) {
         ncol++;
         sum_g += mag;
@@ -409,6 +444,13 @@ __device__ __forceinline__ bool face_bc(const StepParams& p, float3& pos, float3
   return true;
 }
 
+// Whether the box spanned by a path from a to b overlaps the grid's box.
+__device__ __forceinline__ bool path_box_meets_grid(const GridGeom& g, float3 a, float3 b) {
+  return fminf(a.x, b.x) <= g.gmax.x && fmaxf(a.x, b.x) >= g.gmin.x &&
+         fminf(a.y, b.y) <= g.gmax.y && fmaxf(a.y, b.y) >= g.gmin.y &&
+         fminf(a.z, b.z) <= g.gmax.z && fmaxf(a.z, b.z) >= g.gmin.z;
+}
+
 // Whether this step's flight from pos may reach the body: the path is at
 // least the start cell's clearance (nearest mode) or starts or ends in a
 // geometry cell holding triangles (first-hit mode); a start outside the
@@ -423,18 +465,41 @@ __device__ __forceinline__ bool flight_may_meet_body(const StepParams& p, float3
       const float dist = length3(make_float3(e.x - pos.x, e.y - pos.y, e.z - pos.z));
       return !(dist < __ldg(&G.clear[sc]));
     }
-    return fminf(pos.x, e.x) <= G.grid.gmax.x && fmaxf(pos.x, e.x) >= G.grid.gmin.x &&
-           fminf(pos.y, e.y) <= G.grid.gmax.y && fmaxf(pos.y, e.y) >= G.grid.gmin.y &&
-           fminf(pos.z, e.z) <= G.grid.gmax.z && fmaxf(pos.z, e.z) >= G.grid.gmin.z;
+    return path_box_meets_grid(G.grid, pos, e);
   }
   const uint32_t ec = coll_cell_id(G.grid, e);
   return (sc != kNone && __ldg(&G.flags[sc]) != 0) || (ec != kNone && __ldg(&G.flags[ec]) != 0);
 }
 
-// One particle's flight: IntegrateDev / ProcessCollisionsDev,
-// kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.
-__device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, float3& vel,
-                                              uint32_t gidx, uint32_t step) {
+// The boundaries after the flight: the reference's functors or the per-face
+// kinds.
+__device__ __forceinline__ bool apply_bc(const StepParams& p, float3& pos, float3& vel,
+                                         PhiloxStream& rng) {
+  if (p.face_mode == 0) {
+    ref_bc(p.periodic, p.grid, pos, vel);
+    return true;
+  }
+  return face_bc(p, pos, vel, rng);
+}
+
+// Free flight and boundaries: move_particle_full's arithmetic for a path that
+// cannot reach the body (flight_may_meet_body false), or without a body.
+__device__ __forceinline__ bool move_free(const StepParams& p, float3& pos, float3& vel,
+                                          uint32_t gidx, uint32_t step) {
+  const float3 old_pos = pos;
+  pos.x = old_pos.x + vel.x * p.dt;
+  pos.y = old_pos.y + vel.y * p.dt;
+  pos.z = old_pos.z + vel.z * p.dt;
+  PhiloxStream rng;
+  rng.init(p.seed, gidx, step, kPurposeWall);
+  return apply_bc(p, pos, vel, rng);
+}
+
+// One particle's flight with the body: IntegrateDev / ProcessCollisionsDev,
+// kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.  Out
+// of line: only flights that may reach the body come here in the step.
+static __device__ __noinline__ bool move_particle_full(const StepParams& p, float3& pos,
+                                                       float3& vel, uint32_t gidx, uint32_t step) {
   float3 old_pos = pos;
   pos.x = old_pos.x + vel.x * p.dt;
   pos.y = old_pos.y + vel.y * p.dt;
@@ -452,11 +517,14 @@ __device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, 
       // a path shorter than the start cell's clearance cannot reach the body
       const uint32_t sc = coll_cell_id(G.grid, old_pos);
       if (sc != kNone && dist < __ldg(&G.clear[sc])) break;
-      const float3 d = make_float3(seg.x / dist, seg.y / dist, seg.z / dist);
+      // a path outside the geometry grid whose box misses the grid's box
+      if (sc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
+      const float idist = 1.f / dist;
+      const float3 d = make_float3(seg.x * idist, seg.y * idist, seg.z * idist);
       float t;
       uint32_t e;
       if (!nearest_wall_hit(G, old_pos, d, dist, &t, &e)) break;
-      const float4 P = __ldg(&G.tri[kTriStride * (size_t)e + 3]);
+      const float4 P = __ldg(&G.plane[e]);
       const float3 n = make_float3(P.x, P.y, P.z);
       // the mesh is closed with outward normals: a face reached from its
       // back side holds a particle inside the body (left over from a fill of
@@ -498,11 +566,19 @@ __device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, 
       }
     } while (collProcessed && i++ < kCollisionLimit);
   }
-  if (p.face_mode == 0) {
-    ref_bc(p.periodic, p.grid, pos, vel);
-    return true;
-  }
-  return face_bc(p, pos, vel, rng);
+  return apply_bc(p, pos, vel, rng);
+}
+
+
+// One particle's flight (free flight inline, with a body out of line).
+__device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, float3& vel,
+                                              uint32_t gidx, uint32_t step) {
+  if (!p.has_geom) return move_free(p, pos, vel, gidx, step);
+  float3 tp = pos, tv = vel;
+  const bool live = move_particle_full(p, tp, tv, gidx, step);
+  pos = tp;
+  vel = tv;
+  return live;
 }
 
 // Sampling of one cell from sorted velocities (SampleCellStatisticsDev,

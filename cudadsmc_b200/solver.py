@@ -141,10 +141,10 @@ class DSMCSolver:
 
     def Autotune(self, dt, steps=10):
         """Times every cell-kernel variant on real timesteps (the run advances
-        by 4 * (steps + 2) steps) and keeps the fastest; returns (best, ms per
-        step of each variant)."""
+        by KernelVariantCount() * (steps + 2) steps) and keeps the fastest;
+        returns (best, ms per step of each variant)."""
         best = ctypes.c_int(0)
-        ms = np.zeros(4, np.float32)
+        ms = np.zeros(KernelVariantCount(), np.float32)
         self._check(lib().dsmc_autotune(self.h, dt, int(steps), ctypes.byref(best), _ptr(ms)),
                     "Autotune")
         return best.value, [float(x) for x in ms]
@@ -296,6 +296,11 @@ class DSMCBatch:
         v = np.zeros(len(self.solvers), np.int32)
         self._check(lib().dsmc_batch_autotune(self.b, _ptr(d), int(steps), _ptr(v)), "Autotune")
         return [int(x) for x in v]
+
+
+def KernelVariantCount():
+    """Number of launch shapes of the cell kernel (dsmc_kernel_variant_count)."""
+    return int(lib().dsmc_kernel_variant_count())
 
 
 def CreateSolver(kind="gpu"):

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 from cudadsmc_b200 import DSMCBatch, DSMCSolver, mesh_icosphere, settings_t
+from cudadsmc_b200.solver import KernelVariantCount
 
 pytestmark = pytest.mark.gpu
 
@@ -55,7 +56,7 @@ def test_batch_equals_members_stepped_alone(cuda):
         assert np.array_equal(a.Fields(), b.Fields(), equal_nan=True)
     # launch shapes chosen per member; the batch keeps stepping afterwards
     variants = batch.Autotune(steps=1)
-    assert len(variants) == 4 and all(0 <= v < 4 for v in variants)
+    assert len(variants) == 4 and all(0 <= v < KernelVariantCount() for v in variants)
     n0 = [s.Info().step for s in batched]
     batch.Step(3)
     batch.Sync()

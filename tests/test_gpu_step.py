@@ -12,6 +12,7 @@ import pytest
 import torch
 
 from cudadsmc_b200 import DSMCSolver, settings_t
+from cudadsmc_b200.solver import KernelVariantCount
 from oracle import oracle as O
 
 from helpers import box_case, taus_seeds, maxrem_init, sim_for
@@ -166,10 +167,16 @@ def test_steps_vs_reference_kernels(cuda, periodic, steps):
 
 @pytest.mark.parametrize("rng,density", [("taus", 1e20), ("philox", 1e20), ("philox", 6e20)])
 def test_kernel_variants_give_identical_steps(cuda, rng, density):
-    """Every launch shape of the cell kernel computes the same step (no cell
-    here exceeds the smallest chunk); the autotuner keeps one of them."""
+    """Every launch shape of the cell kernel (the CTA-wide and the
+    warp-autonomous kernels) computes the same step for cells that fit its
+    chunk; the autotuner keeps one of them.  At 6e20 about 146 particles sit
+    in a cell, more than the 128-particle warp chunks hold: those variants
+    collide such cells with one thread (a different Philox stream, by
+    design) and are only required to report them as giant cells."""
+    nv = KernelVariantCount()
+    assert nv == 8
     out = []
-    for v in range(4):
+    for v in range(nv):
         s = make_settings(density=density, rng=rng, init_kind="maxwell", seed=5).set(sample_every=3)
         solver = DSMCSolver().Init(s)
         solver.SetKernelVariant(v)
@@ -179,15 +186,21 @@ def test_kernel_variants_give_identical_steps(cuda, rng, density):
         solver.StepGraph(1e-5, 3)
         solver.Sync()
         out.append((solver.DownloadState(), solver.GetCellState(), solver.Fields(),
-                    solver.Info().giant_cells))
-        if v == 3:
+                    solver.Info().giant_cells, solver.KernelVariant()[1]))
+        if v == nv - 1:
             best, ms = solver.Autotune(1e-5, steps=2)
-            assert 0 <= best < 4 and all(m > 0 for m in ms)
+            assert 0 <= best < nv and len(ms) == nv and all(m > 0 for m in ms)
             assert solver.KernelVariant()[0] == best
         solver.close()
-    for v in range(1, 4):
-        assert out[v][3] == 0
+    compared = 0
+    for v in range(1, nv):
+        if out[v][3] != 0:
+            # only cells above the chunk may be giant
+            assert density > 1e20 and out[v][4] < 256
+            continue
+        compared += 1
         assert np.array_equal(out[0][0], out[v][0])
         assert np.array_equal(out[0][1][0], out[v][1][0])
         assert np.array_equal(out[0][1][1], out[v][1][1])
         assert np.array_equal(out[0][2], out[v][2], equal_nan=True)
+    assert compared >= (nv - 1 if density <= 1e20 else 4)
