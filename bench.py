@@ -288,13 +288,40 @@ def reduce_over_ranks(elapsed, count, world, device):
     return float(t.item()), float(c.item())
 
 
-def algorithmic_bytes(kernel, n_particles, cells, rng_taus, sample_frac):
-    """Bytes a kernel must move per launch (SoA FP32 state, 24 B/particle)."""
+def kernels_per_step(settings, variant, has_mesh):
+    """Kernels one timestep launches: scan and scatter; the fused cell kernel,
+    or the split variants' collide, flight, mesh flights (with a body) and
+    sampling (with sampling on: it returns at once on other steps); two per
+    inflow face (plan, fill)."""
+    n = 2
+    if variant >= 4:
+        n += 2 + (1 if has_mesh else 0) + (1 if settings.get("sample_every", 0) > 0 else 0)
+    else:
+        n += 1
+    faces = settings.get("face_kind", {})
+    return n + 2 * sum(1 for k in faces.values() if k == "inflow")
+
+
+def algorithmic_bytes(kernel, n_particles, cells, rng_taus, sample_frac, split=True):
+    """Bytes a kernel must move per launch (SoA FP32 state, 24 B/particle).
+
+    scatter: key read 4 + orig written 4 (split variants; for the fused cell
+    kernel it also moves the state: + 24 read + 24 written).  collide: orig 4
+    + state gathered 24 + sorted state written 24 per particle; per cell its
+    start 4 and (sigma g)max/remainder read + written 16 (+ 32 of HybridTaus
+    state in the reference RNG mode).  flight: state read 24 + written 24 +
+    next-step key 4 per particle.  cell (fused): state + orig read 28, state +
+    key written 28, the per-cell terms of collide and 80 B of sampling sums on
+    sampling steps."""
+    per_cell = 4 + 16 + (32 if rng_taus else 0)
     if kernel == "scatter":
-        return n_particles * (4 + 24 + 24 + 4)
+        return n_particles * (4 + 4 + (0 if split else 48))
+    if kernel == "collide":
+        return n_particles * (4 + 24 + 24) + cells * per_cell
+    if kernel == "flight":
+        return n_particles * (24 + 24 + 4)
     if kernel == "cell":
-        per_cell = 4 + 16 + (32 if rng_taus else 0) + sample_frac * 80
-        return n_particles * (24 + 4 + 24 + 4) + cells * per_cell
+        return n_particles * (24 + 4 + 24 + 4) + cells * (per_cell + sample_frac * 80)
     if kernel == "scan":
         return cells * 12
     return 0
@@ -314,6 +341,18 @@ def run_ours(args, rank, world):
     # autotuner of the cell kernel on real steps of the run
     sol.RunSimulationStep(dt, args.warmup)
     variant, tune_ms = sol.Autotune(dt, steps=args.tune_steps)
+    split = variant >= 4
+    # per-kernel breakdown on a short window with events around every kernel
+    # (an event pair costs the GPU a few microseconds, so the timed region
+    # below keeps events around the dominant kernel only)
+    bsteps = max(1, min(50, args.steps))
+    sol.Profile(True)
+    sol.RunSimulationStep(dt, bsteps)
+    breakdown = sol.ProfileReadKernels()
+    dom_slot = max((k for k in breakdown if k in ("scatter", "collide", "flight")),
+                   key=lambda k: breakdown[k][0])
+    if not split:
+        breakdown["cell"] = breakdown.pop("collide")  # the fused cell kernel's slot
     sol.Sync()
     info0 = sol.Info()
     if world > 1:
@@ -323,18 +362,19 @@ def run_ours(args, rank, world):
     gpu_index = int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0) if world == 1 else dev.index
     with ClockSampler(gpu_index) as clk:
         sol.Profile(True)
+        sol.ProfileOnly([dom_slot])
         ev0.record()
         sol.RunSimulationStep(dt, args.steps)
         ev1.record()
         torch.cuda.synchronize()
-        prof = sol.ProfileRead()
+        prof = sol.ProfileReadKernels()
     ms = ev0.elapsed_time(ev1)
     sol.Sync()
     info1 = sol.Info()
     pst = int(info1.particle_steps - info0.particle_steps)
     ms_max, total_ps = reduce_over_ranks(ms, pst, world, dev)
     value = total_ps / (ms_max * 1e-3)
-    launches = sum(v[1] for v in prof.values())
+    launches = args.steps * kernels_per_step(wl["settings"], variant, wl["mesh"] is not None)
     n_avg = pst / args.steps
     # dominant kernel and its roofline
     peaks = {}
@@ -344,10 +384,10 @@ def run_ours(args, rank, world):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    dom = max(("scatter", "cell"), key=lambda k: prof[k][0])
-    dom_ms = prof[dom][0] / max(prof[dom][1], 1)
+    dom = dom_slot if split or dom_slot != "collide" else "cell"
+    dom_ms = prof[dom_slot][0] / max(prof[dom_slot][1], 1)
     taus = wl["settings"].get("rng", "taus") == "taus"
-    alg = algorithmic_bytes(dom, n_avg, sol.Info().cells, taus, 1.0 / 100)
+    alg = algorithmic_bytes(dom, n_avg, sol.Info().cells, taus, 1.0 / 100, split)
     achieved = alg / (dom_ms * 1e-3) / 1e9
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "dram_traffic.json")
@@ -359,7 +399,10 @@ def run_ours(args, rank, world):
         except (OSError, ValueError, KeyError):
             traffic = None
     kernels = {k: {"ms_per_launch": (v[0] / v[1] if v[1] else None), "launches": v[1],
-                   "share": v[0] / max(sum(x[0] for x in prof.values()), 1e-12)} for k, v in prof.items()}
+                   "share": v[0] / max(sum(x[0] for x in breakdown.values()), 1e-12)}
+               for k, v in breakdown.items()}
+    kernels["window"] = (f"{bsteps} steps before the timed region, CUDA events around every "
+                         "kernel; the timed region times only the dominant kernel")
     # whole-step roofline at 128 B per particle-timestep (algorithmic)
     step_frac = value / max(world, 1) * 128 / (peak * 1e9)
     # end-to-end through the C ABI with host buffers
@@ -466,7 +509,9 @@ def run_batch(args, rank, world):
                    "l2_policy": "working set of all members (several GB) > 126 MB L2"},
         "sequential": {"value": seq_value, "ms_per_step": seq_ms / k2,
                        "note": "same members, one graph launch per member per step, one stream"},
-        "gpu_launches": args.steps * 4 * len(sols),  # scan, scatter, cell, inflow per member
+        "gpu_launches": args.steps * sum(kernels_per_step(m["settings"], v, True)
+                                         for m, v in zip(wl["members"],
+                                                         variants or [5] * len(wl["members"]))),
         "clocks": clk.summary(),
     }
     batch.close()

@@ -124,6 +124,8 @@ SIGNATURES = [
     ("dsmc_to_bf16", _I, [_P, _P, ctypes.c_size_t, _P]),
     ("dsmc_set_kernel_variant", _I, [_P, _I]),
     ("dsmc_get_kernel_variant", _I, [_P, _P, _P]),
+    ("dsmc_profile_read_kernels", _I, [_P, _I, _P, _P]),
+    ("dsmc_profile_mask", _I, [_P, ctypes.c_uint32]),
     ("dsmc_kernel_variant_count", _I, []),
     ("dsmc_autotune", _I, [_P, ctypes.c_float, _I, _P, _P]),
     ("dsmc_batch_create", _I, [_P, _U32, _P]),

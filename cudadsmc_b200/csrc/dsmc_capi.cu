@@ -61,11 +61,14 @@ struct dsmc_handle {
 
   // per-kernel event timing (dsmc_profile)
   bool profiling = false;
+  uint32_t prof_mask = 0x7f;  // slots that get events while profiling
   std::vector<cudaEvent_t> ev;      // pairs
   std::vector<int> ev_kernel;       // kernel id of each pair
   size_t ev_used = 0;
-  double prof_ms[4] = {0, 0, 0, 0};
-  uint32_t prof_n[4] = {0, 0, 0, 0};
+  // slots: 0 scan, 1 scatter, 2 cell (fused) / collide (split), 3 injection,
+  // 4 flight, 5 mesh flights, 6 sampling (split)
+  double prof_ms[7] = {0, 0, 0, 0, 0, 0, 0};
+  uint32_t prof_n[7] = {0, 0, 0, 0, 0, 0, 0};
 
   std::string err;
 };
@@ -232,7 +235,7 @@ void prof_flush(dsmc_handle* h) {
 // Launches `launch` with CUDA events around it when the handle is profiling.
 template <class F>
 cudaError_t timed(dsmc_handle* h, int kernel, F launch) {
-  if (!h->profiling) return launch();
+  if (!h->profiling || !((h->prof_mask >> kernel) & 1u)) return launch();
   if (h->ev_used == kProfPairs) prof_flush(h);
   size_t i = h->ev_used++;
   h->ev_kernel[i] = kernel;
@@ -269,8 +272,18 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
   if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
   p.cell_variant = h->variant;
   p.defer_list = h->orig;
-  e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
-  if (e) return e;
+  if (split) {
+    static const int slot[4] = {2, 4, 5, 6};
+    for (int stage = 0; stage < 4; stage++) {
+      e = timed(h, slot[stage], [&] {
+        return dsmcb::launch_split_stage(p, h->variant - 4, stage, h->stream);
+      });
+      if (e) return e;
+    }
+  } else {
+    e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
+    if (e) return e;
+  }
   for (const auto& in : h->inflows) {
     dsmcb::InjectParams ip{};
     ip.grid = h->grid;
@@ -552,11 +565,18 @@ int dsmc_profile(dsmc_handle* h, int enable) {
       for (auto& e : h->ev) CK(h, cudaEventCreate(&e), "event create");
     }
     h->ev_used = 0;
-    for (int k = 0; k < 4; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+    for (int k = 0; k < 7; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
   } else {
     prof_flush(h);
   }
   h->profiling = enable != 0;
+  h->prof_mask = 0x7f;
+  return DSMC_OK;
+}
+
+int dsmc_profile_mask(dsmc_handle* h, uint32_t slots) {
+  if (!h || !h->profiling) return fail(h, DSMC_ERR_STATE, "dsmc_profile_mask needs an open window");
+  h->prof_mask = slots & 0x7fu;
   return DSMC_OK;
 }
 
@@ -564,6 +584,19 @@ int dsmc_profile_read(dsmc_handle* h, double ms[4], uint32_t launches[4]) {
   if (!h || !ms || !launches) return DSMC_ERR_ARG;
   prof_flush(h);
   for (int k = 0; k < 4; k++) { ms[k] = h->prof_ms[k]; launches[k] = h->prof_n[k]; }
+  // the cell work of the split variants: collide + flight + mesh + sampling
+  for (int k = 4; k < 7; k++) ms[2] += h->prof_ms[k];
+  h->profiling = false;
+  return DSMC_OK;
+}
+
+int dsmc_profile_read_kernels(dsmc_handle* h, int n, double* ms, uint32_t* launches) {
+  if (!h || !ms || !launches || n < 1) return DSMC_ERR_ARG;
+  prof_flush(h);
+  for (int k = 0; k < n; k++) {
+    ms[k] = k < 7 ? h->prof_ms[k] : 0.0;
+    launches[k] = k < 7 ? h->prof_n[k] : 0u;
+  }
   h->profiling = false;
   return DSMC_OK;
 }

@@ -1,37 +1,36 @@
-// The timestep's cell work as two warp-autonomous kernels (sm_100a).
+// The timestep's cell work as warp-autonomous kernels (sm_100a); none has a
+// CTA-wide barrier inside its loop.
 //
-// Both kernels hand out tiles of 32 consecutive cells to warps (lane L owns
-// cell L of a tile; tiles past the first wave come from a dynamic counter),
-// and neither has a CTA-wide barrier inside its loop.
-//
-// k_collide_w (order + collisions): a tile is cut into chunks of whole cells
-// holding at most CAPW particles.  The particle arrays of a chunk (x, y, z,
-// u, v, w, orig) are staged in the warp's slice of shared memory by 1-D bulk
-// copies completing on the warp's mbarrier, double buffered (the copy of the
-// next chunk is in flight while the current one is processed):
-//   A  cell of each staged particle; rank by orig inside the cell (the stable
-//      order of the reference's sort)
+// k_collide_w (order + collisions): warps take tiles of 32 consecutive cells
+// (lane L owns cell L; tiles past the first wave come from a dynamic counter)
+// and cut them into chunks of whole cells holding at most CAPW particles.  A
+// chunk's orig (the pre-scatter index of every sorted slot) is staged in the
+// warp's slice of shared memory by a 1-D bulk copy completing on the warp's
+// mbarrier, double buffered (the next chunk's copy is in flight while the
+// current one is processed); then
+//   A  the chunk's state is gathered from the unsorted array through orig by
+//      asynchronous 4-byte copies, while the cell of each slot and its rank
+//      by orig inside the cell (the stable order of the reference's sort) are
+//      computed
 //   B  NTC collisions: light cells one lane each, dense cells (Philox mode)
 //      one whole warp each
-//   C  the chunk back to global memory in sorted order
-// k_flight_w (flight + keys): streams the tile's particles, 32 at a time:
-// free flight and boundaries, next-step key and count (warp-aggregated
-// atomics on the per-cell counts and the per scan tile totals, so the kernel
-// has no CTA-wide barrier at all).  Flights that may reach the body are
-// listed instead: they cluster in the tiles next to the body, so
-// k_mesh_w flies them afterwards one per thread over the whole GPU.
-// k_sample_w then samples (FP64) on sampling steps.
+//   C  the chunk goes to the mid arrays in sorted order
+// k_flight_w (flight + keys): streams the sorted particles, 32 at a time per
+// warp in grid-stride order: free flight and boundaries, next-step key and
+// count (warp-aggregated atomics on the per-cell counts and on the per scan
+// tile totals).  Flights that may reach the body are listed instead: they
+// cluster next to the body, so k_mesh_w flies them afterwards one per thread
+// over the whole GPU.  k_sample_w samples (FP64) on sampling steps.
 //
 // The per-cell and per-particle arithmetic is that of the fused CTA-wide
 // kernel (dsmc_cell.cu), in the same order, so both compute the same step for
-// every cell that fits a chunk; the split only costs one more pass over the
-// state (24 B written + 24 B read per particle) and lets each kernel run at
-// its own register budget and occupancy.
+// every cell that fits a chunk.  Gathering through orig lets the scatter write
+// orig alone (one scattered 4-byte store per particle instead of seven).
 //
-// Traffic per particle: k_collide_w 28 B read (state + orig) + 24 B written;
-// k_flight_w 24 B read + 28 B written (state + key).  Per cell: 8 B of starts
-// per kernel, 16 B ((sigma g)max read + write), 32 B more in the reference
-// RNG mode, 80 B on sampling steps.
+// Traffic per particle: k_collide_w orig 4 + state 24 read, 24 written;
+// k_flight_w 24 read, 24 + key 4 written.  Per cell: 8 B of starts, 16 B of
+// (sigma g)max read + written, 32 B more in the reference RNG mode, 80 B of
+// sampling sums on sampling steps.
 #include "dsmc_bulk.cuh"
 #include "dsmc_step_dev.cuh"
 
@@ -390,69 +389,65 @@ __device__ __forceinline__ void list_deferred(const StepParams& p, const uint32_
   if (lane < cnt) p.defer_list[base + lane] = q[from + lane];
 }
 
-// Free flights, 32 particles at a time per warp, read from p.mid (the sorted
-// state k_collide_w produced) and written to p.out.  Flights that may reach
-// the body are listed for k_mesh_w instead, which spreads them over the whole
-// GPU (they cluster in the tiles next to the body).
+// Free flights of the sorted particles [0, n_alive), read from p.mid (the
+// state k_collide_w produced) and written to p.out.  Warps take groups of 32
+// in grid-stride order (the work per particle is even once the flights that
+// may reach the body are listed for k_mesh_w, which spreads them over the
+// whole GPU: they cluster next to the body).  The state of a group is loaded
+// two iterations ahead, and in nearest mode the clearance lookup of its
+// deferral test one iteration ahead, so that both latencies are covered.
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
   __shared__ uint32_t s_q[WARPS][kFlightQ];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const uint32_t n = p.meta->n_alive;
   const bool do_move = (p.flags & kDoMove) != 0;
   const bool split = p.has_geom && do_move;
+  const bool piped = split && p.geom.nearest;
   uint32_t* q = s_q[warp];
-
-  const uint32_t nwarps = gridDim.x * WARPS;
-  const uint32_t gw = blockIdx.x * WARPS + warp;
-  TileQueue tq{nwarps, gw + nwarps, p.meta ? &p.meta->tile_next2 : nullptr};
-  uint32_t tnext = 0;
-  if (lane == 0 && gw < p.n_tiles) tnext = tq.grab();
+  const uint32_t stride = gridDim.x * WARPS * 32u;
+  const uint32_t g0 = (blockIdx.x * WARPS + warp) * 32u + lane;
+  auto load = [&](uint32_t g, float3& pos, float3& vel) {
+    if (g < n) {
+      pos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
+      vel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
+    }
+  };
+  const float3 zero = make_float3(0.f, 0.f, 0.f);
+  float3 pos0 = zero, vel0 = zero;  // group g
+  float3 pos1 = zero, vel1 = zero;  // group g + stride
+  float3 pos2 = zero, vel2 = zero;  // group g + 2 stride
+  load(g0, pos0, vel0);
+  load(g0 + stride, pos1, vel1);
+  float clr0 = -1.f;
+  if (piped && g0 < n) clr0 = defer_lookup(p, pos0);
   uint32_t removed = 0, nq = 0;
-  WTile T = load_tile(p, gw);
-  while (T.t < p.n_tiles) {
-    // the warp's next tile (its starts load while this one is flown); lane 0
-    // asks for the one after it
-    const uint32_t t2 = __shfl_sync(kFull, tnext, 0);
-    if (lane == 0 && t2 < p.n_tiles) tnext = tq.grab();
-    const WTile T2 = load_tile(p, t2);
-    const uint32_t ts = __shfl_sync(kFull, T.s, 0), te = __shfl_sync(kFull, T.e, T.nct - 1u);
-    // the state of the first group of 32; each iteration loads the next
-    // group's while it flies the current one
-    float3 npos = make_float3(0.f, 0.f, 0.f), nvel = npos;
-    if (ts + lane < te) {
-      const uint32_t g = ts + lane;
-      npos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
-      nvel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
+  for (uint32_t g = g0; g - lane < n; g += stride) {
+    const bool active = g < n;
+    load(g + 2u * stride, pos2, vel2);
+    float clr1 = -1.f;
+    if (piped && g + stride < n) clr1 = defer_lookup(p, pos1);
+    float3 pos = pos0, vel = vel0;
+    bool defer = false;
+    if (active && split)
+      defer = piped ? defer_decide(p, pos, vel, clr0) : flight_may_meet_body(p, pos, vel);
+    const unsigned dm = __ballot_sync(kFull, defer);
+    if (defer) q[nq + __popc(dm & ((1u << lane) - 1u))] = g;
+    nq += __popc(dm);
+    const bool go = active && !defer;
+    bool live = true;
+    // a path that cannot reach the body
+    if (go && do_move) live = move_free(p, pos, vel, g, step);
+    finish_flight(p, go, live, g, pos, vel, removed);
+    if (nq >= 32) {
+      __syncwarp();
+      nq -= 32;
+      list_deferred(p, q, nq, 32);
+      __syncwarp();
     }
-    for (uint32_t qb = ts; qb < te; qb += 32) {
-      const uint32_t g = qb + lane;
-      const bool active = g < te;
-      const float3 pos0 = npos, vel0 = nvel;
-      if (g + 32u < te) {
-        const uint32_t gn = g + 32u;
-        npos = make_float3(p.mid.x[gn], p.mid.y[gn], p.mid.z[gn]);
-        nvel = make_float3(p.mid.u[gn], p.mid.v[gn], p.mid.w[gn]);
-      }
-      float3 pos = pos0, vel = vel0;
-      bool defer = false;
-      if (active && split) defer = flight_may_meet_body(p, pos, vel);
-      const unsigned dm = __ballot_sync(kFull, defer);
-      if (defer) q[nq + __popc(dm & ((1u << lane) - 1u))] = g;
-      nq += __popc(dm);
-      const bool go = active && !defer;
-      bool live = true;
-      // a path that cannot reach the body
-      if (go && do_move) live = move_free(p, pos, vel, g, step);
-      finish_flight(p, go, live, g, pos, vel, removed);
-      if (nq >= 32) {
-        __syncwarp();
-        nq -= 32;
-        list_deferred(p, q, nq, 32);
-        __syncwarp();
-      }
-    }
-    T = T2;
+    pos0 = pos1; vel0 = vel1; clr0 = clr1;
+    pos1 = pos2; vel1 = vel2;
   }
   if (nq) {
     __syncwarp();
@@ -558,11 +553,9 @@ cudaError_t launch_flight_w(const StepParams& p, cudaStream_t stream) {
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  uint32_t grid = (uint32_t)(num_sms() * ls.per_sm);
-  const uint32_t need = (p.n_tiles + kFlightWarps - 1) / kFlightWarps;
-  if (grid > need) grid = need;
-  if (grid == 0) return cudaSuccess;
-  k_flight_w<kFlightWarps, MINB><<<grid, kFlightWarps * 32, 0, stream>>>(p);
+  // a full wave of warps: the particle count is known only on the device
+  k_flight_w<kFlightWarps, MINB>
+      <<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32, 0, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -607,26 +600,32 @@ int cell_kernel_w_capacity(int v) {
 
 uint32_t cell_kernel_w_tile() { return kWarpTile; }
 
+cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream_t stream) {
+  switch (stage) {
+    case 0:
+      switch (v) {
+        case 0: return launch_collide_w<256, 4, 4>(p, stream);
+        case 2: return launch_collide_w<128, 8, 3>(p, stream);
+        case 3: return launch_collide_w<128, 4, 8>(p, stream);
+        default: return launch_collide_w<128, 4, 4>(p, stream);
+      }
+    case 1:
+      return (v == 2 || v == 3) ? launch_flight_w<4>(p, stream) : launch_flight_w<3>(p, stream);
+    case 2:
+      // flights that may reach the body (listed only with a body and the move)
+      if (p.has_geom && (p.flags & kDoMove)) return launch_mesh_w<4>(p, stream);
+      return cudaSuccess;
+    default:
+      if (p.flags & kDoSample) return launch_sample_w(p, stream);
+      return cudaSuccess;
+  }
+}
+
 cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream) {
-  cudaError_t e;
-  switch (v) {
-    case 0: e = launch_collide_w<256, 4, 4>(p, stream); break;
-    case 2: e = launch_collide_w<128, 8, 3>(p, stream); break;
-    case 3: e = launch_collide_w<128, 4, 8>(p, stream); break;
-    default: e = launch_collide_w<128, 4, 4>(p, stream); break;
-  }
-  if (e != cudaSuccess) return e;
-  switch (v) {
-    case 2: case 3: e = launch_flight_w<4>(p, stream); break;
-    default: e = launch_flight_w<3>(p, stream); break;
-  }
-  if (e != cudaSuccess) return e;
-  // flights that may reach the body (listed only with a body and the move)
-  if (p.has_geom && (p.flags & kDoMove)) {
-    e = launch_mesh_w<4>(p, stream);
+  for (int stage = 0; stage < 4; stage++) {
+    const cudaError_t e = launch_split_stage(p, v, stage, stream);
     if (e != cudaSuccess) return e;
   }
-  if (p.flags & kDoSample) return launch_sample_w(p, stream);
   return cudaSuccess;
 }
 

@@ -157,6 +157,9 @@ int cell_kernel_w_variants();
 int cell_kernel_w_capacity(int v);
 uint32_t cell_kernel_w_tile();
 cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream);
+// One kernel of the split variants: 0 collide, 1 flight, 2 mesh flights,
+// 3 sampling (launch_cell_w runs the four in order).
+cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream_t stream);
 // Free flight + boundaries in place on p.out for n particles (move stage);
 // particles that leave through an outflow face get x = NaN.
 cudaError_t launch_move(const StepParams& p, uint32_t n, uint32_t step, cudaStream_t stream);

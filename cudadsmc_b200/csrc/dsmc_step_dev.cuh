@@ -495,6 +495,23 @@ __device__ __forceinline__ bool move_free(const StepParams& p, float3& pos, floa
   return apply_bc(p, pos, vel, rng);
 }
 
+// The deferral test of flight_may_meet_body in nearest mode, in two halves so
+// that the table lookup can be issued ahead of the decision: the clearance of
+// the start position's geometry cell (-1 outside the geometry grid), then the
+// decision from it (the same arithmetic as flight_may_meet_body).
+__device__ __forceinline__ float defer_lookup(const StepParams& p, float3 pos) {
+  const uint32_t sc = coll_cell_id(p.geom.grid, pos);
+  return sc == kNone ? -1.f : __ldg(&p.geom.clear[sc]);
+}
+__device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, float3 vel, float clr) {
+  const float3 e = make_float3(pos.x + vel.x * p.dt, pos.y + vel.y * p.dt, pos.z + vel.z * p.dt);
+  if (clr >= 0.f) {
+    const float dist = length3(make_float3(e.x - pos.x, e.y - pos.y, e.z - pos.z));
+    return !(dist < clr);
+  }
+  return path_box_meets_grid(p.geom.grid, pos, e);
+}
+
 // One particle's flight with the body: IntegrateDev / ProcessCollisionsDev,
 // kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.  Out
 // of line: only flights that may reach the body come here in the step.

@@ -202,6 +202,25 @@ class DSMCSolver:
         self._check(lib().dsmc_profile_read(self.h, _ptr(ms), _ptr(n)), "ProfileRead")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNELS)}
 
+    KERNEL_SLOTS = ("scan", "scatter", "collide", "inject", "flight", "mesh", "sample")
+
+    def ProfileOnly(self, kernels):
+        """Keeps the open profile window's events to the named kernels."""
+        mask = 0
+        for k in kernels:
+            mask |= 1 << self.KERNEL_SLOTS.index(k)
+        self._check(lib().dsmc_profile_mask(self.h, mask), "ProfileOnly")
+
+    def ProfileReadKernels(self):
+        """{kernel: (total ms, launches)} since Profile(True), kernel by kernel
+        ("collide" is the fused cell kernel when a variant below 4 runs)."""
+        n = len(self.KERNEL_SLOTS)
+        ms = np.zeros(n, np.float64)
+        cnt = np.zeros(n, np.uint32)
+        self._check(lib().dsmc_profile_read_kernels(self.h, n, _ptr(ms), _ptr(cnt)),
+                    "ProfileReadKernels")
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(self.KERNEL_SLOTS) if cnt[i]}
+
     def UploadState(self, pos, vel=None, soa=False):
         """soa=True: pos is a [6, n] float32 array (x,y,z,u,v,w); else pos/vel
         are [n, 4] float4 arrays as the reference's particles_state_t."""
