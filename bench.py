@@ -340,7 +340,12 @@ def run_ours(args, rank, world):
     # warm-up (also develops the flow a little), then the launch-shape
     # autotuner of the cell kernel on real steps of the run
     sol.RunSimulationStep(dt, args.warmup)
-    variant, tune_ms = sol.Autotune(dt, steps=args.tune_steps)
+    if args.tune_steps > 0:
+        variant, tune_ms = sol.Autotune(dt, steps=args.tune_steps)
+    else:
+        # a fixed launch shape (profiling runs)
+        sol.SetKernelVariant(args.variant)
+        variant, tune_ms = args.variant, None
     split = variant >= 4
     # per-kernel breakdown on a short window with events around every kernel
     # (an event pair costs the GPU a few microseconds, so the timed region
@@ -587,7 +592,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=100)
-    ap.add_argument("--tune-steps", type=int, default=10)
+    ap.add_argument("--tune-steps", type=int, default=10,
+                    help="steps per launch shape of the autotuner (0: use --variant)")
+    ap.add_argument("--variant", type=int, default=5,
+                    help="cell-kernel launch shape when --tune-steps is 0")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -52,6 +52,7 @@ class Info(ctypes.Structure):
         ("step", ctypes.c_uint64), ("samples", ctypes.c_uint32), ("sim_time", ctypes.c_double),
         ("particle_steps", ctypes.c_uint64), ("injected", ctypes.c_uint32),
         ("removed", ctypes.c_uint32), ("giant_cells", ctypes.c_uint32),
+        ("mesh_flights", ctypes.c_uint32),
     ]
 
 
@@ -126,6 +127,7 @@ SIGNATURES = [
     ("dsmc_get_kernel_variant", _I, [_P, _P, _P]),
     ("dsmc_profile_read_kernels", _I, [_P, _I, _P, _P]),
     ("dsmc_profile_mask", _I, [_P, ctypes.c_uint32]),
+    ("dsmc_clearance_at", _I, [_P, _P, _U32, _P, _P]),
     ("dsmc_kernel_variant_count", _I, []),
     ("dsmc_autotune", _I, [_P, ctypes.c_float, _I, _P, _P]),
     ("dsmc_batch_create", _I, [_P, _U32, _P]),

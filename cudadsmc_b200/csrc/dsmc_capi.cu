@@ -47,6 +47,7 @@ struct dsmc_handle {
   uint2* gse = nullptr;
   float4* gtri = nullptr;
   float4* gplane = nullptr;
+  GridGeom gcgrid{};  // grid of the clearance table gclear
 
   bool has_state = false;
   uint64_t step = 0;
@@ -197,6 +198,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.tri = h->gtri;
     p.geom.plane = h->gplane;
     p.geom.clear = h->gclear;
+    p.geom.cgrid = h->gcgrid;
     p.geom.diffuse = h->cfg.wall_diffuse;
     p.geom.nearest = h->cfg.geom_nearest;
     p.geom.wall_vstd = std::sqrt(1.3806e-23f * h->cfg.wall_temp / h->cfg.gas_mass);
@@ -553,6 +555,7 @@ int dsmc_get_info(dsmc_handle* h, dsmc_info* info) {
   info->injected = m.injected;
   info->removed = m.removed;
   info->giant_cells = m.giant_cells;
+  info->mesh_flights = m.n_defer;
   return DSMC_OK;
 }
 
@@ -665,9 +668,10 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
     }
     off += g.count[c];
   }
-  // clearance: (Chebyshev cell distance to the nearest cell holding triangles
-  // - 1) x the smallest cell size, a lower bound of the distance from any point
-  // of the cell to the surface (multi-source BFS over the 26-neighbourhood)
+  // Chebyshev cell distance of every cell to the nearest cell holding
+  // triangles (multi-source BFS over the 26-neighbourhood): (distance - 1) x
+  // the smallest cell size bounds the distance from any point of the cell to
+  // the surface; the clearance table refines it next to the body
   std::vector<int> dist(gc, -1);
   std::vector<uint32_t> queue;
   queue.reserve(gc);
@@ -688,9 +692,10 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
         }
   }
   const float cmin = std::min(g.cell[0], std::min(g.cell[1], g.cell[2]));
-  std::vector<float> clear(gc);
-  for (uint32_t c = 0; c < gc; c++)
-    clear[c] = dist[c] <= 0 ? (dist[c] < 0 ? 3.0e38f : 0.f) : 0.999f * (float)(dist[c] - 1) * cmin;
+  // the clearance table lives on the triangle grid refined by cfac (2 unless
+  // that would pass 16.8M cells); it is filled on the device below
+  const uint32_t cfac = (uint64_t)gc * 8 <= (16u << 20) ? 2u : 1u;
+  const uint32_t fc = gc * cfac * cfac * cfac;
   cudaFree(h->gflags);
   cudaFree(h->gclear);
   cudaFree(h->gse);
@@ -699,17 +704,37 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
   h->gflags = nullptr; h->gclear = nullptr; h->gse = nullptr; h->gtri = nullptr;
   h->gplane = nullptr;
   CK(h, dalloc(&h->gflags, gc), "geometry alloc");
-  CK(h, dalloc(&h->gclear, gc), "geometry alloc");
+  CK(h, dalloc(&h->gclear, fc), "geometry alloc");
   CK(h, dalloc(&h->gse, gc), "geometry alloc");
   CK(h, dalloc(&h->gtri, tri.size()), "geometry alloc");
   CK(h, dalloc(&h->gplane, plane.size()), "geometry alloc");
   CK(h, cudaMemcpy(h->gflags, flags.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
-  CK(h, cudaMemcpy(h->gclear, clear.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
+
   CK(h, cudaMemcpy(h->gse, se.data(), gc * sizeof(uint2), cudaMemcpyHostToDevice), "geometry upload");
   CK(h, cudaMemcpy(h->gtri, tri.data(), tri.size() * sizeof(float4), cudaMemcpyHostToDevice),
      "geometry upload");
   CK(h, cudaMemcpy(h->gplane, plane.data(), plane.size() * sizeof(float4), cudaMemcpyHostToDevice),
      "geometry upload");
+  {
+    h->gcgrid.gmin = make_float3(g.bbox[0], g.bbox[1], g.bbox[2]);
+    h->gcgrid.gmax = make_float3(g.bbox[3], g.bbox[4], g.bbox[5]);
+    h->gcgrid.cell = make_float3(g.cell[0] / cfac, g.cell[1] / cfac, g.cell[2] / cfac);
+    h->gcgrid.dim = make_uint3(g.dim[0] * cfac, g.dim[1] * cfac, g.dim[2] * cfac);
+    dsmcb::GeomView gv{};
+    gv.grid.gmin = h->gcgrid.gmin;
+    gv.grid.gmax = h->gcgrid.gmax;
+    gv.grid.cell = make_float3(g.cell[0], g.cell[1], g.cell[2]);
+    gv.grid.dim = make_uint3(g.dim[0], g.dim[1], g.dim[2]);
+    gv.start_end = h->gse;
+    gv.tri = h->gtri;
+    int* ddist = nullptr;
+    CK(h, cudaMalloc(&ddist, gc * sizeof(int)), "geometry alloc");
+    cudaError_t ce = cudaMemcpy(ddist, dist.data(), gc * sizeof(int), cudaMemcpyHostToDevice);
+    if (!ce) ce = dsmcb::launch_fine_clearance(gv, h->gcgrid, cfac, ddist, cmin, h->gclear, nullptr);
+    if (!ce) ce = cudaDeviceSynchronize();
+    cudaFree(ddist);
+    CK(h, ce, "clearance table");
+  }
   h->has_geom = true;
   h->cfg.geometry = 1;
   drop_graph(h);
@@ -1496,6 +1521,14 @@ int dsmc_stage_move(dsmc_handle* h, const dsmc_move_params* mp, float* x, float*
   p.out = SoA{x, y, z, u, v, w};
   cudaError_t e = dsmcb::launch_move(p, n, mp->step ? mp->step : 1u, (cudaStream_t)stream);
   return e ? DSMC_ERR_CUDA : DSMC_OK;
+}
+
+int dsmc_clearance_at(dsmc_handle* h, const float* xyz, uint32_t n, float* out, void* stream) {
+  if (!h || (n && (!xyz || !out))) return DSMC_ERR_ARG;
+  if (!h->has_geom) return fail(h, DSMC_ERR_STATE, "no geometry");
+  dsmcb::StepParams p = base_params(h, h->cfg.dt);
+  cudaError_t e = dsmcb::launch_clearance_at(p.geom, xyz, n, out, (cudaStream_t)stream);
+  return e ? cuda_fail(h, e, "clearance lookup") : DSMC_OK;
 }
 
 int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint32_t* cell_start,

@@ -589,7 +589,7 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 // CTA-wide ones): (particles per warp chunk, warps per CTA, register cap) of
 // the order + collide kernel and the register cap of the flight kernel (8
 // warps per CTA): 0 (256, 4, 128; 80), 1 (128, 4, 128; 80), 2 (128, 8, 80;
-// 64), 3 (128, 4, 64; 64).  The mesh kernel runs at 64 registers (more warps
+// 64), 3 (128, 4, 96; 64).  The mesh kernel runs at 64 registers (more warps
 // to cover its chains of L2 loads).
 int cell_kernel_w_variants() { return 4; }
 
@@ -606,7 +606,7 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
       switch (v) {
         case 0: return launch_collide_w<256, 4, 4>(p, stream);
         case 2: return launch_collide_w<128, 8, 3>(p, stream);
-        case 3: return launch_collide_w<128, 4, 8>(p, stream);
+        case 3: return launch_collide_w<128, 4, 5>(p, stream);
         default: return launch_collide_w<128, 4, 4>(p, stream);
       }
     case 1:

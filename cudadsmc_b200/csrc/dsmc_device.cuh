@@ -183,8 +183,10 @@ struct GeomView {
   // per bin entry, the triangle's plane (unit normal, offset), packed apart
   // from the vertices so that a cell's planes share cache lines
   const float4* plane;
-  // per cell, a lower bound of the distance from any point of the cell to the
-  // surface (0 in cells holding triangles)
+  // clearance table: per cell of cgrid (the triangle grid refined by a small
+  // factor, same bounds), a lower bound of the distance from any point of the
+  // cell to the surface
+  GridGeom cgrid;
   const float* clear;
   int diffuse;        // 0: specular (reference); 1: diffuse at wall_temp
   float wall_vstd;    // sqrt(k T_wall / m)

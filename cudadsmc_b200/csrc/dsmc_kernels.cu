@@ -676,6 +676,108 @@ __global__ void k_outside_fraction(const GridGeom grid, const __grid_constant__ 
   }
 }
 
+// Distance from q to the triangle (a, b, c): inside the prism over the
+// triangle the distance to its plane, otherwise the nearest of its edges
+// (closest point of each edge segment).
+__device__ float point_triangle_distance(float3 q, float3 a, float3 b, float3 c) {
+  const float3 ab = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
+  const float3 bc = make_float3(c.x - b.x, c.y - b.y, c.z - b.z);
+  const float3 ca = make_float3(a.x - c.x, a.y - c.y, a.z - c.z);
+  const float3 n = make_float3(ab.y * (-ca.z) - ab.z * (-ca.y), ab.z * (-ca.x) - ab.x * (-ca.z),
+                               ab.x * (-ca.y) - ab.y * (-ca.x));
+  const float nn = n.x * n.x + n.y * n.y + n.z * n.z;
+  auto side = [&](float3 e, float3 p0) {
+    const float3 r = make_float3(q.x - p0.x, q.y - p0.y, q.z - p0.z);
+    const float3 x = make_float3(e.y * r.z - e.z * r.y, e.z * r.x - e.x * r.z, e.x * r.y - e.y * r.x);
+    return x.x * n.x + x.y * n.y + x.z * n.z;
+  };
+  if (nn > 0.f && side(ab, a) >= 0.f && side(bc, b) >= 0.f && side(ca, c) >= 0.f) {
+    const float h = (q.x - a.x) * n.x + (q.y - a.y) * n.y + (q.z - a.z) * n.z;
+    return fabsf(h) * rsqrtf(nn);
+  }
+  auto seg = [&](float3 p0, float3 e) {
+    const float ee = e.x * e.x + e.y * e.y + e.z * e.z;
+    float t = ee > 0.f ? ((q.x - p0.x) * e.x + (q.y - p0.y) * e.y + (q.z - p0.z) * e.z) / ee : 0.f;
+    t = fminf(fmaxf(t, 0.f), 1.f);
+    const float3 d = make_float3(q.x - (p0.x + t * e.x), q.y - (p0.y + t * e.y), q.z - (p0.z + t * e.z));
+    return sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+  };
+  return fminf(seg(a, ab), fminf(seg(b, bc), seg(c, ca)));
+}
+
+// Clearance table on the refined grid `fine` (fac x fac x fac cells per cell
+// of the triangle grid).  cdist holds each triangle-grid cell's Chebyshev
+// distance in cells to the nearest cell holding triangles (-1: none at all).
+// Cells at distance >= 2 keep the cell-count bound (cdist - 1) * cmin; the
+// others take the exact distance from their centre to the triangles of the
+// 27 triangle-grid cells around, less half their diagonal, capped by cmin
+// (triangles farther out are at least one triangle-grid cell away).  All
+// bounds are scaled by 0.999 to stay below the true distance.
+__global__ void k_fine_clearance(const __grid_constant__ GeomView g, GridGeom fine, uint32_t fac,
+                                 const int* __restrict__ cdist, float cmin, float* out) {
+  const uint32_t n = fine.dim.x * fine.dim.y * fine.dim.z;
+  const float hd = 0.5f * sqrtf(fine.cell.x * fine.cell.x + fine.cell.y * fine.cell.y +
+                                fine.cell.z * fine.cell.z);
+  for (uint32_t f = blockIdx.x * blockDim.x + threadIdx.x; f < n; f += gridDim.x * blockDim.x) {
+    const uint32_t fx = f % fine.dim.x, fy = (f / fine.dim.x) % fine.dim.y,
+                   fz = f / (fine.dim.x * fine.dim.y);
+    const int cx = (int)(fx / fac), cy = (int)(fy / fac), cz = (int)(fz / fac);
+    const int D = cdist[((uint32_t)cz * g.grid.dim.y + (uint32_t)cy) * g.grid.dim.x + (uint32_t)cx];
+    float c;
+    if (D < 0) {
+      c = 3.0e38f;
+    } else if (D >= 2) {
+      c = 0.999f * (float)(D - 1) * cmin;
+    } else {
+      const float3 q = make_float3(fine.gmin.x + ((float)fx + 0.5f) * fine.cell.x,
+                                   fine.gmin.y + ((float)fy + 0.5f) * fine.cell.y,
+                                   fine.gmin.z + ((float)fz + 0.5f) * fine.cell.z);
+      float best = 3.0e38f;
+      for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+          for (int dx = -1; dx <= 1; dx++) {
+            const int x = cx + dx, y = cy + dy, z = cz + dz;
+            if (x < 0 || y < 0 || z < 0 || x >= (int)g.grid.dim.x || y >= (int)g.grid.dim.y ||
+                z >= (int)g.grid.dim.z)
+              continue;
+            const uint2 se = g.start_end[((uint32_t)z * g.grid.dim.y + (uint32_t)y) * g.grid.dim.x + (uint32_t)x];
+            for (uint32_t i = se.x; i < se.y; i++) {
+              const float4 A = g.tri[kTriStride * (size_t)i], B = g.tri[kTriStride * (size_t)i + 1],
+                           C = g.tri[kTriStride * (size_t)i + 2];
+              best = fminf(best, point_triangle_distance(q, make_float3(A.x, A.y, A.z),
+                                                         make_float3(B.x, B.y, B.z),
+                                                         make_float3(C.x, C.y, C.z)));
+            }
+          }
+      c = 0.999f * fmaxf(0.f, fminf(best - hd, cmin));
+    }
+    out[f] = c;
+  }
+}
+
+__global__ void k_clearance_at(const __grid_constant__ GeomView g, const float* __restrict__ xyz,
+                               uint32_t n, float* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float3 q = make_float3(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2]);
+    const uint32_t c = coll_cell_id(g.cgrid, q);
+    out[i] = c == kNone ? -1.f : g.clear[c];
+  }
+}
+
+cudaError_t launch_clearance_at(const GeomView& g, const float* xyz, uint32_t n, float* out,
+                                cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  k_clearance_at<<<grid_for(n, 256, 8), 256, 0, stream>>>(g, xyz, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fine_clearance(const GeomView& g, const GridGeom& fine, uint32_t fac,
+                                  const int* cdist, float cmin, float* out, cudaStream_t stream) {
+  const uint32_t n = fine.dim.x * fine.dim.y * fine.dim.z;
+  k_fine_clearance<<<grid_for(n, 256, 8), 256, 0, stream>>>(g, fine, fac, cdist, cmin, out);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_outside_fraction(const GridGeom& grid, const GeomView& geom, uint32_t cells,
                                     float* frac, float4* point, cudaStream_t stream) {
   const uint32_t blocks = (uint32_t)std::min<uint64_t>(((uint64_t)cells + 7) / 8, 8u * num_sms());

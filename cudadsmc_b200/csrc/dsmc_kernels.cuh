@@ -210,6 +210,15 @@ cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);
 cudaError_t launch_outside_fraction(const GridGeom& grid, const GeomView& geom, uint32_t cells,
                                     float* frac, float4* point, cudaStream_t stream);
 
+// Clearance table of the deferral test on `fine` (the triangle grid refined
+// by fac), from the triangle grid's CSR and its cell distances cdist.
+cudaError_t launch_fine_clearance(const GeomView& g, const GridGeom& fine, uint32_t fac,
+                                  const int* cdist, float cmin, float* out, cudaStream_t stream);
+
+// out[i] = clearance table entry at point i (xyz interleaved), -1 outside.
+cudaError_t launch_clearance_at(const GeomView& g, const float* xyz, uint32_t n, float* out,
+                                cudaStream_t stream);
+
 // Inflow injection: appends particles after the ones in cells and counts them
 // for the next scan.
 struct InjectParams {

@@ -459,14 +459,15 @@ __device__ __forceinline__ bool path_box_meets_grid(const GridGeom& g, float3 a,
 __device__ __forceinline__ bool flight_may_meet_body(const StepParams& p, float3 pos, float3 vel) {
   const GeomView& G = p.geom;
   const float3 e = make_float3(pos.x + vel.x * p.dt, pos.y + vel.y * p.dt, pos.z + vel.z * p.dt);
-  const uint32_t sc = coll_cell_id(G.grid, pos);
   if (G.nearest) {
-    if (sc != kNone) {
+    const uint32_t cc = coll_cell_id(G.cgrid, pos);
+    if (cc != kNone) {
       const float dist = length3(make_float3(e.x - pos.x, e.y - pos.y, e.z - pos.z));
-      return !(dist < __ldg(&G.clear[sc]));
+      return !(dist < __ldg(&G.clear[cc]));
     }
     return path_box_meets_grid(G.grid, pos, e);
   }
+  const uint32_t sc = coll_cell_id(G.grid, pos);
   const uint32_t ec = coll_cell_id(G.grid, e);
   return (sc != kNone && __ldg(&G.flags[sc]) != 0) || (ec != kNone && __ldg(&G.flags[ec]) != 0);
 }
@@ -500,8 +501,8 @@ __device__ __forceinline__ bool move_free(const StepParams& p, float3& pos, floa
 // the start position's geometry cell (-1 outside the geometry grid), then the
 // decision from it (the same arithmetic as flight_may_meet_body).
 __device__ __forceinline__ float defer_lookup(const StepParams& p, float3 pos) {
-  const uint32_t sc = coll_cell_id(p.geom.grid, pos);
-  return sc == kNone ? -1.f : __ldg(&p.geom.clear[sc]);
+  const uint32_t cc = coll_cell_id(p.geom.cgrid, pos);
+  return cc == kNone ? -1.f : __ldg(&p.geom.clear[cc]);
 }
 __device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, float3 vel, float clr) {
   const float3 e = make_float3(pos.x + vel.x * p.dt, pos.y + vel.y * p.dt, pos.z + vel.z * p.dt);
@@ -532,10 +533,10 @@ static __device__ __noinline__ bool move_particle_full(const StepParams& p, floa
       const float dist = length3(seg);
       if (!(dist > 1e-12f)) break;
       // a path shorter than the start cell's clearance cannot reach the body
-      const uint32_t sc = coll_cell_id(G.grid, old_pos);
-      if (sc != kNone && dist < __ldg(&G.clear[sc])) break;
+      const uint32_t cc = coll_cell_id(G.cgrid, old_pos);
+      if (cc != kNone && dist < __ldg(&G.clear[cc])) break;
       // a path outside the geometry grid whose box misses the grid's box
-      if (sc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
+      if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
       const float idist = 1.f / dist;
       const float3 d = make_float3(seg.x * idist, seg.y * idist, seg.z * idist);
       float t;

@@ -139,6 +139,7 @@ typedef struct dsmc_info {
   uint32_t injected;       /* particles injected by inflow faces (total) */
   uint32_t removed;        /* particles removed through outflow faces (total) */
   uint32_t giant_cells;    /* cells processed outside the shared-memory tiles (total) */
+  uint32_t mesh_flights;   /* flights of the last step tested against the mesh (split variants) */
 } dsmc_info;
 int dsmc_get_info(dsmc_handle* h, dsmc_info* info);
 
@@ -396,6 +397,13 @@ typedef struct dsmc_move_params {
   uint64_t seed;
   uint32_t step;
 } dsmc_move_params;
+
+/* The lower bound of the distance to the body that decides which flights
+ * the step tests against the mesh (no counterpart in the reference, which
+ * tests every flight starting or ending in a cell with triangles): out[i] for
+ * the point xyz[3i..3i+2] (device pointers), -1 outside the geometry grid.
+ * The table is built with the mesh (dsmc_set_mesh). */
+int dsmc_clearance_at(dsmc_handle* h, const float* xyz, uint32_t n, float* out, void* stream);
 
 /* IntegrateDev / ProcessCollisionsDev (kernels/dsmc_kernel.cu:1557-1699):
  * free flight, mesh collisions (with the handle's geometry when h != NULL and
