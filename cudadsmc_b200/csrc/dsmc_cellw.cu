@@ -9,9 +9,9 @@
 // mbarrier, double buffered (the next chunk's copy is in flight while the
 // current one is processed); then
 //   A  the chunk's state is gathered from the unsorted array through orig by
-//      asynchronous 4-byte copies, while the cell of each slot and its rank
-//      by orig inside the cell (the stable order of the reference's sort) are
-//      computed
+//      asynchronous 4-byte copies, while the cell of each slot (binary search
+//      of the chunk's cell starts) and its rank by orig inside the cell (the
+//      stable order of the reference's sort) are computed
 //   B  NTC collisions: light cells one lane each, dense cells (Philox mode)
 //      one whole warp each
 //   C  the chunk goes to the mid arrays in sorted order
@@ -51,7 +51,6 @@ struct __align__(16) WarpSmem {
   uint32_t cs[kWarpTile + 1];  // chunk-relative start of each tile cell
   unsigned long long mbar[2];
   uint16_t slot[CAPW];         // sorted position -> staged index
-  uint8_t cellof[CAPW];        // tile cell (lane) of each staged particle
 };
 
 template <int CAPW, int WARPS>
@@ -200,9 +199,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
   double sum_g = 0.0;
   WChunk C;
   C.valid = 0;
+  // per-cell collision state of a chunk, loaded one chunk ahead of its use
+  float2 mr_c = make_float2(0.f, 0.f);
+  uint4 sd_c = make_uint4(0u, 0u, 0u, 0u);
+  auto load_cell_state = [&](const WChunk& K, uint32_t tile, float2& mr, uint4& sd) {
+    if (do_collide && K.valid && !K.giant && K.n && lane >= K.cur && lane < K.cur + K.k) {
+      const uint32_t c = tile * kWarpTile + lane;
+      mr = p.maxrem[c];
+      if (taus) sd = p.seeds[c];
+    }
+  };
   if (A.t < p.n_tiles) {
     C = make_wchunk<CAPW>(A, 0, 0);
     if (!C.giant && C.n) issue_wchunk(p, S, C);
+    load_cell_state(C, A.t, mr_c, sd_c);
   }
 
   while (C.valid) {
@@ -218,6 +228,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
     }
     const bool n_copy = N.valid && !N.giant && N.n;
     if (n_copy) issue_wchunk(p, S, N);
+    float2 mr_n = make_float2(0.f, 0.f);
+    uint4 sd_n = make_uint4(0u, 0u, 0u, 0u);
+    load_cell_state(N, n_in_b ? B.t : A.t, mr_n, sd_n);
 
     const uint32_t c0 = A.t * kWarpTile;
     const uint32_t cell = c0 + lane;
@@ -225,8 +238,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
     const uint32_t s0 = A.s - C.base, nc = A.e - A.s;  // meaningful for `mine`
     if (!C.giant && C.n) {
       if (do_collide && mine) {
-        S.mr[lane] = p.maxrem[cell];
-        if (taus) S.seeds[lane] = p.seeds[cell];
+        S.mr[lane] = mr_c;
+        if (taus) S.seeds[lane] = sd_c;
       }
       S.cs[lane] = s0;
       if (lane == 31) S.cs[32] = A.e - C.base;
@@ -267,9 +280,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
         cp_async4(V + t, p.in.v + i);
         cp_async4(W + t, p.in.w + i);
       }
-      // A1: cell of each staged particle; dense cells
-      if (do_fixup && mine)
-        for (uint32_t j = s0; j < s0 + nc; j++) S.cellof[j] = (uint8_t)lane;
+      // A1: dense cells
       bool heavy = false;
       if (heavy_mode && mine && nc >= 2)
         heavy = (uint32_t)ntc_fpc_fast(p, nc, S.mr[lane]) >= kHeavyMin;
@@ -285,7 +296,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
           S.slot[t] = (uint16_t)t;
           continue;
         }
-        const uint32_t lc = S.cellof[t];
+        // the slot's cell: the last of the chunk's cells starting at or
+        // before t (an empty cell starts where the next one does)
+        uint32_t lc = C.cur, len = C.k;
+        while (len > 1) {
+          const uint32_t half = len >> 1;
+          if (S.cs[lc + half] <= t) lc += half;
+          len -= half;
+        }
         const uint32_t a = S.cs[lc], b = S.cs[lc + 1];
         const uint32_t my = OR[t];
         const uint32_t lo = a + off, hi = b + off;
@@ -343,6 +361,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
       if (lane == 0 && t2 < p.n_tiles) pend = tq.grab();
     }
     C = N;
+    mr_c = mr_n;
+    sd_c = sd_n;
   }
   const unsigned long long s64 = warp_sum((unsigned long long)sel);
   const unsigned long long c64 = warp_sum((unsigned long long)col);
@@ -457,6 +477,106 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
   if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
 }
 
+// Paired form of k_flight_w: lane L flies particles 2L and 2L+1 of each group
+// of 64, with 8-byte loads and stores (half the memory instructions) and two
+// independent chains per lane.  A deferred particle's slot gets its unmoved
+// state and a dead key here; k_mesh_w, which runs after this kernel, writes
+// both again.
+constexpr uint32_t kFlightQ2 = 128;
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_constant__ StepParams p) {
+  __shared__ uint32_t s_q[WARPS][kFlightQ2];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const uint32_t n = p.meta->n_alive;
+  const bool do_move = (p.flags & kDoMove) != 0;
+  const bool do_keys = (p.flags & kDoKeys) != 0;
+  const bool split = p.has_geom && do_move;
+  uint32_t* q = s_q[warp];
+  const uint32_t stride = gridDim.x * WARPS * 64u;
+  struct Pair {
+    float2 x, y, z, u, v, w;
+  };
+  // state of particles g, g + 1 (g even; g + 1 only below n)
+  auto load = [&](uint32_t g, Pair& s) {
+    if (g + 1u < n) {
+      s.x = *reinterpret_cast<const float2*>(p.mid.x + g);
+      s.y = *reinterpret_cast<const float2*>(p.mid.y + g);
+      s.z = *reinterpret_cast<const float2*>(p.mid.z + g);
+      s.u = *reinterpret_cast<const float2*>(p.mid.u + g);
+      s.v = *reinterpret_cast<const float2*>(p.mid.v + g);
+      s.w = *reinterpret_cast<const float2*>(p.mid.w + g);
+    } else if (g < n) {
+      s.x.x = p.mid.x[g]; s.y.x = p.mid.y[g]; s.z.x = p.mid.z[g];
+      s.u.x = p.mid.u[g]; s.v.x = p.mid.v[g]; s.w.x = p.mid.w[g];
+    }
+  };
+  const uint32_t g0 = (blockIdx.x * WARPS + warp) * 64u + 2u * lane;
+  Pair nxt{};
+  load(g0, nxt);
+  uint32_t removed = 0, nq = 0;
+  for (uint32_t g = g0; g - 2u * lane < n; g += stride) {
+    const Pair cur = nxt;
+    load(g + stride, nxt);
+    float3 pos[2] = {make_float3(cur.x.x, cur.y.x, cur.z.x), make_float3(cur.x.y, cur.y.y, cur.z.y)};
+    float3 vel[2] = {make_float3(cur.u.x, cur.v.x, cur.w.x), make_float3(cur.u.y, cur.v.y, cur.w.y)};
+    bool active[2] = {g < n, g + 1u < n};
+    bool defer[2] = {false, false};
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+      if (active[k] && split) defer[k] = flight_may_meet_body(p, pos[k], vel[k]);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const unsigned dm = __ballot_sync(kFull, defer[k]);
+      if (defer[k]) q[nq + __popc(dm & ((1u << lane) - 1u))] = g + k;
+      nq += __popc(dm);
+    }
+    bool live[2] = {true, true};
+    uint32_t key[2] = {kDeadKey, kDeadKey};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const bool go = active[k] && !defer[k];
+      // a path that cannot reach the body
+      if (go && do_move) live[k] = move_free(p, pos[k], vel[k], g + k, step);
+      if (do_keys) {
+        const bool has_key = go && live[k];
+        const unsigned m = __ballot_sync(kFull, has_key);
+        if (go && !live[k]) removed++;
+        if (has_key) {
+          key[k] = cell_id3d(p.grid, pos[k].x, pos[k].y, pos[k].z);
+          warp_count_key_global(p.count, key[k], m, p.tile_sum);
+        }
+      }
+    }
+    if (active[1]) {
+      *reinterpret_cast<float2*>(p.out.x + g) = make_float2(pos[0].x, pos[1].x);
+      *reinterpret_cast<float2*>(p.out.y + g) = make_float2(pos[0].y, pos[1].y);
+      *reinterpret_cast<float2*>(p.out.z + g) = make_float2(pos[0].z, pos[1].z);
+      *reinterpret_cast<float2*>(p.out.u + g) = make_float2(vel[0].x, vel[1].x);
+      *reinterpret_cast<float2*>(p.out.v + g) = make_float2(vel[0].y, vel[1].y);
+      *reinterpret_cast<float2*>(p.out.w + g) = make_float2(vel[0].z, vel[1].z);
+      if (do_keys) *reinterpret_cast<uint2*>(p.out_key + g) = make_uint2(key[0], key[1]);
+    } else if (active[0]) {
+      p.out.x[g] = pos[0].x; p.out.y[g] = pos[0].y; p.out.z[g] = pos[0].z;
+      p.out.u[g] = vel[0].x; p.out.v[g] = vel[0].y; p.out.w[g] = vel[0].z;
+      if (do_keys) p.out_key[g] = key[0];
+    }
+    while (nq >= 32) {
+      __syncwarp();
+      nq -= 32;
+      list_deferred(p, q, nq, 32);
+      __syncwarp();
+    }
+  }
+  if (nq) {
+    __syncwarp();
+    list_deferred(p, q, 0, nq);
+  }
+  const uint32_t r = warp_sum(removed);
+  if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+}
+
 // The listed flights, one particle per thread over the whole grid (the list's
 // order does not matter: each particle's flight, key and count are its own).
 template <int MINB>
@@ -560,6 +680,27 @@ cudaError_t launch_flight_w(const StepParams& p, cudaStream_t stream) {
 }
 
 template <int MINB>
+cudaError_t launch_flight_pw(const StepParams& p, cudaStream_t stream) {
+  static LaunchShapeW cache[8];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  LaunchShapeW& ls = cache[dev & 7];
+  if (ls.device != dev) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flight_pw<kFlightWarps, MINB>,
+                                                      kFlightWarps * 32, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    ls.device = dev;
+    ls.per_sm = per_sm;
+  }
+  k_flight_pw<kFlightWarps, MINB>
+      <<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+template <int MINB>
 cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
@@ -610,7 +751,12 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         default: return launch_collide_w<128, 4, 4>(p, stream);
       }
     case 1:
-      return (v == 2 || v == 3) ? launch_flight_w<4>(p, stream) : launch_flight_w<3>(p, stream);
+      // 0, 1: single particles per lane; 2, 3: pairs (different register caps)
+      switch (v) {
+        case 2: return launch_flight_pw<3>(p, stream);
+        case 3: return launch_flight_pw<4>(p, stream);
+        default: return launch_flight_w<3>(p, stream);
+      }
     case 2:
       // flights that may reach the body (listed only with a body and the move)
       if (p.has_geom && (p.flags & kDoMove)) return launch_mesh_w<4>(p, stream);

@@ -66,8 +66,12 @@ static __device__ __noinline__ uint4 philox_block(uint32_t b, uint32_t c1, uint3
 }
 
 // A Philox stream: (key, counter words 1..3 fixed) and a running block index
-// in word 0; hands out 32-bit words four at a time.
-struct PhiloxStream {
+// in word 0; hands out 32-bit words four at a time.  INLINE_REFILL expands
+// the ten rounds at the draw site (the collision loops, where a call per
+// refill costs more than the code size); elsewhere the refill is the
+// out-of-line philox_block.  Both give the same words.
+template <bool INLINE_REFILL>
+struct PhiloxStreamT {
   uint2 key;
   uint32_t c1, c2, c3;
   uint32_t block;
@@ -78,7 +82,9 @@ struct PhiloxStream {
   }
   __device__ __forceinline__ uint32_t next() {
     if (used == 4) {
-      buf = philox_block(block++, c1, c2, c3, key);
+      buf = INLINE_REFILL ? philox4x32_10(make_uint4(block, c1, c2, c3), key)
+                          : philox_block(block, c1, c2, c3, key);
+      block++;
       used = 0;
     }
     uint32_t r = used == 0 ? buf.x : used == 1 ? buf.y : used == 2 ? buf.z : buf.w;
@@ -90,6 +96,8 @@ struct PhiloxStream {
     return ((float)(next() >> 8) + 0.5f) * (1.0f / 16777216.0f);
   }
 };
+using PhiloxStream = PhiloxStreamT<false>;
+using PhiloxStreamInline = PhiloxStreamT<true>;
 
 // ------------------------------------------------------------ geometry ----
 

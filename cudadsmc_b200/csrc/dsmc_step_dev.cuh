@@ -228,7 +228,7 @@ __device__ __forceinline__ void ntc_fast(const StepParams& p, uint32_t cell, uin
   const uint32_t M = (uint32_t)fpc;
   vm.y = fpc - (float)M;
   sel += M;
-  PhiloxStream r;
+  PhiloxStreamInline r;
   r.init(p.seed, cell, step, kPurposeCollide);
   uint32_t ncol = 0;
   for (uint32_t i = 0; i < M; i++) {
@@ -288,7 +288,7 @@ __device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cel
   const float fpc = ntc_fpc_fast(p, n, vm);
   const uint32_t M = (uint32_t)fpc;
   float vmax = vm.x;
-  PhiloxStream rng;
+  PhiloxStreamInline rng;
   rng.init(p.seed, cell, step, kPurposeHeavy + lane);
   uint32_t drawn = 0, done = 0, pi = 0, pj = 0, ncol = 0;
   bool pend = false;
