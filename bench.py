@@ -290,12 +290,12 @@ def reduce_over_ranks(elapsed, count, world, device):
 
 def kernels_per_step(settings, variant, has_mesh):
     """Kernels one timestep launches: scan and scatter; the fused cell kernel,
-    or the split variants' collide, flight, mesh flights (with a body) and
+    or the split variants' order, NTC, flight, mesh flights (with a body) and
     sampling (with sampling on: it returns at once on other steps); two per
     inflow face (plan, fill)."""
     n = 2
     if variant >= 4:
-        n += 2 + (1 if has_mesh else 0) + (1 if settings.get("sample_every", 0) > 0 else 0)
+        n += 3 + (1 if has_mesh else 0) + (1 if settings.get("sample_every", 0) > 0 else 0)
     else:
         n += 1
     faces = settings.get("face_kind", {})
@@ -306,17 +306,17 @@ def algorithmic_bytes(kernel, n_particles, cells, rng_taus, sample_frac, split=T
     """Bytes a kernel must move per launch (SoA FP32 state, 24 B/particle).
 
     scatter: key read 4 + orig written 4 (split variants; for the fused cell
-    kernel it also moves the state: + 24 read + 24 written).  collide: orig 4
+    kernel it also moves the state: + 24 read + 24 written).  order: orig 4
     + state gathered 24 + sorted state written 24 per particle; per cell its
     start 4 and (sigma g)max/remainder read + written 16 (+ 32 of HybridTaus
     state in the reference RNG mode).  flight: state read 24 + written 24 +
     next-step key 4 per particle.  cell (fused): state + orig read 28, state +
-    key written 28, the per-cell terms of collide and 80 B of sampling sums on
+    key written 28, the per-cell terms of order and 80 B of sampling sums on
     sampling steps."""
     per_cell = 4 + 16 + (32 if rng_taus else 0)
     if kernel == "scatter":
         return n_particles * (4 + 4 + (0 if split else 48))
-    if kernel == "collide":
+    if kernel == "order":
         return n_particles * (4 + 24 + 24) + cells * per_cell
     if kernel == "flight":
         return n_particles * (24 + 24 + 4)
@@ -354,10 +354,10 @@ def run_ours(args, rank, world):
     sol.Profile(True)
     sol.RunSimulationStep(dt, bsteps)
     breakdown = sol.ProfileReadKernels()
-    dom_slot = max((k for k in breakdown if k in ("scatter", "collide", "flight")),
+    dom_slot = max((k for k in breakdown if k in ("scatter", "order", "flight")),
                    key=lambda k: breakdown[k][0])
     if not split:
-        breakdown["cell"] = breakdown.pop("collide")  # the fused cell kernel's slot
+        breakdown["cell"] = breakdown.pop("order")  # the fused cell kernel's slot
     sol.Sync()
     info0 = sol.Info()
     if world > 1:
@@ -389,7 +389,7 @@ def run_ours(args, rank, world):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    dom = dom_slot if split or dom_slot != "collide" else "cell"
+    dom = dom_slot if split or dom_slot != "order" else "cell"
     dom_ms = prof[dom_slot][0] / max(prof[dom_slot][1], 1)
     taus = wl["settings"].get("rng", "taus") == "taus"
     alg = algorithmic_bytes(dom, n_avg, sol.Info().cells, taus, 1.0 / 100, split)

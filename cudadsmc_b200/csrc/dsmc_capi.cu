@@ -28,6 +28,7 @@ struct dsmc_handle {
   float* A[6]{};
   float* B[6]{};
   uint32_t* orig = nullptr;
+  uint4* ntc_list = nullptr;  // 2 x cells entries: light then dense cells with NTC pairs
   uint32_t* keys = nullptr;    // next-step cell key per particle
   uint32_t* cursor = nullptr;  // per-cell ticket counters of the scatter
   uint32_t* count = nullptr;
@@ -62,14 +63,14 @@ struct dsmc_handle {
 
   // per-kernel event timing (dsmc_profile)
   bool profiling = false;
-  uint32_t prof_mask = 0x7f;  // slots that get events while profiling
+  uint32_t prof_mask = 0xff;  // slots that get events while profiling
   std::vector<cudaEvent_t> ev;      // pairs
   std::vector<int> ev_kernel;       // kernel id of each pair
   size_t ev_used = 0;
-  // slots: 0 scan, 1 scatter, 2 cell (fused) / collide (split), 3 injection,
-  // 4 flight, 5 mesh flights, 6 sampling (split)
-  double prof_ms[7] = {0, 0, 0, 0, 0, 0, 0};
-  uint32_t prof_n[7] = {0, 0, 0, 0, 0, 0, 0};
+  // slots: 0 scan, 1 scatter, 2 cell (fused) / order (split), 3 injection,
+  // 4 flight, 5 mesh flights, 6 sampling, 7 NTC selections (split)
+  double prof_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  uint32_t prof_n[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
   std::string err;
 };
@@ -142,7 +143,7 @@ void free_all(dsmc_handle* h) {
     cudaFree(h->B[i]);
     h->A[i] = h->B[i] = nullptr;
   }
-  void* ps[] = {h->orig, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
+  void* ps[] = {h->orig, h->ntc_list, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
                 h->acc, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse, h->gtri, h->gplane};
   for (void* p : ps) cudaFree(p);
 }
@@ -274,9 +275,11 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
   if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
   p.cell_variant = h->variant;
   p.defer_list = h->orig;
+  p.ntc_light = h->ntc_list;
+  p.ntc_heavy = h->ntc_list + h->cells;
   if (split) {
-    static const int slot[4] = {2, 4, 5, 6};
-    for (int stage = 0; stage < 4; stage++) {
+    static const int slot[5] = {2, 7, 4, 5, 6};
+    for (int stage = 0; stage < 5; stage++) {
       e = timed(h, slot[stage], [&] {
         return dsmcb::launch_split_stage(p, h->variant - 4, stage, h->stream);
       });
@@ -467,6 +470,7 @@ int dsmc_create(const dsmc_config* cfg, dsmc_handle** out) {
   }
   if (!e) e = dalloc(&h->orig, h->capacity);
   if (!e) e = dalloc(&h->keys, h->capacity);
+  if (!e) e = dalloc(&h->ntc_list, 2 * (size_t)h->cells);
   if (!e) e = dalloc(&h->cursor, h->cells + 1);
   if (!e) e = dalloc(&h->count, h->cells + 1);
   if (!e) e = dalloc(&h->start, h->cells + 1);
@@ -568,18 +572,18 @@ int dsmc_profile(dsmc_handle* h, int enable) {
       for (auto& e : h->ev) CK(h, cudaEventCreate(&e), "event create");
     }
     h->ev_used = 0;
-    for (int k = 0; k < 7; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
+    for (int k = 0; k < 8; k++) { h->prof_ms[k] = 0; h->prof_n[k] = 0; }
   } else {
     prof_flush(h);
   }
   h->profiling = enable != 0;
-  h->prof_mask = 0x7f;
+  h->prof_mask = 0xff;
   return DSMC_OK;
 }
 
 int dsmc_profile_mask(dsmc_handle* h, uint32_t slots) {
   if (!h || !h->profiling) return fail(h, DSMC_ERR_STATE, "dsmc_profile_mask needs an open window");
-  h->prof_mask = slots & 0x7fu;
+  h->prof_mask = slots & 0xffu;
   return DSMC_OK;
 }
 
@@ -587,8 +591,8 @@ int dsmc_profile_read(dsmc_handle* h, double ms[4], uint32_t launches[4]) {
   if (!h || !ms || !launches) return DSMC_ERR_ARG;
   prof_flush(h);
   for (int k = 0; k < 4; k++) { ms[k] = h->prof_ms[k]; launches[k] = h->prof_n[k]; }
-  // the cell work of the split variants: collide + flight + mesh + sampling
-  for (int k = 4; k < 7; k++) ms[2] += h->prof_ms[k];
+  // the cell work of the split variants: order + NTC + flight + mesh + sampling
+  for (int k = 4; k < 8; k++) ms[2] += h->prof_ms[k];
   h->profiling = false;
   return DSMC_OK;
 }
@@ -597,8 +601,8 @@ int dsmc_profile_read_kernels(dsmc_handle* h, int n, double* ms, uint32_t* launc
   if (!h || !ms || !launches || n < 1) return DSMC_ERR_ARG;
   prof_flush(h);
   for (int k = 0; k < n; k++) {
-    ms[k] = k < 7 ? h->prof_ms[k] : 0.0;
-    launches[k] = k < 7 ? h->prof_n[k] : 0u;
+    ms[k] = k < 8 ? h->prof_ms[k] : 0.0;
+    launches[k] = k < 8 ? h->prof_n[k] : 0u;
   }
   h->profiling = false;
   return DSMC_OK;

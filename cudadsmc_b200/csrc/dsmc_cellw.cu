@@ -1,7 +1,7 @@
 // The timestep's cell work as warp-autonomous kernels (sm_100a); none has a
 // CTA-wide barrier inside its loop.
 //
-// k_collide_w (order + collisions): warps take tiles of 32 consecutive cells
+// k_order_w (order + pair counts): warps take tiles of 32 consecutive cells
 // (lane L owns cell L; tiles past the first wave come from a dynamic counter)
 // and cut them into chunks of whole cells holding at most CAPW particles.  A
 // chunk's orig (the pre-scatter index of every sorted slot) is staged in the
@@ -12,9 +12,10 @@
 //      asynchronous 4-byte copies, while the cell of each slot (binary search
 //      of the chunk's cell starts) and its rank by orig inside the cell (the
 //      stable order of the reference's sort) are computed
-//   B  NTC collisions: light cells one lane each, dense cells (Philox mode)
-//      one whole warp each
+//   B  NTC pair counts (and remainders); cells with pairs are listed
 //   C  the chunk goes to the mid arrays in sorted order
+// k_ntc_w: the listed cells' NTC selections in place on the mid arrays, a
+// lane per light cell, a warp per dense cell (Philox mode).
 // k_flight_w (flight + keys): streams the sorted particles, 32 at a time per
 // warp in grid-stride order: free flight and boundaries, next-step key and
 // count (warp-aggregated atomics on the per-cell counts and on the per scan
@@ -27,7 +28,7 @@
 // every cell that fits a chunk.  Gathering through orig lets the scatter write
 // orig alone (one scattered 4-byte store per particle instead of seven).
 //
-// Traffic per particle: k_collide_w orig 4 + state 24 read, 24 written;
+// Traffic per particle: k_order_w orig 4 + state 24 read, 24 written;
 // k_flight_w 24 read, 24 + key 4 written.  Per cell: 8 B of starts, 16 B of
 // (sigma g)max read + written, 32 B more in the reference RNG mode, 80 B of
 // sampling sums on sampling steps.
@@ -45,9 +46,6 @@ constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach 
 template <int CAPW>
 struct __align__(16) WarpSmem {
   float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
-  uint4 seeds[kWarpTile];      // HybridTaus states (reference RNG mode)
-  float2 mr[kWarpTile];        // (sigma g)max, NTC remainder
-  uint32_t claim[CAPW];        // pair claims inside a dense cell
   uint32_t cs[kWarpTile + 1];  // chunk-relative start of each tile cell
   unsigned long long mbar[2];
   uint16_t slot[CAPW];         // sorted position -> staged index
@@ -136,11 +134,9 @@ __device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>
 }
 
 // A cell too large for a chunk: the warp gathers it in sorted order into the
-// mid arrays in global memory and one lane collides it there.
-static __device__ __noinline__ void giant_collide_warp(const StepParams& p, uint32_t cell,
-                                                       uint32_t s, uint32_t e, uint32_t step,
-                                                       uint32_t& sel, uint32_t& col,
-                                                       double& sum_g) {
+// mid arrays in global memory; its pairs are collided by one lane of k_ntc_w
+// (the cell is listed as a light cell whatever its pair count).
+static __device__ __noinline__ void giant_order_warp(const StepParams& p, uint32_t s, uint32_t e) {
   const uint32_t n = e - s;
   const uint32_t lane = lane_id();
   if (lane == 0 && p.meta) atomicAdd(&p.meta->giant_cells, 1u);
@@ -152,29 +148,32 @@ static __device__ __noinline__ void giant_collide_warp(const StepParams& p, uint
     p.mid.x[d] = p.in.x[my]; p.mid.y[d] = p.in.y[my]; p.mid.z[d] = p.in.z[my];
     p.mid.u[d] = p.in.u[my]; p.mid.v[d] = p.in.v[my]; p.mid.w[d] = p.in.w[my];
   }
-  __syncwarp();
-  if ((p.flags & kDoCollide) && lane == 0) {
-    GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, s};
-    CellState st{p.maxrem + cell, p.seeds ? p.seeds + cell : nullptr,
-                 p.stat4 ? p.stat4 + cell : nullptr};
-    collide_cell(p, cell, (int)n, acc, step, st, sel, col, sum_g);
-  }
-  __syncwarp();
 }
 
-// ------------------------------------------------------ order + collide ----
+// Appends e for every lane with `put` to list (one atomic per warp; all lanes
+// call it).
+__device__ __forceinline__ void list_cells(uint4* list, uint32_t* counter, bool put, uint4 e) {
+  const uint32_t lane = lane_id();
+  const unsigned m = __ballot_sync(kFull, put);
+  if (!m) return;
+  const int leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(kFull, base, leader);
+  if (put) list[base + __popc(m & ((1u << lane) - 1u))] = e;
+}
+
+// ---------------------------------------------------- order + pair counts ----
 
 template <int CAPW, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_constant__ StepParams p) {
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   WarpSmem<CAPW>& S = reinterpret_cast<WarpSmem<CAPW>*>(smem_raw)[warp];
-  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const bool do_fixup = (p.flags & kDoFixup) != 0;
   const bool do_collide = (p.flags & kDoCollide) != 0;
   const bool taus = p.rng_kind == 0;
   const bool heavy_mode = !taus && do_collide;
-  for (uint32_t t = lane; t < (uint32_t)CAPW; t += 32) S.claim[t] = 0xffffffffu;
   if (lane == 0) {
     mbar_init(&S.mbar[0], 1);
     mbar_init(&S.mbar[1], 1);
@@ -195,24 +194,19 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
   WTile B = load_tile(p, tb);
 
   uint32_t phase = 0;  // bit b: parity of the next phase of buffer b
-  uint32_t sel = 0, col = 0;
-  double sum_g = 0.0;
+  uint32_t sel = 0;
   WChunk C;
   C.valid = 0;
-  // per-cell collision state of a chunk, loaded one chunk ahead of its use
+  // (sigma g)max and remainder of a chunk's cells, loaded one chunk ahead
   float2 mr_c = make_float2(0.f, 0.f);
-  uint4 sd_c = make_uint4(0u, 0u, 0u, 0u);
-  auto load_cell_state = [&](const WChunk& K, uint32_t tile, float2& mr, uint4& sd) {
-    if (do_collide && K.valid && !K.giant && K.n && lane >= K.cur && lane < K.cur + K.k) {
-      const uint32_t c = tile * kWarpTile + lane;
-      mr = p.maxrem[c];
-      if (taus) sd = p.seeds[c];
-    }
+  auto load_cell_state = [&](const WChunk& K, uint32_t tile, float2& mr) {
+    if (do_collide && K.valid && !K.giant && K.n && lane >= K.cur && lane < K.cur + K.k)
+      mr = p.maxrem[tile * kWarpTile + lane];
   };
   if (A.t < p.n_tiles) {
     C = make_wchunk<CAPW>(A, 0, 0);
     if (!C.giant && C.n) issue_wchunk(p, S, C);
-    load_cell_state(C, A.t, mr_c, sd_c);
+    load_cell_state(C, A.t, mr_c);
   }
 
   while (C.valid) {
@@ -229,18 +223,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
     const bool n_copy = N.valid && !N.giant && N.n;
     if (n_copy) issue_wchunk(p, S, N);
     float2 mr_n = make_float2(0.f, 0.f);
-    uint4 sd_n = make_uint4(0u, 0u, 0u, 0u);
-    load_cell_state(N, n_in_b ? B.t : A.t, mr_n, sd_n);
+    load_cell_state(N, n_in_b ? B.t : A.t, mr_n);
 
     const uint32_t c0 = A.t * kWarpTile;
     const uint32_t cell = c0 + lane;
     const bool mine = lane >= C.cur && lane < C.cur + C.k;
     const uint32_t s0 = A.s - C.base, nc = A.e - A.s;  // meaningful for `mine`
     if (!C.giant && C.n) {
-      if (do_collide && mine) {
-        S.mr[lane] = mr_c;
-        if (taus) S.seeds[lane] = sd_c;
-      }
       S.cs[lane] = s0;
       if (lane == 31) S.cs[32] = A.e - C.base;
       const uint32_t par = (phase >> C.buf) & 1u;
@@ -258,7 +247,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
     __syncwarp();
 
     if (C.giant) {
-      giant_collide_warp(p, c0 + C.cur, C.base, C.base + C.n, step, sel, col, sum_g);
+      giant_order_warp(p, C.base, C.base + C.n);
+      if (do_collide) {
+        // the giant cell's pair count, from lane C.cur's (sigma g)max
+        const uint32_t gc = c0 + C.cur;
+        uint32_t M = 0;
+        if (lane == C.cur) {
+          float2 vm = p.maxrem[gc];
+          M = taus ? ntc_pairs_reference(p, (int)C.n, vm) : ntc_pairs_fast(p, C.n, vm);
+          p.maxrem[gc] = vm;
+          sel += M;
+        }
+        list_cells(p.ntc_light, &p.meta->n_light, lane == C.cur && M > 0,
+                   make_uint4(gc, C.base, C.n, M));
+      }
     } else if (C.n > 0) {
       const uint32_t off = C.base & 3u;
       float* X = S.part[C.buf][0] + off;
@@ -280,12 +282,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
         cp_async4(V + t, p.in.v + i);
         cp_async4(W + t, p.in.w + i);
       }
-      // A1: dense cells
-      bool heavy = false;
-      if (heavy_mode && mine && nc >= 2)
-        heavy = (uint32_t)ntc_fpc_fast(p, nc, S.mr[lane]) >= kHeavyMin;
-      const unsigned heavy_mask = __ballot_sync(kFull, heavy);
-      __syncwarp();
       // A2: slot[sorted position] = staged index, sorted = (cell, orig).  The
       // origs are distinct, so a particle's rank in its cell is the number of
       // smaller origs there, counted four at a time from the 16-byte aligned
@@ -324,27 +320,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
       }
       cp_async_wait_all();
       __syncwarp();
-      // B: collisions; light cells one lane each, dense cells one warp each
+      // B: pair counts (the new remainder is stored now); cells with pairs
+      // are listed for k_ntc_w, light ones to get a lane, dense ones a warp
       if (do_collide) {
-        if (mine && !heavy) {
-          SmemVel acc{U, V, W, S.slot, s0};
-          CellState st{&S.mr[lane], taus ? &S.seeds[lane] : nullptr,
-                       p.stat4 ? p.stat4 + cell : nullptr};
-          collide_cell(p, cell, (int)nc, acc, step, st, sel, col, sum_g);
+        uint32_t M = 0;
+        if (mine && nc >= 2) {
+          float2 vm = mr_c;
+          M = taus ? ntc_pairs_reference(p, (int)nc, vm) : ntc_pairs_fast(p, nc, vm);
+          p.maxrem[cell] = vm;
+          sel += M;
         }
-        __syncwarp();
-        for (unsigned hm = heavy_mask; hm; hm &= hm - 1u) {
-          const uint32_t lc = (uint32_t)__ffs(hm) - 1u;
-          const uint32_t a = S.cs[lc], b = S.cs[lc + 1];
-          SmemVel acc{U, V, W, S.slot, a};
-          CellState st{&S.mr[lc], nullptr, p.stat4 ? p.stat4 + c0 + lc : nullptr};
-          ntc_heavy_warp(p, c0 + lc, b - a, acc, S.claim, step, st, sel, col, sum_g);
-          __syncwarp();
-        }
-        if (mine) {
-          p.maxrem[cell] = S.mr[lane];
-          if (taus) p.seeds[cell] = S.seeds[lane];
-        }
+        const bool heavy = heavy_mode && M >= kHeavyMin;
+        const uint4 e = make_uint4(cell, base + s0, nc, M);
+        list_cells(p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
+        list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
       // C: the chunk in sorted order
       for (uint32_t q = lane; q < n; q += 32) {
@@ -362,13 +351,60 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_collide_w(const __grid_con
     }
     C = N;
     mr_c = mr_n;
-    sd_c = sd_n;
   }
   const unsigned long long s64 = warp_sum((unsigned long long)sel);
+  if (lane == 0 && p.meta && s64) atomicAdd(&p.meta->selections, s64);
+}
+
+// ------------------------------------------------------- NTC selections ----
+
+constexpr uint32_t kNtcClaim = 256;  // claim slots per warp: the largest chunk
+
+// The NTC selections of the cells k_order_w listed, in place on the sorted
+// post-collision state p.mid: a lane per light cell, a warp per dense cell
+// (at most kNtcClaim particles: larger cells were collided by k_order_w).
+// The pair counts and remainders come from k_order_w; this kernel updates
+// (sigma g)max (and the HybridTaus state in the reference RNG mode) with the
+// same arithmetic and random streams as the fused path.
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ StepParams p) {
+  __shared__ uint32_t s_claim[WARPS][kNtcClaim];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const bool taus = p.rng_kind == 0;
+  for (uint32_t t = lane; t < kNtcClaim; t += 32) s_claim[warp][t] = 0xffffffffu;
+  __syncwarp();
+  uint32_t col = 0;
+  double sum_g = 0.0;
+  const uint32_t nl = p.meta->n_light, nh = p.meta->n_heavy;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
+    const uint4 e = p.ntc_light[i];  // cell, first sorted slot, count, pairs
+    GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, e.y};
+    float2 vm = p.maxrem[e.x];
+    if (taus) {
+      TausRng r;
+      r.s = p.seeds[e.x];
+      float4 stat = make_float4(0.f, 0.f, 0.f, 0.f);
+      ntc_select_reference(p, (int)e.z, acc, r, e.w, vm, stat, col, sum_g);
+      p.seeds[e.x] = r.s;
+    } else {
+      col += ntc_select_fast(p, e.x, e.z, acc, step, e.w, vm, sum_g);
+    }
+    p.maxrem[e.x] = vm;
+  }
+  const uint32_t gw = blockIdx.x * WARPS + warp, nw = gridDim.x * WARPS;
+  for (uint32_t h = gw; h < nh; h += nw) {
+    const uint4 e = p.ntc_heavy[h];
+    GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, e.y};
+    const float2 vm = p.maxrem[e.x];  // .y: the remainder k_order_w stored
+    const float vmax =
+        ntc_select_heavy_warp(p, e.x, e.z, acc, s_claim[warp], step, e.w, vm.x, col, sum_g);
+    __syncwarp();
+    if (lane == 0) p.maxrem[e.x] = make_float2(vmax, vm.y);
+  }
   const unsigned long long c64 = warp_sum((unsigned long long)col);
   const double g = warp_sum(sum_g);
   if (lane == 0 && p.meta) {
-    if (s64) atomicAdd(&p.meta->selections, s64);
     if (c64) atomicAdd(&p.meta->collisions, c64);
     if (g != 0.0) atomicAdd(&p.meta->sum_g, g);
   }
@@ -410,7 +446,7 @@ __device__ __forceinline__ void list_deferred(const StepParams& p, const uint32_
 }
 
 // Free flights of the sorted particles [0, n_alive), read from p.mid (the
-// state k_collide_w produced) and written to p.out.  Warps take groups of 32
+// state k_order_w and k_ntc_w produced) and written to p.out.  Warps take groups of 32
 // in grid-stride order (the work per particle is even once the flights that
 // may reach the body are listed for k_mesh_w, which spreads them over the
 // whole GPU: they cluster next to the body).  The state of a group is loaded
@@ -628,7 +664,7 @@ struct LaunchShapeW {
 };
 
 template <int CAPW, int WARPS, int MINB>
-cudaError_t launch_collide_w(const StepParams& p, cudaStream_t stream) {
+cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -636,11 +672,11 @@ cudaError_t launch_collide_w(const StepParams& p, cudaStream_t stream) {
   LaunchShapeW& ls = cache[dev & 7];
   const size_t smem = collide_smem_bytes<CAPW, WARPS>();
   if (ls.device != dev) {
-    e = cudaFuncSetAttribute(k_collide_w<CAPW, WARPS, MINB>,
+    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_collide_w<CAPW, WARPS, MINB>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB>,
                                                       WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -651,7 +687,7 @@ cudaError_t launch_collide_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  k_collide_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
+  k_order_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -700,6 +736,26 @@ cudaError_t launch_flight_pw(const StepParams& p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+constexpr int kNtcWarps = 8;
+
+cudaError_t launch_ntc_w(const StepParams& p, cudaStream_t stream) {
+  static LaunchShapeW cache[8];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  LaunchShapeW& ls = cache[dev & 7];
+  if (ls.device != dev) {
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ntc_w<kNtcWarps>, kNtcWarps * 32, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    ls.device = dev;
+    ls.per_sm = per_sm;
+  }
+  k_ntc_w<kNtcWarps><<<(uint32_t)(num_sms() * ls.per_sm), kNtcWarps * 32, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
 template <int MINB>
 cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
@@ -728,10 +784,10 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 
 // Split variants (cell_kernel_variants() numbers them after the fused
 // CTA-wide ones): (particles per warp chunk, warps per CTA, register cap) of
-// the order + collide kernel and the register cap of the flight kernel (8
-// warps per CTA): 0 (256, 4, 128; 80), 1 (128, 4, 128; 80), 2 (128, 8, 80;
-// 64), 3 (128, 4, 96; 64).  The mesh kernel runs at 64 registers (more warps
-// to cover its chains of L2 loads).
+// the order kernel and the flight kernel's form (8 warps per CTA): 0 (256, 4,
+// 128; one particle per lane, 80 registers), 1 (128, 4, 128; one, 80), 2
+// (128, 8, 80; pairs, 80), 3 (128, 4, 80; pairs, 64).  The mesh kernel runs
+// at 64 registers (more warps to cover its chains of L2 loads).
 int cell_kernel_w_variants() { return 4; }
 
 int cell_kernel_w_capacity(int v) {
@@ -745,19 +801,22 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
   switch (stage) {
     case 0:
       switch (v) {
-        case 0: return launch_collide_w<256, 4, 4>(p, stream);
-        case 2: return launch_collide_w<128, 8, 3>(p, stream);
-        case 3: return launch_collide_w<128, 4, 5>(p, stream);
-        default: return launch_collide_w<128, 4, 4>(p, stream);
+        case 0: return launch_order_w<256, 4, 4>(p, stream);
+        case 2: return launch_order_w<128, 8, 3>(p, stream);
+        case 3: return launch_order_w<128, 4, 6>(p, stream);
+        default: return launch_order_w<128, 4, 4>(p, stream);
       }
     case 1:
+      if (p.flags & kDoCollide) return launch_ntc_w(p, stream);
+      return cudaSuccess;
+    case 2:
       // 0, 1: single particles per lane; 2, 3: pairs (different register caps)
       switch (v) {
         case 2: return launch_flight_pw<3>(p, stream);
         case 3: return launch_flight_pw<4>(p, stream);
         default: return launch_flight_w<3>(p, stream);
       }
-    case 2:
+    case 3:
       // flights that may reach the body (listed only with a body and the move)
       if (p.has_geom && (p.flags & kDoMove)) return launch_mesh_w<4>(p, stream);
       return cudaSuccess;
@@ -768,7 +827,7 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
 }
 
 cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream) {
-  for (int stage = 0; stage < 4; stage++) {
+  for (int stage = 0; stage < 5; stage++) {
     const cudaError_t e = launch_split_stage(p, v, stage, stream);
     if (e != cudaSuccess) return e;
   }

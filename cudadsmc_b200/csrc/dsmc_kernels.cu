@@ -126,6 +126,8 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
     meta->tile_next = 0;
     meta->tile_next2 = 0;
     meta->n_defer = 0;
+    meta->n_light = 0;
+    meta->n_heavy = 0;
     if (bump) {
       meta->step += 1;
       meta->particle_steps += run;

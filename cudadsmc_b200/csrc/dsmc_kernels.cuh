@@ -42,6 +42,8 @@ struct Meta {
   uint32_t tile_next;    // the cell kernel's dynamic tile counter (reset by the scan)
   uint32_t tile_next2;   // the flight kernel's dynamic tile counter (reset by the scan)
   uint32_t n_defer;      // flights listed for the mesh kernel this step (reset by the scan)
+  uint32_t n_light;      // cells listed for the NTC kernel, one lane each (reset by the scan)
+  uint32_t n_heavy;      // cells listed for the NTC kernel, one warp each (reset by the scan)
   unsigned long long particle_steps;  // sum over steps of the particles placed by the scan
 };
 
@@ -123,6 +125,8 @@ struct StepParams {
   uint32_t n_tiles;
   uint32_t step_override;  // 0: use meta->step
   int cell_variant;        // (threads, chunk capacity) of the cell kernel
+  uint4* ntc_light;        // split variants: (cell, first sorted slot, count, pairs) of
+  uint4* ntc_heavy;        // the cells with NTC pairs this step (cells entries each)
   uint32_t* defer_list;    // split variants: flights that may reach the body
                            // (capacity entries; the orig buffer, dead once the
                            // collide kernel has read it)
@@ -157,8 +161,9 @@ int cell_kernel_w_variants();
 int cell_kernel_w_capacity(int v);
 uint32_t cell_kernel_w_tile();
 cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream);
-// One kernel of the split variants: 0 collide, 1 flight, 2 mesh flights,
-// 3 sampling (launch_cell_w runs the four in order).
+// One kernel of the split variants: 0 order (gather, stable order, pair
+// counts), 1 NTC selections, 2 flight, 3 mesh flights, 4 sampling
+// (launch_cell_w runs the five in order).
 cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream_t stream);
 // Free flight + boundaries in place on p.out for n particles (move stage);
 // particles that leave through an outflow face get x = NaN.

@@ -99,6 +99,8 @@ struct SmemVel {
     const uint32_t j = slot[off + k];
     u[j] = a.x; v[j] = a.y; w[j] = a.z;
   }
+  // a distinct small index per particle of the cell (pair claims)
+  __device__ __forceinline__ uint32_t claim_index(uint32_t k) const { return slot[off + k]; }
 };
 
 struct GlobalVel {
@@ -110,6 +112,7 @@ struct GlobalVel {
   __device__ __forceinline__ void set(uint32_t k, float3 a) const {
     u[off + k] = a.x; v[off + k] = a.y; w[off + k] = a.z;
   }
+  __device__ __forceinline__ uint32_t claim_index(uint32_t k) const { return k; }
 };
 
 // Per-cell collision state of one cell, wherever it is staged.
@@ -149,20 +152,22 @@ __device__ __forceinline__ float sigma_g_fast(const StepParams& p, float mag) {
 // NTC collisions of one cell with the reference's arithmetic:
 // ComputeBirdCollisionsNoMTDev, kernels/dsmc_kernel.cu:912-1000.  Particles of
 // the cell are acc.get(0..n-1) in sorted order; pair members are
-// start + rand % n; the pair count is evaluated in double.
-template <class Rng, class Acc>
-__device__ __forceinline__ void ntc_reference(const StepParams& p, int partCount, Acc acc, Rng& rng,
-                                              CellState cs, uint32_t& sel, uint32_t& col,
-                                              double& sum_g) {
-  float4 stat = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (cs.stat4) stat = *cs.stat4;
-  float2 vmax = *cs.maxrem;
+// start + rand % n; the pair count is evaluated in double.  In two parts: the
+// pair count (which also leaves the new remainder in vmax.y) and the
+// selections, so that kernels may do them apart.
+__device__ __forceinline__ uint32_t ntc_pairs_reference(const StepParams& p, int partCount,
+                                                        float2& vmax) {
   const float avgConc = p.ntc_local ? (float)(partCount - 1) : p.avg_conc;
   float fpc = (0.5 * partCount * avgConc * p.fnum * vmax.x * p.dt) / p.cell_volume + vmax.y;
   uint32_t pairsCount = fpc;
-  stat.x += pairsCount;
   vmax.y = fpc - pairsCount;
-  sel += pairsCount;
+  return pairsCount;
+}
+
+template <class Rng, class Acc>
+__device__ __forceinline__ void ntc_select_reference(const StepParams& p, int partCount, Acc acc,
+                                                     Rng& rng, uint32_t pairsCount, float2& vmax,
+                                                     float4& stat, uint32_t& col, double& sum_g) {
   for (uint32_t i = 0; i < pairsCount; i++) {
     uint32_t px = rng.u32() % (uint32_t)partCount;
     float3 v1 = acc.get(px);
@@ -192,6 +197,19 @@ __device__ __forceinline__ void ntc_reference(const StepParams& p, int partCount
     }
     if (v > vmax.x) vmax.x = v;
   }
+}
+
+template <class Rng, class Acc>
+__device__ __forceinline__ void ntc_reference(const StepParams& p, int partCount, Acc acc, Rng& rng,
+                                              CellState cs, uint32_t& sel, uint32_t& col,
+                                              double& sum_g) {
+  float4 stat = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (cs.stat4) stat = *cs.stat4;
+  float2 vmax = *cs.maxrem;
+  const uint32_t pairsCount = ntc_pairs_reference(p, partCount, vmax);
+  stat.x += pairsCount;
+  sel += pairsCount;
+  ntc_select_reference(p, partCount, acc, rng, pairsCount, vmax, stat, col, sum_g);
   *cs.maxrem = vmax;
   if (cs.stat4) *cs.stat4 = stat;
 }
@@ -217,17 +235,20 @@ __device__ __forceinline__ void scatter_pair(float3 v1, float3 v2, float mag, fl
   o2 = make_float3(cm.x - ang.x, cm.y - ang.y, cm.z - ang.z);
 }
 
-// NTC of one cell in the Philox mode (one lane): distinct pairs, acceptance
-// sigma*g > R (sigma*g)max.
-template <class Acc>
-__device__ __forceinline__ void ntc_fast(const StepParams& p, uint32_t cell, uint32_t n, Acc acc,
-                                         uint32_t step, CellState cs, uint32_t& sel, uint32_t& col,
-                                         double& sum_g) {
-  float2 vm = *cs.maxrem;
+// Pair count of the Philox mode (leaves the new remainder in vm.y).
+__device__ __forceinline__ uint32_t ntc_pairs_fast(const StepParams& p, uint32_t n, float2& vm) {
   const float fpc = ntc_fpc_fast(p, n, vm);
   const uint32_t M = (uint32_t)fpc;
   vm.y = fpc - (float)M;
-  sel += M;
+  return M;
+}
+
+// NTC selections of one cell in the Philox mode (one lane): distinct pairs,
+// acceptance sigma*g > R (sigma*g)max; returns the collisions.
+template <class Acc>
+__device__ __forceinline__ uint32_t ntc_select_fast(const StepParams& p, uint32_t cell, uint32_t n,
+                                                    Acc acc, uint32_t step, uint32_t M, float2& vm,
+                                                    double& sum_g) {
   PhiloxStreamInline r;
   r.init(p.seed, cell, step, kPurposeCollide);
   uint32_t ncol = 0;
@@ -249,6 +270,17 @@ __device__ __forceinline__ void ntc_fast(const StepParams& p, uint32_t cell, uin
     }
     if (v > vm.x) vm.x = v;
   }
+  return ncol;
+}
+
+template <class Acc>
+__device__ __forceinline__ void ntc_fast(const StepParams& p, uint32_t cell, uint32_t n, Acc acc,
+                                         uint32_t step, CellState cs, uint32_t& sel, uint32_t& col,
+                                         double& sum_g) {
+  float2 vm = *cs.maxrem;
+  const uint32_t M = ntc_pairs_fast(p, n, vm);
+  sel += M;
+  const uint32_t ncol = ntc_select_fast(p, cell, n, acc, step, M, vm, sum_g);
   col += ncol;
   *cs.maxrem = vm;
   if (cs.stat4) {
@@ -278,16 +310,16 @@ __device__ __forceinline__ void collide_cell(const StepParams& p, uint32_t cell,
 // NTC selections of one dense cell by a whole warp (Philox mode).  Pairs are
 // distinct particles drawn uniformly; each round processes every pair whose
 // two particles are not claimed by a lower lane, the others retry with the
-// same pair.  Acceptance uses (sigma*g)max as of the round's start.
-__device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cell, uint32_t n,
-                                               SmemVel acc, uint32_t* claim, uint32_t step,
-                                               CellState cs, uint32_t& sel, uint32_t& col,
-                                               double& sum_g) {
+// same pair.  Acceptance uses (sigma*g)max as of the round's start.  M pairs
+// from vmax_in; returns the new (sigma*g)max (the same in every lane).
+// claim[] holds 0xffffffff for every claim index of the cell and is left so.
+template <class Acc>
+__device__ __forceinline__ float ntc_select_heavy_warp(const StepParams& p, uint32_t cell,
+                                                       uint32_t n, Acc acc, uint32_t* claim,
+                                                       uint32_t step, uint32_t M, float vmax_in,
+                                                       uint32_t& col, double& sum_g) {
   const unsigned lane = lane_id();
-  const float2 vm = *cs.maxrem;
-  const float fpc = ntc_fpc_fast(p, n, vm);
-  const uint32_t M = (uint32_t)fpc;
-  float vmax = vm.x;
+  float vmax = vmax_in;
   PhiloxStreamInline rng;
   rng.init(p.seed, cell, step, kPurposeHeavy + lane);
   uint32_t drawn = 0, done = 0, pi = 0, pj = 0, ncol = 0;
@@ -305,8 +337,8 @@ __device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cel
     drawn += want;
     uint32_t ji = 0, jj = 0;
     if (pend) {
-      ji = acc.slot[acc.off + pi];
-      jj = acc.slot[acc.off + pj];
+      ji = acc.claim_index(pi);
+      jj = acc.claim_index(pj);
       atomicMin(&claim[ji], lane);
       atomicMin(&claim[jj], lane);
     }
@@ -341,7 +373,21 @@ __device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cel
     __syncwarp();
   }
   col += ncol;
-  const uint32_t wcol = warp_sum(ncol);
+  return vmax;
+}
+
+template <class Acc>
+__device__ __forceinline__ void ntc_heavy_warp(const StepParams& p, uint32_t cell, uint32_t n,
+                                               Acc acc, uint32_t* claim, uint32_t step,
+                                               CellState cs, uint32_t& sel, uint32_t& col,
+                                               double& sum_g) {
+  const unsigned lane = lane_id();
+  const float2 vm = *cs.maxrem;
+  const float fpc = ntc_fpc_fast(p, n, vm);
+  const uint32_t M = (uint32_t)fpc;
+  const uint32_t col0 = col;
+  const float vmax = ntc_select_heavy_warp(p, cell, n, acc, claim, step, M, vm.x, col, sum_g);
+  const uint32_t wcol = warp_sum(col - col0);
   if (lane == 0) {
     sel += M;
     *cs.maxrem = make_float2(vmax, fpc - (float)M);

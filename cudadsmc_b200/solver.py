@@ -202,7 +202,7 @@ class DSMCSolver:
         self._check(lib().dsmc_profile_read(self.h, _ptr(ms), _ptr(n)), "ProfileRead")
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNELS)}
 
-    KERNEL_SLOTS = ("scan", "scatter", "collide", "inject", "flight", "mesh", "sample")
+    KERNEL_SLOTS = ("scan", "scatter", "order", "inject", "flight", "mesh", "sample", "ntc")
 
     def ProfileOnly(self, kernels):
         """Keeps the open profile window's events to the named kernels."""
@@ -213,7 +213,7 @@ class DSMCSolver:
 
     def ProfileReadKernels(self):
         """{kernel: (total ms, launches)} since Profile(True), kernel by kernel
-        ("collide" is the fused cell kernel when a variant below 4 runs)."""
+        ("order" is the fused cell kernel when a variant below 4 runs)."""
         n = len(self.KERNEL_SLOTS)
         ms = np.zeros(n, np.float64)
         cnt = np.zeros(n, np.uint32)

@@ -151,12 +151,12 @@ int dsmc_get_info(dsmc_handle* h, dsmc_info* info);
  * 2 cell, 3 inflow injection) and closes the window. */
 int dsmc_profile(dsmc_handle* h, int enable);
 int dsmc_profile_read(dsmc_handle* h, double ms[4], uint32_t launches[4]);
-/* The same window kernel by kernel (n slots, at most 7 used): 0 scan,
+/* The same window kernel by kernel (n slots, at most 8 used): 0 scan,
  * 1 scatter, 2 the fused cell kernel or, with a split variant
- * (dsmc_set_kernel_variant >= 4), its order + collide kernel, 3 inflow
- * injection, 4 flight, 5 flights that may reach the body, 6 sampling.
- * dsmc_profile_read reports slots 2 and 4-6 summed as "cell".  No
- * counterpart in the reference. */
+ * (dsmc_set_kernel_variant >= 4), its order kernel (gather, stable order,
+ * pair counts), 3 inflow injection, 4 flight, 5 flights that may reach the
+ * body, 6 sampling, 7 NTC selections.  dsmc_profile_read reports slots 2 and
+ * 4-7 summed as "cell".  No counterpart in the reference. */
 int dsmc_profile_read_kernels(dsmc_handle* h, int n, double* ms, uint32_t* launches);
 /* Restricts the open window's events to the slots whose bits are set in
  * `slots` (bit k = slot k above); dsmc_profile(h, 1) times all of them.  An
