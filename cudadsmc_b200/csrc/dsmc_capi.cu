@@ -64,6 +64,14 @@ struct dsmc_handle {
   // per-kernel event timing (dsmc_profile)
   bool profiling = false;
   uint32_t prof_mask = 0xff;  // slots that get events while profiling
+  // graph replay with per-kernel events: event-record nodes are captured
+  // around the profiled kernels, and before every replay they are pointed at
+  // fresh events of ev[]
+  bool capturing = false;
+  std::vector<cudaEvent_t> cap_ev;        // placeholders used during capture (pairs)
+  std::vector<int> cap_slot;              // kernel slot of each captured pair
+  std::vector<cudaGraphNode_t> gev_node;  // the graph's event-record nodes, 2 per pair
+  uint32_t graph_prof_mask = 0;           // profiled slots the graph was captured with
   std::vector<cudaEvent_t> ev;      // pairs
   std::vector<int> ev_kernel;       // kernel id of each pair
   size_t ev_used = 0;
@@ -98,6 +106,9 @@ int cuda_fail(dsmc_handle* h, cudaError_t e, const char* where) {
 
 void drop_graph(dsmc_handle* h) {
   h->gen++;
+  h->graph_prof_mask = 0;
+  h->cap_slot.clear();
+  h->gev_node.clear();
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->graph_exec = nullptr;
@@ -134,6 +145,8 @@ cudaError_t dalloc(T** p, size_t n) {
 void free_all(dsmc_handle* h) {
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   h->ev.clear();
+  for (cudaEvent_t e : h->cap_ev) cudaEventDestroy(e);
+  h->cap_ev.clear();
   if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
   if (h->graph) cudaGraphDestroy(h->graph);
   h->graph_exec = nullptr;
@@ -235,10 +248,24 @@ void prof_flush(dsmc_handle* h) {
   h->ev_used = 0;
 }
 
+// Profiled launches a captured step may hold (each kernel slot at most twice).
+constexpr size_t kCapPairs = 16;
+
 // Launches `launch` with CUDA events around it when the handle is profiling.
 template <class F>
 cudaError_t timed(dsmc_handle* h, int kernel, F launch) {
   if (!h->profiling || !((h->prof_mask >> kernel) & 1u)) return launch();
+  if (h->capturing) {
+    // event-record nodes around the kernel, with placeholder events (created
+    // before the capture); a plain record inside a capture makes no node
+    const size_t k = h->cap_slot.size();
+    if (h->cap_ev.size() < 2 * (k + 1)) return cudaErrorInvalidValue;
+    h->cap_slot.push_back(kernel);
+    cudaError_t e = cudaEventRecordWithFlags(h->cap_ev[2 * k], h->stream, cudaEventRecordExternal);
+    if (!e) e = launch();
+    if (!e) e = cudaEventRecordWithFlags(h->cap_ev[2 * k + 1], h->stream, cudaEventRecordExternal);
+    return e;
+  }
   if (h->ev_used == kProfPairs) prof_flush(h);
   size_t i = h->ev_used++;
   h->ev_kernel[i] = kernel;
@@ -1106,25 +1133,61 @@ int dsmc_step(dsmc_handle* h, float dt, int nsteps) {
 int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps) {
   if (!h || nsteps < 0) return DSMC_ERR_ARG;
   if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
-  if (!h->graph_exec || h->graph_dt != dt) {
+  const uint32_t want_mask = h->profiling ? h->prof_mask : 0u;
+  if (!h->graph_exec || h->graph_dt != dt || h->graph_prof_mask != want_mask) {
     drop_graph(h);
+    while (h->cap_ev.size() < 2 * kCapPairs) {
+      cudaEvent_t ev = nullptr;
+      CK(h, cudaEventCreate(&ev), "graph event create");
+      h->cap_ev.push_back(ev);
+    }
     cudaStream_t cap = nullptr;
     CK(h, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "graph stream");
     cudaStream_t saved = h->stream;
-    const bool prof = h->profiling;
-    h->profiling = false;  // per-kernel events are not captured into the graph
+    h->capturing = true;  // profiled kernels get event-record nodes
     h->stream = cap;
     cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
     if (!e) e = enqueue_step(h, dt);
     cudaError_t e2 = cudaStreamEndCapture(cap, &h->graph);
     h->stream = saved;
-    h->profiling = prof;
+    h->capturing = false;
     cudaStreamDestroy(cap);
     if (e || e2) return cuda_fail(h, e ? e : e2, "graph capture");
+    // the event-record nodes, matched to their pairs by placeholder event
+    h->gev_node.assign(2 * h->cap_slot.size(), nullptr);
+    if (!h->cap_slot.empty()) {
+      size_t nn = 0;
+      CK(h, cudaGraphGetNodes(h->graph, nullptr, &nn), "graph nodes");
+      std::vector<cudaGraphNode_t> nodes(nn);
+      CK(h, cudaGraphGetNodes(h->graph, nodes.data(), &nn), "graph nodes");
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        CK(h, cudaGraphNodeGetType(nd, &ty), "graph node type");
+        if (ty != cudaGraphNodeTypeEventRecord) continue;
+        cudaEvent_t ev = nullptr;
+        CK(h, cudaGraphEventRecordNodeGetEvent(nd, &ev), "graph event node");
+        for (size_t k = 0; k < h->gev_node.size(); k++)
+          if (h->cap_ev[k] == ev) h->gev_node[k] = nd;
+      }
+      for (cudaGraphNode_t nd : h->gev_node)
+        if (!nd) return fail(h, DSMC_ERR_CUDA, "graph capture: an event-record node is missing");
+    }
     CK(h, cudaGraphInstantiate(&h->graph_exec, h->graph, 0), "graph instantiate");
     h->graph_dt = dt;
+    h->graph_prof_mask = want_mask;
   }
   for (int i = 0; i < nsteps; i++) {
+    // fresh events for this replay's profiled kernels
+    for (size_t k = 0; k < h->cap_slot.size(); k++) {
+      if (h->ev_used == kProfPairs) prof_flush(h);
+      const size_t j = h->ev_used++;
+      h->ev_kernel[j] = h->cap_slot[k];
+      CK(h, cudaGraphExecEventRecordNodeSetEvent(h->graph_exec, h->gev_node[2 * k], h->ev[2 * j]),
+         "graph event");
+      CK(h, cudaGraphExecEventRecordNodeSetEvent(h->graph_exec, h->gev_node[2 * k + 1],
+                                                 h->ev[2 * j + 1]),
+         "graph event");
+    }
     CK(h, cudaGraphLaunch(h->graph_exec, h->stream), "graph launch");
     h->step++;
     h->sim_time += dt;

@@ -630,7 +630,9 @@ __global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ St
       g = p.defer_list[i];
       pos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
       vel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
-      live = move_particle(p, pos, vel, g, step);
+      // listed because the path may reach the body: the first clearance test
+      // is already done
+      live = move_particle(p, pos, vel, g, step, true);
     }
     finish_flight(p, go, live, g, pos, vel, removed);
   }

@@ -274,6 +274,45 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
       tdel[a] = 3.0e38f;
     }
   }
+  // The cells the segment crosses are known before any triangle is tested:
+  // load the triangle ranges of the first few together and prefetch their
+  // planes and vertices into L2, so that the walk below pays one round trip to
+  // memory instead of three per cell (its loads then hit the caches).
+  {
+    constexpr int kAhead = 6;
+    int pidx[3] = {idx[0], idx[1], idx[2]};
+    float ptmax[3] = {tmax[0], tmax[1], tmax[2]};
+    uint2 pse[kAhead];
+    int np = 0;
+    bool more = true;
+#pragma unroll
+    for (int k = 0; k < kAhead; k++) {
+      if (more) {
+        // the walk's own stepping rule
+        const uint32_t c = ((uint32_t)pidx[2] * g.dim.y + (uint32_t)pidx[1]) * g.dim.x + (uint32_t)pidx[0];
+        pse[k] = __ldg(&G.start_end[c]);
+        np = k + 1;
+        const float texit = fminf(ptmax[0], fminf(ptmax[1], ptmax[2]));
+        if (texit > t1) {
+          more = false;
+        } else {
+          const int a = (ptmax[0] <= ptmax[1] && ptmax[0] <= ptmax[2]) ? 0 : (ptmax[1] <= ptmax[2] ? 1 : 2);
+          pidx[a] += stp[a];
+          if (pidx[a] < 0 || pidx[a] >= dm[a]) more = false;
+          else ptmax[a] += tdel[a];
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kAhead; k++) {
+      if (k < np && pse[k].x < pse[k].y) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(G.plane + pse[k].x));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(G.tri + kTriStride * (size_t)pse[k].x));
+        if (kTriStride * (pse[k].y - pse[k].x) > 8u)  // stays inside the cell's entries
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(G.tri + kTriStride * (size_t)pse[k].x + 8));
+      }
+    }
+  }
   float best = 3.0e38f;
   uint32_t best_i = kNone;
   const int max_iter = dm[0] + dm[1] + dm[2] + 3;

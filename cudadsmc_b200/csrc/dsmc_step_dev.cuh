@@ -562,8 +562,12 @@ __device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, fl
 // One particle's flight with the body: IntegrateDev / ProcessCollisionsDev,
 // kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.  Out
 // of line: only flights that may reach the body come here in the step.
+// pretested: the caller already found that the path from pos may reach the
+// body (flight_may_meet_body or its halves), so the first clearance test is
+// skipped (its answer is known).
 static __device__ __noinline__ bool move_particle_full(const StepParams& p, float3& pos,
-                                                       float3& vel, uint32_t gidx, uint32_t step) {
+                                                       float3& vel, uint32_t gidx, uint32_t step,
+                                                       bool pretested) {
   float3 old_pos = pos;
   pos.x = old_pos.x + vel.x * p.dt;
   pos.y = old_pos.y + vel.y * p.dt;
@@ -579,10 +583,12 @@ static __device__ __noinline__ bool move_particle_full(const StepParams& p, floa
       const float dist = length3(seg);
       if (!(dist > 1e-12f)) break;
       // a path shorter than the start cell's clearance cannot reach the body
-      const uint32_t cc = coll_cell_id(G.cgrid, old_pos);
-      if (cc != kNone && dist < __ldg(&G.clear[cc])) break;
-      // a path outside the geometry grid whose box misses the grid's box
-      if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
+      if (!(pretested && b == 0)) {
+        const uint32_t cc = coll_cell_id(G.cgrid, old_pos);
+        if (cc != kNone && dist < __ldg(&G.clear[cc])) break;
+        // a path outside the geometry grid whose box misses the grid's box
+        if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
+      }
       const float idist = 1.f / dist;
       const float3 d = make_float3(seg.x * idist, seg.y * idist, seg.z * idist);
       float t;
@@ -636,10 +642,11 @@ static __device__ __noinline__ bool move_particle_full(const StepParams& p, floa
 
 // One particle's flight (free flight inline, with a body out of line).
 __device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, float3& vel,
-                                              uint32_t gidx, uint32_t step) {
+                                              uint32_t gidx, uint32_t step,
+                                              bool pretested = false) {
   if (!p.has_geom) return move_free(p, pos, vel, gidx, step);
   float3 tp = pos, tv = vel;
-  const bool live = move_particle_full(p, tp, tv, gidx, step);
+  const bool live = move_particle_full(p, tp, tv, gidx, step, pretested);
   pos = tp;
   vel = tv;
   return live;

@@ -8,6 +8,7 @@ the C ABI of libdsmc_b200.so; errors raise ``DsmcError`` (the reference throws
 std::runtime_error).
 """
 import ctypes
+import sys
 
 import numpy as np
 
@@ -82,6 +83,8 @@ class DSMCSolver:
 
     def close(self):
         if getattr(self, "h", None):
+            if sys.is_finalizing():  # the interpreter is tearing down modules
+                return
             lib().dsmc_destroy(self.h)
             self.h = None
 
@@ -286,6 +289,8 @@ class DSMCBatch:
 
     def close(self):
         if getattr(self, "b", None):
+            if sys.is_finalizing():
+                return
             lib().dsmc_batch_destroy(self.b)
             self.b = None
 

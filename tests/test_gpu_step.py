@@ -204,3 +204,37 @@ def test_kernel_variants_give_identical_steps(cuda, rng, density):
         assert np.array_equal(out[0][1][1], out[v][1][1])
         assert np.array_equal(out[0][2], out[v][2], equal_nan=True)
     assert compared >= (nv - 1 if density <= 1e20 else 4)
+
+
+def test_graph_replay_profiles_kernels_without_changing_results(cuda):
+    """Graph replay with per-kernel events (event-record nodes retargeted
+    before every replay) times each kernel once per step and computes the
+    same steps as graph replay without them."""
+    out = []
+    for prof in (False, True):
+        s = make_settings(rng="philox", init_kind="maxwell", seed=9).set(sample_every=2)
+        solver = DSMCSolver().Init(s)
+        solver.SetKernelVariant(5)
+        solver.InitSystemState()
+        solver.RunSimulationStep(1e-5, 2)
+        if prof:
+            solver.Profile(True)
+        solver.StepGraph(1e-5, 5)
+        if prof:
+            k = solver.ProfileReadKernels()
+            for name in ("scan", "scatter", "order", "ntc", "flight", "sample"):
+                assert k[name][1] == 5 and k[name][0] > 0, (name, k[name])
+            # only the flight kernel, on the graph captured again for the mask
+            solver.Profile(True)
+            solver.ProfileOnly(["flight"])
+            solver.StepGraph(1e-5, 3)
+            k = solver.ProfileReadKernels()
+            assert set(k) == {"flight"} and k["flight"][1] == 3
+        else:
+            solver.StepGraph(1e-5, 3)
+        solver.Sync()
+        out.append((solver.DownloadState(), solver.GetCellState(), solver.Fields()))
+        solver.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1][0], out[1][1][0])
+    assert np.array_equal(out[0][2], out[1][2], equal_nan=True)
