@@ -144,8 +144,11 @@ typedef struct dsmc_info {
 int dsmc_get_info(dsmc_handle* h, dsmc_info* info);
 
 /* Per-kernel timing with CUDA events recorded around every launch of
- * dsmc_step on the handle's stream (no equivalent in the reference, which
- * times the whole loop only, kernels/dsmc.cu:440-449).  dsmc_profile(h, 1)
+ * dsmc_step and dsmc_step_graph on the handle's stream (no equivalent in the
+ * reference, which times the whole loop only, kernels/dsmc.cu:440-449).  A
+ * graph is captured with event-record nodes around the profiled kernels,
+ * retargeted at fresh events before each replay, and captured again when the
+ * profiled set changes.  dsmc_profile(h, 1)
  * starts a window, dsmc_profile_read returns per kernel the summed
  * milliseconds and launch counts since then (kernels: 0 scan, 1 scatter,
  * 2 cell, 3 inflow injection) and closes the window. */
@@ -237,7 +240,9 @@ int dsmc_get_cell_state(dsmc_handle* h, float* maxrem, uint32_t* seeds);
  * kernels/dsmc_base.cu:64-84): nsteps timesteps of length dt, sampling every
  * sample_every steps.  Asynchronous on the handle's stream. */
 int dsmc_step(dsmc_handle* h, float dt, int nsteps);
-/* Same as dsmc_step but replays a captured CUDA graph of the step. */
+/* Same as dsmc_step but replays a captured CUDA graph of the step (captured
+ * on the first call, and again after a change of dt, variant or profiled
+ * kernel set). */
 int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps);
 
 /* Launch shape of the step's cell kernel (no counterpart in the reference,
