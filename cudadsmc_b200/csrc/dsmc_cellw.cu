@@ -413,9 +413,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ St
 // ------------------------------------------------ flight + keys + sample ----
 
 // Next-step key and count of a flown particle (all lanes; `go`: this lane
-// flew one), its state stored at g.
+// flew one), its state stored at g.  The count goes to count[key]; the scan
+// tile's total to the block's histogram s_tile when given (flushed by the
+// caller), else straight to tile_sum.  Per group the tile atomic lands on one
+// of a few hundred addresses: from every warp of a full-GPU pass these
+// serialise in L2 (70 of the flight kernel's 125 us on 3.7M particles), so
+// the streaming kernels count tiles in shared memory.
 __device__ __forceinline__ void finish_flight(const StepParams& p, bool go, bool live, uint32_t g,
-                                              float3 pos, float3 vel, uint32_t& removed) {
+                                              float3 pos, float3 vel, uint32_t& removed,
+                                              uint32_t* s_tile = nullptr) {
   if (go) {
     p.out.x[g] = pos.x; p.out.y[g] = pos.y; p.out.z[g] = pos.z;
     p.out.u[g] = vel.x; p.out.v[g] = vel.y; p.out.w[g] = vel.z;
@@ -426,7 +432,10 @@ __device__ __forceinline__ void finish_flight(const StepParams& p, bool go, bool
     if (go && !live) removed++;
     if (has_key) {
       const uint32_t key = cell_id3d(p.grid, pos.x, pos.y, pos.z);
-      warp_count_key_global(p.count, key, m, p.tile_sum);
+      if (s_tile)
+        warp_count_key(p.count, key, m, s_tile);
+      else
+        warp_count_key_global(p.count, key, m, p.tile_sum);
       p.out_key[g] = key;
     } else if (go) {
       p.out_key[g] = kDeadKey;
@@ -455,6 +464,9 @@ __device__ __forceinline__ void list_deferred(const StepParams& p, const uint32_
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
   __shared__ uint32_t s_q[WARPS][kFlightQ];
+  extern __shared__ uint32_t s_tile[];  // this block's next-step counts per scan tile
+  for (uint32_t t = threadIdx.x; t < p.n_scan_tiles; t += blockDim.x) s_tile[t] = 0;
+  __syncthreads();
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const uint32_t n = p.meta->n_alive;
@@ -495,7 +507,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
     bool live = true;
     // a path that cannot reach the body
     if (go && do_move) live = move_free(p, pos, vel, g, step);
-    finish_flight(p, go, live, g, pos, vel, removed);
+    finish_flight(p, go, live, g, pos, vel, removed, s_tile);
     if (nq >= 32) {
       __syncwarp();
       nq -= 32;
@@ -511,6 +523,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
   }
   const uint32_t r = warp_sum(removed);
   if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+  __syncthreads();
+  flush_tile_hist(s_tile, p.tile_sum, p.n_scan_tiles);
 }
 
 // Paired form of k_flight_w: lane L flies particles 2L and 2L+1 of each group
@@ -523,6 +537,9 @@ constexpr uint32_t kFlightQ2 = 128;
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_constant__ StepParams p) {
   __shared__ uint32_t s_q[WARPS][kFlightQ2];
+  extern __shared__ uint32_t s_tile[];  // this block's next-step counts per scan tile
+  for (uint32_t t = threadIdx.x; t < p.n_scan_tiles; t += blockDim.x) s_tile[t] = 0;
+  __syncthreads();
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const uint32_t n = p.meta->n_alive;
@@ -581,7 +598,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_con
         if (go && !live[k]) removed++;
         if (has_key) {
           key[k] = cell_id3d(p.grid, pos[k].x, pos[k].y, pos[k].z);
-          warp_count_key_global(p.count, key[k], m, p.tile_sum);
+          warp_count_key(p.count, key[k], m, s_tile);
         }
       }
     }
@@ -611,6 +628,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_con
   }
   const uint32_t r = warp_sum(removed);
   if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+  __syncthreads();
+  flush_tile_hist(s_tile, p.tile_sum, p.n_scan_tiles);
 }
 
 // The listed flights, one particle per thread over the whole grid (the list's
@@ -705,15 +724,15 @@ cudaError_t launch_flight_w(const StepParams& p, cudaStream_t stream) {
   if (ls.device != dev) {
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flight_w<kFlightWarps, MINB>,
-                                                      kFlightWarps * 32, 0);
+                                                      kFlightWarps * 32, kMaxScanTiles * 4);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     ls.device = dev;
     ls.per_sm = per_sm;
   }
   // a full wave of warps: the particle count is known only on the device
-  k_flight_w<kFlightWarps, MINB>
-      <<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32, 0, stream>>>(p);
+  k_flight_w<kFlightWarps, MINB><<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
+                                   p.n_scan_tiles * 4u, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -727,14 +746,14 @@ cudaError_t launch_flight_pw(const StepParams& p, cudaStream_t stream) {
   if (ls.device != dev) {
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_flight_pw<kFlightWarps, MINB>,
-                                                      kFlightWarps * 32, 0);
+                                                      kFlightWarps * 32, kMaxScanTiles * 4);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  k_flight_pw<kFlightWarps, MINB>
-      <<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32, 0, stream>>>(p);
+  k_flight_pw<kFlightWarps, MINB><<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
+                                    p.n_scan_tiles * 4u, stream>>>(p);
   return cudaGetLastError();
 }
 
