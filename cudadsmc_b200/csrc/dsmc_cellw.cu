@@ -46,7 +46,8 @@ constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach 
 template <int CAPW>
 struct __align__(16) WarpSmem {
   float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
-  uint32_t cs[kWarpTile + 1];  // chunk-relative start of each tile cell
+  uint4 lbuf[2 * kWarpTile];   // light-cell list entries not yet in the global list
+  uint32_t cr[kWarpTile];      // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
   unsigned long long mbar[2];
   uint16_t slot[CAPW];         // sorted position -> staged index
 };
@@ -163,6 +164,41 @@ __device__ __forceinline__ void list_cells(uint4* list, uint32_t* counter, bool 
   if (put) list[base + __popc(m & ((1u << lane) - 1u))] = e;
 }
 
+// Appends e for every lane with `put` to the warp's buffer `buf` (cnt entries,
+// fewer than 32 between calls) and moves 32 at a time to the global list: one
+// returning atomic on the list's counter per 32 entries instead of one per
+// call, which every warp of the grid would otherwise wait on.
+__device__ __forceinline__ void buffer_cells(uint4* buf, uint32_t& cnt, uint4* list,
+                                             uint32_t* counter, bool put, uint4 e) {
+  const uint32_t lane = lane_id();
+  const unsigned m = __ballot_sync(kFull, put);
+  if (put) buf[cnt + __popc(m & ((1u << lane) - 1u))] = e;
+  cnt += __popc(m);
+  if (cnt >= 32) {
+    __syncwarp();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(kFull, base, 0);
+    list[base + lane] = buf[lane];
+    cnt -= 32;
+    __syncwarp();
+    if (lane < cnt) buf[lane] = buf[32 + lane];
+    __syncwarp();
+  }
+}
+
+// The rest of the buffer (cnt < 32 entries) to the global list.
+__device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint4* list,
+                                            uint32_t* counter) {
+  if (!cnt) return;
+  const uint32_t lane = lane_id();
+  __syncwarp();
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(counter, cnt);
+  base = __shfl_sync(kFull, base, 0);
+  if (lane < cnt) list[base + lane] = buf[lane];
+}
+
 // ---------------------------------------------------- order + pair counts ----
 
 template <int CAPW, int WARPS, int MINB>
@@ -195,6 +231,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
 
   uint32_t phase = 0;  // bit b: parity of the next phase of buffer b
   uint32_t sel = 0;
+  uint32_t lcnt = 0;   // entries in S.lbuf
   WChunk C;
   C.valid = 0;
   // (sigma g)max and remainder of a chunk's cells, loaded one chunk ahead
@@ -229,9 +266,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     const uint32_t cell = c0 + lane;
     const bool mine = lane >= C.cur && lane < C.cur + C.k;
     const uint32_t s0 = A.s - C.base, nc = A.e - A.s;  // meaningful for `mine`
+    const bool ne = mine && nc > 0;
     if (!C.giant && C.n) {
-      S.cs[lane] = s0;
-      if (lane == 31) S.cs[32] = A.e - C.base;
+      const unsigned ne_mask = __ballot_sync(kFull, ne);
+      if (ne) S.cr[__popc(ne_mask & ((1u << lane) - 1u))] = s0 | ((s0 + nc) << 16);
       const uint32_t par = (phase >> C.buf) & 1u;
       bool ok = mbar_wait_bounded(&S.mbar[C.buf], par);
       phase ^= 1u << C.buf;
@@ -258,8 +296,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
           p.maxrem[gc] = vm;
           sel += M;
         }
-        list_cells(p.ntc_light, &p.meta->n_light, lane == C.cur && M > 0,
-                   make_uint4(gc, C.base, C.n, M));
+        buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, lane == C.cur && M > 0,
+                     make_uint4(gc, C.base, C.n, M));
       }
     } else if (C.n > 0) {
       const uint32_t off = C.base & 3u;
@@ -287,20 +325,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       // smaller origs there, counted four at a time from the 16-byte aligned
       // staging row (element j sits at ORA[j + off]).
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][6]);
-      for (uint32_t t = lane; t < n; t += 32) {
+      for (uint32_t b0 = 0; b0 < n; b0 += 32) {
+        const uint32_t t = b0 + lane;
         if (!do_fixup) {
-          S.slot[t] = (uint16_t)t;
+          if (t < n) S.slot[t] = (uint16_t)t;
           continue;
         }
-        // the slot's cell: the last of the chunk's cells starting at or
-        // before t (an empty cell starts where the next one does)
-        uint32_t lc = C.cur, len = C.k;
-        while (len > 1) {
-          const uint32_t half = len >> 1;
-          if (S.cs[lc + half] <= t) lc += half;
-          len -= half;
-        }
-        const uint32_t a = S.cs[lc], b = S.cs[lc + 1];
+        // the slot's cell: the last nonempty cell starting at or before t,
+        // by its ordinal among them (lanes here stand for the tile's cells:
+        // the starts in [b0, b0 + 32) as a bit mask, and the count before)
+        const unsigned starts =
+            __reduce_or_sync(kFull, (ne && s0 >= b0 && s0 < b0 + 32u) ? 1u << (s0 - b0) : 0u);
+        const uint32_t before = __popc(__ballot_sync(kFull, ne && s0 < b0));
+        if (t >= n) continue;
+        const uint32_t ab = S.cr[before + __popc(starts & (0xffffffffu >> (31u - lane))) - 1u];
+        const uint32_t a = ab & 0xffffu, b = ab >> 16;
         const uint32_t my = OR[t];
         const uint32_t lo = a + off, hi = b + off;
         uint32_t rank = 0;
@@ -332,7 +371,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         }
         const bool heavy = heavy_mode && M >= kHeavyMin;
         const uint4 e = make_uint4(cell, base + s0, nc, M);
-        list_cells(p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
+        buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
       // C: the chunk in sorted order
@@ -352,6 +391,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     C = N;
     mr_c = mr_n;
   }
+  if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
   const unsigned long long s64 = warp_sum((unsigned long long)sel);
   if (lane == 0 && p.meta && s64) atomicAdd(&p.meta->selections, s64);
 }
@@ -634,6 +674,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_con
 
 // The listed flights, one particle per thread over the whole grid (the list's
 // order does not matter: each particle's flight, key and count are its own).
+// The flight with the body is inlined, at 2 CTAs per SM for its registers:
+// the list is a partial wave whose time is one traversal's chain of loads,
+// and a call's spills lengthened it (47 -> 35 us for 61k flights).
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
@@ -651,7 +694,7 @@ __global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ St
       vel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
       // listed because the path may reach the body: the first clearance test
       // is already done
-      live = move_particle(p, pos, vel, g, step, true);
+      live = move_particle_body(p, pos, vel, g, step, true);
     }
     finish_flight(p, go, live, g, pos, vel, removed);
   }
@@ -839,7 +882,7 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
       }
     case 3:
       // flights that may reach the body (listed only with a body and the move)
-      if (p.has_geom && (p.flags & kDoMove)) return launch_mesh_w<4>(p, stream);
+      if (p.has_geom && (p.flags & kDoMove)) return launch_mesh_w<2>(p, stream);
       return cudaSuccess;
     default:
       if (p.flags & kDoSample) return launch_sample_w(p, stream);

@@ -560,14 +560,14 @@ __device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, fl
 }
 
 // One particle's flight with the body: IntegrateDev / ProcessCollisionsDev,
-// kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.  Out
-// of line: only flights that may reach the body come here in the step.
+// kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.
 // pretested: the caller already found that the path from pos may reach the
 // body (flight_may_meet_body or its halves), so the first clearance test is
-// skipped (its answer is known).
-static __device__ __noinline__ bool move_particle_full(const StepParams& p, float3& pos,
-                                                       float3& vel, uint32_t gidx, uint32_t step,
-                                                       bool pretested) {
+// skipped (its answer is known).  Inline in the kernel that flies only such
+// flights (k_mesh_w: without a call its state stays in registers); other
+// kernels call the out-of-line move_particle_full.
+__device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& pos, float3& vel,
+                                                   uint32_t gidx, uint32_t step, bool pretested) {
   float3 old_pos = pos;
   pos.x = old_pos.x + vel.x * p.dt;
   pos.y = old_pos.y + vel.y * p.dt;
@@ -639,6 +639,12 @@ static __device__ __noinline__ bool move_particle_full(const StepParams& p, floa
   return apply_bc(p, pos, vel, rng);
 }
 
+// Out of line: only flights that may reach the body come here in the step.
+static __device__ __noinline__ bool move_particle_full(const StepParams& p, float3& pos,
+                                                       float3& vel, uint32_t gidx, uint32_t step,
+                                                       bool pretested) {
+  return move_particle_body(p, pos, vel, gidx, step, pretested);
+}
 
 // One particle's flight (free flight inline, with a body out of line).
 __device__ __forceinline__ bool move_particle(const StepParams& p, float3& pos, float3& vel,
