@@ -75,48 +75,70 @@ __global__ void k_index(GridGeom g, const float* __restrict__ x, const float* __
 __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor, uint32_t* start,
                                               uint32_t cells, const uint32_t* tile_sum, Meta* meta,
                                               int bump) {
-  __shared__ uint32_t s_warp[8];
-  __shared__ uint32_t s_base;
+  __shared__ uint32_t s_warp[8], s_part[8];
   const uint32_t b = blockIdx.x;
+  // the block's counts and the totals of the tiles before it, loaded together
+  const uint32_t c0 = b * kScanTile + threadIdx.x * 8;
+  // 8 whole counts, read and written 16 bytes at a time where the arrays
+  // allow it (the stage API's workspace may be only 4-byte aligned)
+  const bool vec = (((uintptr_t)count | (uintptr_t)start | (uintptr_t)cursor) & 15u) == 0;
+  const bool whole = vec && c0 + 8u <= cells;
+  uint32_t v[8];
+  if (whole) {
+    const uint4 lo = *reinterpret_cast<const uint4*>(count + c0);
+    const uint4 hi = *reinterpret_cast<const uint4*>(count + c0 + 4);
+    v[0] = lo.x; v[1] = lo.y; v[2] = lo.z; v[3] = lo.w;
+    v[4] = hi.x; v[5] = hi.y; v[6] = hi.z; v[7] = hi.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = (c0 + i < cells) ? count[c0 + i] : 0u;
+  }
   uint32_t part = 0;
   for (uint32_t t = threadIdx.x; t < b; t += blockDim.x) part += tile_sum[t];
   part = warp_sum(part);
-  if (lane_id() == 0) s_warp[threadIdx.x / 32] = part;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t s = 0;
-    for (int i = 0; i < 8; i++) s += s_warp[i];
-    s_base = s;
-  }
-  __syncthreads();
-  const uint32_t c0 = b * kScanTile + threadIdx.x * 8;
-  uint32_t v[8];
   uint32_t tsum = 0;
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    v[i] = (c0 + i < cells) ? count[c0 + i] : 0u;
-    tsum += v[i];
-  }
+  for (int i = 0; i < 8; i++) tsum += v[i];
   uint32_t incl = tsum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t t = __shfl_up_sync(kFull, incl, o);
     if ((int)lane_id() >= o) incl += t;
   }
-  __syncthreads();
   if (lane_id() == 31) s_warp[threadIdx.x / 32] = incl;
+  if (lane_id() == 0) s_part[threadIdx.x / 32] = part;
   __syncthreads();
-  uint32_t warp_off = 0;
-  for (uint32_t w = 0; w < threadIdx.x / 32; w++) warp_off += s_warp[w];
-  uint32_t run = s_base + warp_off + incl - tsum;
+  uint32_t run = incl - tsum;
+#pragma unroll
+  for (uint32_t w = 0; w < 8; w++) {
+    run += s_part[w];
+    if (w < threadIdx.x / 32) run += s_warp[w];
+  }
+  uint32_t st[8];
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    if (c0 + i < cells) {
-      start[c0 + i] = run;
-      count[c0 + i] = 0u;
-      if (cursor) cursor[c0 + i] = 0u;
-    }
+    st[i] = run;
     run += v[i];
+  }
+  if (whole) {
+    *reinterpret_cast<uint4*>(start + c0) = make_uint4(st[0], st[1], st[2], st[3]);
+    *reinterpret_cast<uint4*>(start + c0 + 4) = make_uint4(st[4], st[5], st[6], st[7]);
+    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(count + c0) = z;
+    *reinterpret_cast<uint4*>(count + c0 + 4) = z;
+    if (cursor) {
+      *reinterpret_cast<uint4*>(cursor + c0) = z;
+      *reinterpret_cast<uint4*>(cursor + c0 + 4) = z;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      if (c0 + i < cells) {
+        start[c0 + i] = st[i];
+        count[c0 + i] = 0u;
+        if (cursor) cursor[c0 + i] = 0u;
+      }
+    }
   }
   if (b == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) {
     start[cells] = run;
@@ -158,13 +180,26 @@ __global__ void __launch_bounds__(256, 4) k_scatter(SoA src, SoA dst, const uint
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   constexpr int U = kScatterU;
-  for (uint32_t base = gw * 32u * U; base < n; base += nw * 32u * U) {
+  const uint32_t stride = nw * 32u * U;
+  // keys of the next iteration load while this one's tickets are in flight
+  uint32_t nkey[U];
+#pragma unroll
+  for (int k = 0; k < U; k++) {
+    const uint32_t i = gw * 32u * U + 32u * k + lane;
+    nkey[k] = i < n ? __ldcs(&keys[i]) : kDeadKey;
+  }
+  for (uint32_t base = gw * 32u * U; base < n; base += stride) {
     uint32_t key[U];
     float x[U], y[U], z[U], u[U], v[U], w[U];
 #pragma unroll
     for (int k = 0; k < U; k++) {
+      key[k] = nkey[k];
+      const uint32_t i2 = base + stride + 32u * k + lane;
+      nkey[k] = i2 < n ? __ldcs(&keys[i2]) : kDeadKey;
+    }
+#pragma unroll
+    for (int k = 0; k < U; k++) {
       const uint32_t i = base + 32u * k + lane;
-      key[k] = i < n ? keys[i] : kDeadKey;
       x[k] = y[k] = z[k] = u[k] = v[k] = w[k] = 0.f;
       if (STATE && i < n) {
         x[k] = src.x[i]; y[k] = src.y[i]; z[k] = src.z[i];
