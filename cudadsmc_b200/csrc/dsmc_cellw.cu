@@ -164,6 +164,22 @@ __device__ __forceinline__ void list_cells(uint4* list, uint32_t* counter, bool 
   if (put) list[base + __popc(m & ((1u << lane) - 1u))] = e;
 }
 
+// Adds v, summed over the block, to *dst with one atomic (every thread of the
+// block calls it; s_red holds a slot per warp).  Per-warp atomics on one
+// address from every warp of a full-GPU pass serialise in L2 at the end of
+// the kernel, which then waits for them.
+template <class T>
+__device__ __forceinline__ void block_add(T* dst, T v, T* s_red) {
+  v = warp_sum(v);
+  if (lane_id() == 0) s_red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T t = s_red[0];
+    for (uint32_t w = 1; w < (blockDim.x >> 5); w++) t += s_red[w];
+    if (t != T(0)) atomicAdd(dst, t);
+  }
+}
+
 // Appends e for every lane with `put` to the warp's buffer `buf` (cnt entries,
 // fewer than 32 between calls) and moves 32 at a time to the global list: one
 // returning atomic on the list's counter per 32 entries instead of one per
@@ -392,8 +408,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     mr_c = mr_n;
   }
   if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
-  const unsigned long long s64 = warp_sum((unsigned long long)sel);
-  if (lane == 0 && p.meta && s64) atomicAdd(&p.meta->selections, s64);
+  __shared__ unsigned long long s_red[WARPS];
+  if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
 }
 
 // ------------------------------------------------------- NTC selections ----
@@ -442,11 +458,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ St
     __syncwarp();
     if (lane == 0) p.maxrem[e.x] = make_float2(vmax, vm.y);
   }
-  const unsigned long long c64 = warp_sum((unsigned long long)col);
-  const double g = warp_sum(sum_g);
-  if (lane == 0 && p.meta) {
-    if (c64) atomicAdd(&p.meta->collisions, c64);
-    if (g != 0.0) atomicAdd(&p.meta->sum_g, g);
+  __shared__ unsigned long long s_col[WARPS];
+  __shared__ double s_g[WARPS];
+  if (p.meta) {
+    block_add(&p.meta->collisions, (unsigned long long)col, s_col);
+    block_add(&p.meta->sum_g, sum_g, s_g);
   }
 }
 
@@ -561,8 +577,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
     __syncwarp();
     list_deferred(p, q, 0, nq);
   }
-  const uint32_t r = warp_sum(removed);
-  if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+  __shared__ uint32_t s_rm[WARPS];
+  if (p.meta) block_add(&p.meta->removed, removed, s_rm);
   __syncthreads();
   flush_tile_hist(s_tile, p.tile_sum, p.n_scan_tiles);
 }
@@ -666,8 +682,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_con
     __syncwarp();
     list_deferred(p, q, 0, nq);
   }
-  const uint32_t r = warp_sum(removed);
-  if (lane == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+  __shared__ uint32_t s_rm[WARPS];
+  if (p.meta) block_add(&p.meta->removed, removed, s_rm);
   __syncthreads();
   flush_tile_hist(s_tile, p.tile_sum, p.n_scan_tiles);
 }
@@ -698,8 +714,8 @@ __global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ St
     }
     finish_flight(p, go, live, g, pos, vel, removed);
   }
-  const uint32_t r = warp_sum(removed);
-  if (lane_id() == 0 && p.meta && r) atomicAdd(&p.meta->removed, r);
+  __shared__ uint32_t s_rm[8];
+  if (p.meta) block_add(&p.meta->removed, removed, s_rm);
 }
 
 // FP64 sampling after the flights, one cell per thread (the reference's
