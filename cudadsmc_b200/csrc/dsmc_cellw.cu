@@ -421,7 +421,11 @@ constexpr uint32_t kNtcClaim = 256;  // claim slots per warp: the largest chunk
 // (at most kNtcClaim particles: larger cells were collided by k_order_w).
 // The pair counts and remainders come from k_order_w; this kernel updates
 // (sigma g)max (and the HybridTaus state in the reference RNG mode) with the
-// same arithmetic and random streams as the fused path.
+// same arithmetic and random streams as the fused path.  The grid is one
+// wave: dense cells (the longest chains) go first, a warp each, then warps
+// claim light cells 32 at a time, so that the warps that finish early take
+// more (with a static split the blocks holding both a second round of light
+// cells and a dense cell set the kernel's length).
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ StepParams p) {
   __shared__ uint32_t s_claim[WARPS][kNtcClaim];
@@ -433,7 +437,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ St
   uint32_t col = 0;
   double sum_g = 0.0;
   const uint32_t nl = p.meta->n_light, nh = p.meta->n_heavy;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
+  const uint32_t gw = blockIdx.x * WARPS + warp, nw = gridDim.x * WARPS;
+  for (uint32_t h = gw; h < nh; h += nw) {
+    const uint4 e = p.ntc_heavy[h];
+    GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, e.y};
+    const float2 vm = p.maxrem[e.x];  // .y: the remainder k_order_w stored
+    const float vmax =
+        ntc_select_heavy_warp(p, e.x, e.z, acc, s_claim[warp], step, e.w, vm.x, col, sum_g);
+    __syncwarp();
+    if (lane == 0) p.maxrem[e.x] = make_float2(vmax, vm.y);
+  }
+  uint32_t* claims = &p.meta->tile_next2;
+  uint32_t next = 0;
+  if (lane == 0) next = atomicAdd(claims, 32u);
+  for (uint32_t base = __shfl_sync(kFull, next, 0); base < nl;) {
+    // the claim after this one, asked for ahead of need
+    if (lane == 0) next = atomicAdd(claims, 32u);
+    const uint32_t i = base + lane;
+    base = __shfl_sync(kFull, next, 0);
+    if (i >= nl) continue;
     const uint4 e = p.ntc_light[i];  // cell, first sorted slot, count, pairs
     GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, e.y};
     float2 vm = p.maxrem[e.x];
@@ -447,16 +469,6 @@ __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ St
       col += ntc_select_fast(p, e.x, e.z, acc, step, e.w, vm, sum_g);
     }
     p.maxrem[e.x] = vm;
-  }
-  const uint32_t gw = blockIdx.x * WARPS + warp, nw = gridDim.x * WARPS;
-  for (uint32_t h = gw; h < nh; h += nw) {
-    const uint4 e = p.ntc_heavy[h];
-    GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, e.y};
-    const float2 vm = p.maxrem[e.x];  // .y: the remainder k_order_w stored
-    const float vmax =
-        ntc_select_heavy_warp(p, e.x, e.z, acc, s_claim[warp], step, e.w, vm.x, col, sum_g);
-    __syncwarp();
-    if (lane == 0) p.maxrem[e.x] = make_float2(vmax, vm.y);
   }
   __shared__ unsigned long long s_col[WARPS];
   __shared__ double s_g[WARPS];

@@ -40,7 +40,7 @@ struct Meta {
   uint32_t injected;     // particles injected by the inflow faces (total)
   uint32_t removed;      // particles removed through outflow faces (total)
   uint32_t tile_next;    // the cell kernel's dynamic tile counter (reset by the scan)
-  uint32_t tile_next2;   // the flight kernel's dynamic tile counter (reset by the scan)
+  uint32_t tile_next2;   // the NTC kernel's claims of light cells (reset by the scan)
   uint32_t n_defer;      // flights listed for the mesh kernel this step (reset by the scan)
   uint32_t n_light;      // cells listed for the NTC kernel, one lane each (reset by the scan)
   uint32_t n_heavy;      // cells listed for the NTC kernel, one warp each (reset by the scan)
