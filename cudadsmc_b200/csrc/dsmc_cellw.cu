@@ -338,8 +338,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       }
       // A2: slot[sorted position] = staged index, sorted = (cell, orig).  The
       // origs are distinct, so a particle's rank in its cell is the number of
-      // smaller origs there, counted four at a time from the 16-byte aligned
-      // staging row (element j sits at ORA[j + off]).
+      // smaller origs there (element j of the chunk sits at ORA[j + off]).
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][6]);
       for (uint32_t b0 = 0; b0 < n; b0 += 32) {
         const uint32_t t = b0 + lane;
@@ -359,18 +358,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         const uint32_t my = OR[t];
         const uint32_t lo = a + off, hi = b + off;
         uint32_t rank = 0;
-        for (uint32_t jj = lo & ~3u; jj < hi; jj += 4) {
-          const uint4 o = *reinterpret_cast<const uint4*>(ORA + jj);
-          if (jj >= lo && jj + 4u <= hi) {
-            rank += (uint32_t)(o.x < my) + (uint32_t)(o.y < my) + (uint32_t)(o.z < my) +
-                    (uint32_t)(o.w < my);
-          } else {
-            rank += (uint32_t)(jj >= lo && o.x < my) +
-                    (uint32_t)(jj + 1u >= lo && jj + 1u < hi && o.y < my) +
-                    (uint32_t)(jj + 2u >= lo && jj + 2u < hi && o.z < my) +
-                    (uint32_t)(jj + 3u < hi && o.w < my);
-          }
-        }
+        // one element per step: the lanes of a cell read the same word
+        // (a broadcast), and lanes of different cells only differ in the
+        // trip count (a 16-byte form with edge cases diverged in both)
+        for (uint32_t j = lo; j < hi; j++) rank += (uint32_t)(ORA[j] < my);
         S.slot[a + rank] = (uint16_t)t;
       }
       cp_async_wait_all();
@@ -906,7 +897,7 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
       switch (v) {
         case 2: return launch_flight_pw<3>(p, stream);
         case 3: return launch_flight_pw<4>(p, stream);
-        default: return launch_flight_w<3>(p, stream);
+        default: return launch_flight_w<4>(p, stream);
       }
     case 3:
       // flights that may reach the body (listed only with a body and the move)
