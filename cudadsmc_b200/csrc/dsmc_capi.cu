@@ -61,6 +61,12 @@ struct dsmc_handle {
   cudaGraph_t graph = nullptr;
   float graph_dt = -1.f;
 
+  // the inflow branch: injection runs on `side` beside the NTC, flight,
+  // mesh and sampling kernels (forked after the order kernel, joined at the
+  // end of the step)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+
   // per-kernel event timing (dsmc_profile)
   bool profiling = false;
   uint32_t prof_mask = 0xff;  // slots that get events while profiling
@@ -143,6 +149,11 @@ cudaError_t dalloc(T** p, size_t n) {
 }
 
 void free_all(dsmc_handle* h) {
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join) cudaEventDestroy(h->ev_join);
+  if (h->side) cudaStreamDestroy(h->side);
+  h->ev_fork = h->ev_join = nullptr;
+  h->side = nullptr;
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   h->ev.clear();
   for (cudaEvent_t e : h->cap_ev) cudaEventDestroy(e);
@@ -275,7 +286,48 @@ cudaError_t timed(dsmc_handle* h, int kernel, F launch) {
   return e;
 }
 
-// One timestep: scan -> scatter -> cell (-> inflow injection).
+// The side stream and events of the inflow branch (created on first use,
+// outside any stream capture).
+cudaError_t ensure_side(dsmc_handle* h) {
+  if (h->side) return cudaSuccess;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+  if (!e) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+  if (!e) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+  return e;
+}
+
+// Inflow injection of every inflow face on `stream` (timed when on the
+// handle's stream).
+cudaError_t enqueue_inflow(dsmc_handle* h, float dt, uint2 seed, cudaStream_t stream) {
+  for (const auto& in : h->inflows) {
+    dsmcb::InjectParams ip{};
+    ip.grid = h->grid;
+    ip.cells = h->cells;
+    ip.inflow = in;
+    ip.dt = dt;
+    ip.seed = seed;
+    ip.capacity = h->capacity;
+    ip.remainder = h->inj_rem + in.face;
+    ip.st = soa_of(h->A);
+    ip.keys = h->keys;
+    ip.count = h->count;
+    ip.tile_sum = h->tile_sum;
+    ip.n_scan_tiles = h->n_scan_tiles;
+    ip.plan = h->inj_plan + 2 * in.face;
+    ip.meta = h->meta;
+    const cudaError_t e = stream == h->stream
+                              ? timed(h, 3, [&] { return dsmcb::launch_inject(ip, stream); })
+                              : dsmcb::launch_inject(ip, stream);
+    if (e) return e;
+  }
+  return cudaSuccess;
+}
+
+// One timestep: scan -> scatter -> cell (-> inflow injection).  With the split
+// kernels the injection runs on the side stream once the order kernel has
+// gathered the old state: it writes only slots past the sorted particles and
+// adds to the counts atomically, so it overlaps the NTC, flight, mesh and
+// sampling kernels, which touch only the sorted particles.
 cudaError_t enqueue_step(dsmc_handle* h, float dt) {
   cudaError_t e;
   e = timed(h, 0, [&] {
@@ -304,6 +356,10 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
   p.defer_list = h->orig;
   p.ntc_light = h->ntc_list;
   p.ntc_heavy = h->ntc_list + h->cells;
+  // the inflow branch (not while the injection itself is being timed: its
+  // events are on the handle's stream)
+  const bool fork = split && !h->inflows.empty() && h->side &&
+                    !(h->profiling && ((h->prof_mask >> 3) & 1u));
   if (split) {
     static const int slot[5] = {2, 7, 4, 5, 6};
     for (int stage = 0; stage < 5; stage++) {
@@ -311,31 +367,20 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
         return dsmcb::launch_split_stage(p, h->variant - 4, stage, h->stream);
       });
       if (e) return e;
+      if (stage == 0 && fork) {
+        e = cudaEventRecord(h->ev_fork, h->stream);
+        if (!e) e = cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+        if (!e) e = enqueue_inflow(h, dt, p.seed, h->side);
+        if (!e) e = cudaEventRecord(h->ev_join, h->side);
+        if (e) return e;
+      }
     }
+    if (fork) return cudaStreamWaitEvent(h->stream, h->ev_join, 0);
   } else {
     e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
     if (e) return e;
   }
-  for (const auto& in : h->inflows) {
-    dsmcb::InjectParams ip{};
-    ip.grid = h->grid;
-    ip.cells = h->cells;
-    ip.inflow = in;
-    ip.dt = dt;
-    ip.seed = p.seed;
-    ip.capacity = h->capacity;
-    ip.remainder = h->inj_rem + in.face;
-    ip.st = soa_of(h->A);
-    ip.keys = h->keys;
-    ip.count = h->count;
-    ip.tile_sum = h->tile_sum;
-    ip.n_scan_tiles = h->n_scan_tiles;
-    ip.plan = h->inj_plan + 2 * in.face;
-    ip.meta = h->meta;
-    e = timed(h, 3, [&] { return dsmcb::launch_inject(ip, h->stream); });
-    if (e) return e;
-  }
-  return cudaSuccess;
+  return enqueue_inflow(h, dt, p.seed, h->stream);
 }
 
 // Inflow fluxes of the faces marked DSMC_FACE_INFLOW: number flux of a
@@ -548,6 +593,7 @@ int dsmc_create(const dsmc_config* cfg, dsmc_handle** out) {
 int dsmc_destroy(dsmc_handle* h) {
   if (!h) return DSMC_ERR_ARG;
   cudaStreamSynchronize(h->stream);
+  if (h->side) cudaStreamSynchronize(h->side);
   free_all(h);
   delete h;
   return DSMC_OK;
@@ -1121,6 +1167,7 @@ int dsmc_get_cell_state(dsmc_handle* h, float* maxrem, uint32_t* seeds) {
 int dsmc_step(dsmc_handle* h, float dt, int nsteps) {
   if (!h || nsteps < 0) return DSMC_ERR_ARG;
   if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
+  CK(h, ensure_side(h), "side stream");
   for (int i = 0; i < nsteps; i++) {
     cudaError_t e = enqueue_step(h, dt);
     if (e) return cuda_fail(h, e, "step launch");
@@ -1133,6 +1180,7 @@ int dsmc_step(dsmc_handle* h, float dt, int nsteps) {
 int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps) {
   if (!h || nsteps < 0) return DSMC_ERR_ARG;
   if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
+  CK(h, ensure_side(h), "side stream");
   const uint32_t want_mask = h->profiling ? h->prof_mask : 0u;
   if (!h->graph_exec || h->graph_dt != dt || h->graph_prof_mask != want_mask) {
     drop_graph(h);
@@ -1659,6 +1707,10 @@ int batch_capture(dsmc_batch* b, const std::vector<float>& dt) {
   const size_t n = b->members.size();
   std::vector<cudaStream_t> saved(n);
   std::vector<bool> prof(n);
+  for (size_t i = 0; i < n; i++) {
+    const cudaError_t es = ensure_side(b->members[i]);
+    if (es) return batch_fail(b, DSMC_ERR_CUDA, std::string("side stream: ") + cudaGetErrorString(es));
+  }
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (!e) e = cudaEventRecord(b->ev[0], b->stream);
   for (size_t i = 0; i < n && !e; i++) {

@@ -121,3 +121,43 @@ def test_run_to_run_deterministic(cuda, rng):
         out.append(sol.DownloadState())
         sol.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_inflow_branch_matches_serial_injection(cuda, graph):
+    """With the split kernels the inflow injection runs on a side stream
+    beside the NTC, flight, mesh and sampling kernels; while the injection is
+    profiled it runs in line on the handle's stream.  Both orders compute the
+    same steps."""
+    U, T, nd = 1500.0, 200.0, 1e20
+    dims = (32, 16, 16)
+    out = []
+    for profiled in (False, True):
+        s = settings_t().set(grid_min=(0, 0, 0), grid_max=(1.2, 0.6, 0.6), grid_dim=dims,
+                             density=nd, fnum=nd * (1.2 / 32) * (0.6 / 16) ** 2 / 10, temp=T,
+                             stream_vel=(U, 0, 0), gas_mass=M_AR, gas_diam=D_AR, gas_tref=273.0,
+                             gas_omega=0.81, rng="philox", ntc_local=1, init_kind="maxwell",
+                             sample_every=5, capacity_factor=1.5,
+                             face_kind={"-x": "inflow", "+x": "outflow", "-y": "outflow",
+                                        "+y": "outflow", "-z": "outflow", "+z": "outflow"}, seed=5)
+        sol = DSMCSolver().Init(s)
+        sol.SetKernelVariant(5)
+        sol.InitSystemState()
+        if profiled:
+            sol.Profile(True)
+        if graph:
+            sol.StepGraph(4e-6, 60)
+        else:
+            sol.RunSimulationStep(4e-6, 60)
+        if profiled:
+            k = sol.ProfileReadKernels()
+            assert k["inject"][1] == 60, k["inject"]
+        sol.Sync()
+        info = sol.Info()
+        out.append((sol.DownloadState(), sol.Fields(), info.injected, info.removed,
+                    info.num_particles))
+        sol.close()
+    assert out[0][2] > 0 and out[0][3] > 0
+    assert out[0][2:] == out[1][2:]
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1], equal_nan=True)
