@@ -49,7 +49,6 @@ struct __align__(16) WarpSmem {
   uint4 lbuf[2 * kWarpTile];   // light-cell list entries not yet in the global list
   uint32_t cr[kWarpTile];      // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
   unsigned long long mbar[2];
-  uint16_t slot[CAPW];         // sorted position -> staged index
 };
 
 template <int CAPW, int WARPS>
@@ -325,47 +324,45 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       float* W = S.part[C.buf][5] + off;
       const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][6] + off);
       const uint32_t base = C.base, n = C.n;
-      // A0: gather of the chunk's state through orig (asynchronous 4-byte
-      // copies, in flight while the order is restored)
-      for (uint32_t t = lane; t < n; t += 32) {
-        const uint32_t i = OR[t];
-        cp_async4(X + t, p.in.x + i);
-        cp_async4(Y + t, p.in.y + i);
-        cp_async4(Z + t, p.in.z + i);
-        cp_async4(U + t, p.in.u + i);
-        cp_async4(V + t, p.in.v + i);
-        cp_async4(W + t, p.in.w + i);
-      }
-      // A2: slot[sorted position] = staged index, sorted = (cell, orig).  The
-      // origs are distinct, so a particle's rank in its cell is the number of
-      // smaller origs there (element j of the chunk sits at ORA[j + off]).
+      // A: each particle's sorted position, sorted = (cell, orig), then the
+      // gather of its state through orig straight to that position
+      // (asynchronous 4-byte copies, in flight while the pair counts run).
+      // The origs are distinct, so a particle's rank in its cell is the
+      // number of smaller origs there (element j of the chunk sits at
+      // ORA[j + off]).
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][6]);
       for (uint32_t b0 = 0; b0 < n; b0 += 32) {
         const uint32_t t = b0 + lane;
-        if (!do_fixup) {
-          if (t < n) S.slot[t] = (uint16_t)t;
-          continue;
+        const uint32_t my = t < n ? OR[t] : 0u;
+        uint32_t pos = t;
+        if (do_fixup) {
+          // the slot's cell: the last nonempty cell starting at or before t,
+          // by its ordinal among them (lanes here stand for the tile's cells:
+          // the starts in [b0, b0 + 32) as a bit mask, and the count before)
+          const unsigned starts =
+              __reduce_or_sync(kFull, (ne && s0 >= b0 && s0 < b0 + 32u) ? 1u << (s0 - b0) : 0u);
+          const uint32_t before = __popc(__ballot_sync(kFull, ne && s0 < b0));
+          if (t < n) {
+            const uint32_t ab = S.cr[before + __popc(starts & (0xffffffffu >> (31u - lane))) - 1u];
+            const uint32_t a = ab & 0xffffu, b = ab >> 16;
+            const uint32_t lo = a + off, hi = b + off;
+            uint32_t rank = 0;
+            // one element per step: the lanes of a cell read the same word
+            // (a broadcast), and lanes of different cells only differ in the
+            // trip count (a 16-byte form with edge cases diverged in both)
+            for (uint32_t j = lo; j < hi; j++) rank += (uint32_t)(ORA[j] < my);
+            pos = a + rank;
+          }
         }
-        // the slot's cell: the last nonempty cell starting at or before t,
-        // by its ordinal among them (lanes here stand for the tile's cells:
-        // the starts in [b0, b0 + 32) as a bit mask, and the count before)
-        const unsigned starts =
-            __reduce_or_sync(kFull, (ne && s0 >= b0 && s0 < b0 + 32u) ? 1u << (s0 - b0) : 0u);
-        const uint32_t before = __popc(__ballot_sync(kFull, ne && s0 < b0));
-        if (t >= n) continue;
-        const uint32_t ab = S.cr[before + __popc(starts & (0xffffffffu >> (31u - lane))) - 1u];
-        const uint32_t a = ab & 0xffffu, b = ab >> 16;
-        const uint32_t my = OR[t];
-        const uint32_t lo = a + off, hi = b + off;
-        uint32_t rank = 0;
-        // one element per step: the lanes of a cell read the same word
-        // (a broadcast), and lanes of different cells only differ in the
-        // trip count (a 16-byte form with edge cases diverged in both)
-        for (uint32_t j = lo; j < hi; j++) rank += (uint32_t)(ORA[j] < my);
-        S.slot[a + rank] = (uint16_t)t;
+        if (t < n) {
+          cp_async4(X + pos, p.in.x + my);
+          cp_async4(Y + pos, p.in.y + my);
+          cp_async4(Z + pos, p.in.z + my);
+          cp_async4(U + pos, p.in.u + my);
+          cp_async4(V + pos, p.in.v + my);
+          cp_async4(W + pos, p.in.w + my);
+        }
       }
-      cp_async_wait_all();
-      __syncwarp();
       // B: pair counts (the new remainder is stored now); cells with pairs
       // are listed for k_ntc_w, light ones to get a lane, dense ones a warp
       if (do_collide) {
@@ -381,11 +378,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      // C: the chunk in sorted order
+      cp_async_wait_all();
+      __syncwarp();
+      // C: the chunk, now in sorted order, to the mid arrays
       for (uint32_t q = lane; q < n; q += 32) {
-        const uint32_t j = S.slot[q], g = base + q;
-        p.mid.x[g] = X[j]; p.mid.y[g] = Y[j]; p.mid.z[g] = Z[j];
-        p.mid.u[g] = U[j]; p.mid.v[g] = V[j]; p.mid.w[g] = W[j];
+        const uint32_t g = base + q;
+        p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
+        p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
       }
     }
     __syncwarp();
