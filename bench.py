@@ -533,20 +533,27 @@ def run_batch(args, rank, world):
 
 
 def run_e2e(args, wl, rank, world, dev, variant):
-    """The same metric through the C ABI with host buffers: per run the
-    pinned initial state is uploaded (h2d), then every step is one dsmc_step
-    call followed by a device->host read of that step's collision totals, and
-    the sampled fields are read back at the end (d2h)."""
+    """The same metric through the C ABI with host buffers, driven as a host
+    program would: per run the pinned initial state is uploaded (h2d); every
+    step is one replay of the step's graph (dsmc_step_graph) followed by an
+    asynchronous copy of that step's collision totals into pinned host memory
+    (dsmc_totals_async), which the host reads while the next step runs (after
+    enqueueing step i it waits for step i-1's copy); the sampled fields are
+    read back at the end (d2h)."""
     import torch
     sol = build_solver(wl, seed_offset=rank)
+    sol.SetStream(torch.cuda.current_stream().cuda_stream)
     sol.SetKernelVariant(variant)
-    n0 = sol.InitSystemState()
+    sol.InitSystemState()
     state = sol.DownloadState()  # the initial state, as a host would provide it
     host = torch.from_numpy(state).pin_memory()
+    tot = torch.zeros((2, 24), dtype=torch.uint8).pin_memory()
+    ev = [torch.cuda.Event(), torch.cuda.Event()]
     dt = wl["settings"]["dt"]
-    k = max(3, min(args.steps, args.e2e_steps))
-    sol.UploadState(host.numpy(), soa=True)  # warm the path once
-    sol.RunSimulationStep(dt, 3)
+    # as many steps as the device-timed region: a run uploads its state once
+    k = max(3, args.steps if args.e2e_steps is None else min(args.steps, args.e2e_steps))
+    sol.UploadState(host.numpy(), soa=True)  # warm the path once (captures the step graph)
+    sol.StepGraph(dt, 3)
     sol.Sync()
     if world > 1:
         torch.distributed.barrier()
@@ -554,19 +561,28 @@ def run_e2e(args, wl, rank, world, dev, variant):
     t0 = time.perf_counter()
     sol.UploadState(host.numpy(), soa=True)
     i0 = sol.Info().particle_steps
-    for _ in range(k):
-        sol.RunSimulationStep(dt, 1)
-        sol.Totals()
+    totals = None
+    for i in range(k):
+        sol.StepGraph(dt, 1)
+        sol.TotalsAsync(tot[i % 2].data_ptr())
+        ev[i % 2].record()
+        if i:
+            ev[(i - 1) % 2].synchronize()
+            totals = sol.TotalsFromBytes(tot[(i - 1) % 2].numpy())
+    ev[(k - 1) % 2].synchronize()
+    totals = sol.TotalsFromBytes(tot[(k - 1) % 2].numpy())
     fields = sol.Fields()
     t1 = time.perf_counter()
     pst = sol.Info().particle_steps - i0
-    el, tot = reduce_over_ranks(t1 - t0, pst, world, dev)
+    assert totals[1] > 0 and totals[0] >= totals[1]
+    el, total = reduce_over_ranks(t1 - t0, pst, world, dev)
     sol.close()
-    return {"value": tot / el, "unit": "particle-timesteps/s",
+    return {"value": total / el, "unit": "particle-timesteps/s",
             "h2d_bytes_per_step": int(state.nbytes / k),
             "d2h_bytes_per_step": int(24 + fields.nbytes / k), "steps": k,
-            "note": "upload of the initial pinned state + one C-ABI dsmc_step and a totals read per step "
-                    "+ the sampled fields at the end"}
+            "note": "upload of the initial pinned state + per step one C-ABI dsmc_step_graph and an "
+                    "asynchronous totals read into pinned memory (read by the host during the next "
+                    "step) + the sampled fields at the end"}
 
 
 # ---------------------------------------------------------- reference arm ---
@@ -598,7 +614,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
-    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="steps of the end-to-end leg (default: --steps)")
     ap.add_argument("--tune-steps", type=int, default=10,
                     help="steps per launch shape of the autotuner (0: use --variant)")
     ap.add_argument("--variant", type=int, default=5,

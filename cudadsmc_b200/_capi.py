@@ -142,6 +142,7 @@ SIGNATURES = [
     ("dsmc_read_cell_sums", _I, [_P, _P, ctypes.POINTER(_U32)]),
     ("dsmc_read_fields", _I, [_P, _P]),
     ("dsmc_get_totals", _I, [_P, _P]),
+    ("dsmc_totals_async", _I, [_P, _P]),
     ("dsmc_dump_statistics", _I, [_P, ctypes.c_char_p]),
     ("dsmc_snapshot", _I, [_P, ctypes.c_char_p]),
     ("dsmc_restore", _I, [_P, ctypes.c_char_p]),

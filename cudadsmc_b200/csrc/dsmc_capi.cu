@@ -1,5 +1,6 @@
 // C ABI of the B200 DSMC timestep (declared in include/dsmc_b200.h).
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -1369,6 +1370,16 @@ int dsmc_get_totals(dsmc_handle* h, double totals[3]) {
   totals[0] = (double)m.selections;
   totals[1] = (double)m.collisions;
   totals[2] = m.sum_g;
+  return DSMC_OK;
+}
+
+int dsmc_totals_async(dsmc_handle* h, void* out) {
+  if (!h || !out) return DSMC_ERR_ARG;
+  static_assert(offsetof(Meta, collisions) == offsetof(Meta, selections) + 8 &&
+                    offsetof(Meta, sum_g) == offsetof(Meta, selections) + 16,
+                "the running totals are 24 contiguous bytes of Meta");
+  CK(h, cudaMemcpyAsync(out, &h->meta->selections, 24, cudaMemcpyDeviceToHost, h->stream),
+     "totals copy");
   return DSMC_OK;
 }
 

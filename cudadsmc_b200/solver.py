@@ -187,6 +187,21 @@ class DSMCSolver:
         self._check(lib().dsmc_get_totals(self.h, _ptr(t)), "Totals")
         return t
 
+    def TotalsAsync(self, out_ptr):
+        """Enqueues a copy of the running totals (24 bytes: selections and
+        collisions as uint64, the sum of relative speeds as float64) into the
+        host buffer at out_ptr (pinned memory) without waiting; the values are
+        there once the solver's stream has passed this point."""
+        self._check(lib().dsmc_totals_async(self.h, ctypes.c_void_p(out_ptr)), "TotalsAsync")
+
+    @staticmethod
+    def TotalsFromBytes(buf):
+        """(selections, collisions, sum of relative speeds) from the 24 bytes
+        TotalsAsync wrote (a uint8 array or anything numpy can view)."""
+        b = np.asarray(buf, dtype=np.uint8).reshape(-1)[:24]
+        return np.array([float(b[:8].view(np.uint64)[0]), float(b[8:16].view(np.uint64)[0]),
+                         float(b[16:24].view(np.float64)[0])])
+
     def Info(self):
         i = Info()
         self._check(lib().dsmc_get_info(self.h, ctypes.byref(i)), "Info")

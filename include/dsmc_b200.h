@@ -305,6 +305,14 @@ int dsmc_read_fields(dsmc_handle* h, double* fields5);
 /* GetStatistics (kernels/dsmc_kernel.cu:840-854): selections, collisions,
  * sum of relative speeds of collisions (all steps so far). */
 int dsmc_get_totals(dsmc_handle* h, double totals[3]);
+/* The same totals without waiting: enqueues on the handle's stream a copy of
+ * 24 bytes into `out` (selections and collisions as uint64, the sum of
+ * relative speeds as double), valid once the stream has passed this point
+ * (an event recorded after the call, or dsmc_sync).  `out` should be pinned
+ * host memory for the copy to stay asynchronous.  No counterpart in the
+ * reference, which reads its statistics synchronously; it lets a host read
+ * every step's totals while the next step runs. */
+int dsmc_totals_async(dsmc_handle* h, void* out);
 /* DSMCSolver::DumpStatistics (kernels/dsmc_base.cu:165-174) as text. */
 int dsmc_dump_statistics(dsmc_handle* h, const char* path);
 

@@ -238,3 +238,23 @@ def test_graph_replay_profiles_kernels_without_changing_results(cuda):
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1][0], out[1][1][0])
     assert np.array_equal(out[0][2], out[1][2], equal_nan=True)
+
+
+def test_totals_async_matches_totals(cuda):
+    """dsmc_totals_async copies the running totals (uint64 selections and
+    collisions, float64 sum of relative speeds) without waiting; after a sync
+    they equal dsmc_get_totals."""
+    import torch
+    s = make_settings(rng="philox", init_kind="maxwell", seed=4)
+    solver = DSMCSolver().Init(s)
+    solver.SetStream(torch.cuda.current_stream().cuda_stream)
+    solver.InitSystemState()
+    buf = torch.zeros(24, dtype=torch.uint8).pin_memory()
+    solver.StepGraph(1e-5, 4)
+    solver.TotalsAsync(buf.data_ptr())
+    torch.cuda.current_stream().synchronize()
+    got = DSMCSolver.TotalsFromBytes(buf.numpy())
+    want = solver.Totals()
+    assert want[1] > 0
+    assert np.array_equal(got, want)
+    solver.close()
