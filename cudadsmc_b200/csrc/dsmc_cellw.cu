@@ -513,12 +513,15 @@ __device__ __forceinline__ void list_deferred(const StepParams& p, const uint32_
 }
 
 // Free flights of the sorted particles [0, n_alive), read from p.mid (the
-// state k_order_w and k_ntc_w produced) and written to p.out.  Warps take groups of 32
-// in grid-stride order (the work per particle is even once the flights that
-// may reach the body are listed for k_mesh_w, which spreads them over the
-// whole GPU: they cluster next to the body).  The state of a group is loaded
-// two iterations ahead, and in nearest mode the clearance lookup of its
-// deferral test one iteration ahead, so that both latencies are covered.
+// state k_order_w and k_ntc_w produced) and written to p.out.  Each warp
+// takes a contiguous run of groups of 32 (the work per particle is even once
+// the flights that may reach the body are listed for k_mesh_w, which spreads
+// them over the whole GPU: they cluster next to the body); a warp's listed
+// flights are then neighbours, so each 32-entry chunk of the list holds
+// flights through the same few geometry cells for one warp of k_mesh_w.  The
+// state of a group is loaded two iterations ahead, and in nearest mode the
+// clearance lookup of its deferral test one iteration ahead, so that both
+// latencies are covered.
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
   __shared__ uint32_t s_q[WARPS][kFlightQ];
@@ -532,10 +535,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
   const bool split = p.has_geom && do_move;
   const bool piped = split && p.geom.nearest;
   uint32_t* q = s_q[warp];
-  const uint32_t stride = gridDim.x * WARPS * 32u;
-  const uint32_t g0 = (blockIdx.x * WARPS + warp) * 32u + lane;
+  // this warp's groups: per of the ceil(n / 32) groups from gb, particles [gb * 32, end)
+  const uint32_t ngroups = (n + 31u) / 32u, nwarps = gridDim.x * WARPS;
+  const uint32_t per = (ngroups + nwarps - 1u) / nwarps;
+  const uint32_t gb = min((blockIdx.x * WARPS + warp) * per, ngroups);
+  const uint32_t end = min(min(gb + per, ngroups) * 32u, n);
+  const uint32_t stride = 32u;
+  const uint32_t g0 = gb * 32u + lane;
   auto load = [&](uint32_t g, float3& pos, float3& vel) {
-    if (g < n) {
+    if (g < end) {
       pos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
       vel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
     }
@@ -547,13 +555,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
   load(g0, pos0, vel0);
   load(g0 + stride, pos1, vel1);
   float clr0 = -1.f;
-  if (piped && g0 < n) clr0 = defer_lookup(p, pos0);
+  if (piped && g0 < end) clr0 = defer_lookup(p, pos0);
   uint32_t removed = 0, nq = 0;
-  for (uint32_t g = g0; g - lane < n; g += stride) {
-    const bool active = g < n;
+  for (uint32_t g = g0; g - lane < end; g += stride) {
+    const bool active = g < end;
     load(g + 2u * stride, pos2, vel2);
     float clr1 = -1.f;
-    if (piped && g + stride < n) clr1 = defer_lookup(p, pos1);
+    if (piped && g + stride < end) clr1 = defer_lookup(p, pos1);
     float3 pos = pos0, vel = vel0;
     bool defer = false;
     if (active && split)
