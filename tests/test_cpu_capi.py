@@ -232,3 +232,14 @@ def test_replica_reduction_two_ranks_gloo():
     for rank, ms, tot in res:
         assert ms == 11.0  # slowest rank
         assert tot == 3000.0  # all particle-steps
+
+
+def test_totals_bytes_layout():
+    """dsmc_totals_async writes selections and collisions as uint64 and the
+    sum of relative speeds as float64, 24 bytes; TotalsFromBytes reads them."""
+    b = np.zeros(24, np.uint8)
+    b[:8].view(np.uint64)[0] = 2**40 + 3
+    b[8:16].view(np.uint64)[0] = 12345
+    b[16:24].view(np.float64)[0] = 6.5e9
+    t = cb.DSMCSolver.TotalsFromBytes(b)
+    assert t.tolist() == [float(2**40 + 3), 12345.0, 6.5e9]
