@@ -273,6 +273,28 @@ def cpu_oracle_sample(wl, budget_s=12.0, max_threads=None):
     return n * steps / t_total, O.threads(), desc, n, steps, t_total
 
 
+def legacy_cpu_sample(budget_s=5.0, particles_per_cell=90):
+    """The reference's legacy 2-D CPU solver (src/dsmc_cpu.cpp: UpdateGridCPU,
+    ComputeNanbuCPU, IntegrateCPU on its compile-time 30 x 18 grid), built
+    unchanged from the reference's sources into oracle/_ref/dsmc_cpu_legacy,
+    single thread, for about budget_s seconds.  It is not the 3-D step and
+    its physics is not comparable; it is reported beside the port as the only
+    CPU solver the reference ships.  None when the prebuilt driver is absent."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "dsmc_cpu_legacy")
+    dat = os.path.join(ROOT, "oracle", "_ref", "MersenneTwister.dat")
+    if not (os.path.isfile(exe) and os.path.isfile(dat)):
+        return None
+    r = subprocess.run([exe, dat, str(particles_per_cell), str(budget_s), "100000", "999"],
+                       capture_output=True, text=True, timeout=budget_s + 120)
+    if r.returncode != 0:
+        return {"label": "reference dsmc_cpu (2-D legacy)", "unavailable": (r.stderr or r.stdout).strip()[-200:]}
+    res = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"label": "reference dsmc_cpu (2-D legacy)", "value": res["value"],
+            "unit": "particle-timesteps/s", "cores": 1,
+            "sample": (f"{res['particles']} particles on the 30x18 2-D grid, {res['steps']} steps of "
+                       f"UpdateGridCPU + ComputeNanbuCPU + IntegrateCPU, {res['seconds']:.1f} s")}
+
+
 # ---------------------------------------------------------------- our arm ---
 
 def reduce_over_ranks(elapsed, count, world, device):
@@ -443,6 +465,9 @@ def run_ours(args, rank, world):
         v, cores, desc, *_ = cpu_oracle_sample(wl, budget_s=args.cpu_budget)
         out["cpu_baseline"] = {"value": v, "unit": "particle-timesteps/s", "cores": cores, "kind": "port",
                                "sample": desc}
+        legacy = legacy_cpu_sample()
+        if legacy is not None:
+            out["legacy_dsmc_cpu"] = legacy
     sol.close()
     return out
 
@@ -604,6 +629,9 @@ def run_reference(args):
                             "sample": desc},
            "e2e": {"value": v, "unit": "particle-timesteps/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
+    legacy = legacy_cpu_sample()
+    if legacy is not None:
+        out["legacy_dsmc_cpu"] = legacy
     return out
 
 
