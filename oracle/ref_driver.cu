@@ -303,4 +303,44 @@ int ref_step(float4* pos, float4* old_pos, float4* vel, float4* old_vel, uint* h
   return ref_status();
 }
 
+// DoBenchmark's loop of RunBenchmarkSimulationStep (include/gpu_dsmc.inl:220-274)
+// for `steps` steps, for timing the reference's kernels: before each step the
+// ping-pong buffers are swapped as particles.swap_* do, and every 100th step
+// ends with SampleCellStatistics.  pos[k]/vel[k] (k = 0, 1) are the two
+// buffers and `cur` the one that holds the state at the start; *cur_out is
+// the one that holds it at the end.  *ms is the device time of the loop from
+// CUDA events on the default stream, with one synchronisation at the end.
+int ref_run_steps(float4* pos0, float4* pos1, float4* vel0, float4* vel1, uint* hashes, uint* idx,
+                  uint2* cse, uint n, float dt, int collide, int geometry, int steps, int cur,
+                  int* cur_out, float* ms) {
+  float4* pos[2] = {pos0, pos1};
+  float4* vel[2] = {vel0, vel1};
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, 0);
+  for (int s = 1; s <= steps; ++s) {
+    const int old = cur;
+    cur = 1 - cur;
+    CalculateCellIDs(pos[old], hashes, idx, n);
+    SortParticlesIndices(hashes, idx, n);
+    cudaMemset(cse, 0, g_ref_settings.getCellsCount() * sizeof(uint2));
+    FindCellBoundaries(cse, pos[cur], vel[cur], 0, hashes, idx, pos[old], vel[old], 0, n, false);
+    if (collide) ComputeBird(vel[cur], cse, idx, g_ref_settings.partPerCell, dt, false);
+    if (geometry)
+      IntegrateAndProcessCollisions(pos[cur], vel[cur], 0, dt, g_ref_geom_hashes, n, false,
+                                    g_ref_settings.periodicCondition);
+    else
+      Integrate(pos[cur], vel[cur], 0, dt, n, false, g_ref_settings.periodicCondition);
+    if (s % 100 == 0) SampleCellStatistics(vel[cur], cse, idx, false);
+  }
+  cudaEventRecord(t1, 0);
+  cudaEventSynchronize(t1);
+  cudaEventElapsedTime(ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  *cur_out = cur;
+  return ref_status();
+}
+
 }  // extern "C"
