@@ -84,6 +84,78 @@ float orc_taus_float(uint32_t s[4]) {
   return (float)(2.3283064365387e-10 * (double)orc_taus_int(s));
 }
 
+/* Mersenne Twister variant of the reference's -mt path and of its initial
+ * fill (kernels/mtwister.cu, parameters include/MersenneTwister.h:31-40:
+ * 19-word state, middle word 9, one lower bit, tempering shifts 12/7/15/18).
+ * A twister's parameters are one 16-byte record of data/MersenneTwister.dat
+ * (matrix_a, mask_b, mask_c, seed); its state is
+ *   st[0] = iState, st[1] = mti1, st[2 .. 20] = mt[0 .. 18]
+ * as in mt_state (kernels/mtwister.cu:30-35). */
+#define ORC_MT_NN 19
+#define ORC_MT_MM 9
+
+/* lcg_rand, kernels/mtwister.cu:40-44 (unsigned long is 64 bits here). */
+uint32_t orc_mt_lcg(uint32_t a) { return (uint32_t)(((uint64_t)a * 279470273ull) % 4294967291ull); }
+
+/* The seed chain of InitGPUTwisters (kernels/mtwister.cu:46-68): twister i
+ * gets the (i+1)-th value of lcg_rand from `seed`, in cfg[4*i+3]. */
+void orc_mt_seed_chain(uint32_t seed, uint32_t* cfg, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++) {
+    seed = orc_mt_lcg(seed);
+    cfg[4 * i + 3] = seed;
+  }
+}
+
+/* InitTwisterFast, kernels/mtwister.cu:108-117. */
+void orc_mt_init(const uint32_t cfg[4], uint32_t st[21]) {
+  uint32_t* mt = st + 2;
+  mt[0] = cfg[3];
+  for (int i = 1; i < ORC_MT_NN; i++) mt[i] = 1812433253u * (mt[i - 1] ^ (mt[i - 1] >> 30)) + (uint32_t)i;
+  st[0] = 0;
+  st[1] = mt[0];
+}
+
+/* GetRandomIntegerFast, kernels/mtwister.cu:70-101: one word of the ring
+ * advanced per draw, then tempered. */
+uint32_t orc_mt_int(uint32_t st[21], const uint32_t cfg[4]) {
+  uint32_t* mt = st + 2;
+  int i1 = (int)st[0] + 1, im = (int)st[0] + ORC_MT_MM;
+  if (i1 >= ORC_MT_NN) i1 -= ORC_MT_NN;
+  if (im >= ORC_MT_NN) im -= ORC_MT_NN;
+  const uint32_t mti = st[1];
+  st[1] = mt[i1];
+  uint32_t x = (mti & 0xFFFFFFFEu) | (st[1] & 0x1u);
+  x = mt[im] ^ (x >> 1) ^ ((x & 1u) ? cfg[0] : 0u);
+  mt[st[0]] = x;
+  st[0] = (uint32_t)i1;
+  x ^= x >> 12;
+  x ^= (x << 7) & cfg[1];
+  x ^= (x << 15) & cfg[2];
+  x ^= x >> 18;
+  return x;
+}
+
+/* GetRandomFloatFast, kernels/mtwister.cu:103-106: float arithmetic. */
+float orc_mt_float(uint32_t st[21], const uint32_t cfg[4]) {
+  return ((float)orc_mt_int(st, cfg) + 1.0f) / 4294967296.0f;
+}
+
+/* The random source of one cell's collisions: HybridTaus (default) or the
+ * cell's twister (-mt). */
+typedef struct {
+  uint32_t* taus;
+  uint32_t* mt;
+  const uint32_t* cfg;
+} orc_cell_rng;
+
+static inline uint32_t cell_rng_int(orc_cell_rng* r) {
+  return r->mt ? orc_mt_int(r->mt, r->cfg) : orc_taus_int(r->taus);
+}
+
+static inline float cell_rng_float(orc_cell_rng* r) {
+  return r->mt ? orc_mt_float(r->mt, r->cfg) : orc_taus_float(r->taus);
+}
+
 /* Philox-4x32 with 10 rounds: each round multiplies words 0 and 2 by the
  * published constants, mixes high halves with words 1,3 and the key, and the
  * key advances by the Weyl increments between rounds. */
@@ -200,15 +272,15 @@ void orc_bounds_reorder(const orc_sim* s, uint32_t n, const uint32_t* keys, cons
 
 /* ------------------------------------------------------------- collide ---- */
 
-/* ComputeBirdCollisionsNoMTDev, kernels/dsmc_kernel.cu:912-1000 (one cell).
- * With omega != 0.5 the acceptance uses the VHS cross-section
- * sigma(g) = cross_section * (vhs_gref/g)^(2*omega-1). */
+/* ComputeBirdCollisionsNoMTDev, kernels/dsmc_kernel.cu:912-1000 (one cell),
+ * and ComputeBirdCollisionsDev (:1002-1089), the same steps with the cell's
+ * twister as the random source.  With omega != 0.5 the acceptance uses the
+ * VHS cross-section sigma(g) = cross_section * (vhs_gref/g)^(2*omega-1). */
 static void collide_cell(const orc_sim* s, float* vel4, uint32_t c, const uint32_t* cse,
-                         float* maxrem, float* stat4, uint32_t* seeds, float avg_conc, float dt) {
+                         float* maxrem, float* stat4, orc_cell_rng* rng, float avg_conc, float dt) {
   uint32_t st = cse[2 * c], en = cse[2 * c + 1];
   int part = (int)(en - st);
   if (part < 2) return;
-  uint32_t seed[4] = {seeds[4 * c], seeds[4 * c + 1], seeds[4 * c + 2], seeds[4 * c + 3]};
   float stat[4] = {stat4[4 * c], stat4[4 * c + 1], stat4[4 * c + 2], stat4[4 * c + 3]};
   float vmax_x = maxrem[2 * c], vmax_y = maxrem[2 * c + 1];
   /* (0.5*partCount*avgConc*fnum*vmax*dt)/cell_volume + rem, in double (:934). */
@@ -219,10 +291,10 @@ static void collide_cell(const orc_sim* s, float* vel4, uint32_t c, const uint32
   vmax_y = fpc - (float)pairs;
   const int hard_sphere = (s->omega == 0.5f);
   for (uint32_t i = 0; i < pairs; i++) {
-    uint32_t px = st + orc_taus_int(seed) % (uint32_t)part;
+    uint32_t px = st + cell_rng_int(rng) % (uint32_t)part;
     float v1[4];
     memcpy(v1, vel4 + 4 * (size_t)px, 16);
-    uint32_t py = st + orc_taus_int(seed) % (uint32_t)part;
+    uint32_t py = st + cell_rng_int(rng) % (uint32_t)part;
     float v2[4];
     memcpy(v2, vel4 + 4 * (size_t)py, 16);
     float mag = sqrtf(len2f(v1[0] - v2[0], v1[1] - v2[1], v1[2] - v2[2]));
@@ -231,12 +303,12 @@ static void collide_cell(const orc_sim* s, float* vel4, uint32_t c, const uint32
       v = mag * s->cross_section;
     else
       v = mag * (s->cross_section * powf(s->vhs_gref / mag, 2.0f * s->omega - 1.0f));
-    if (v / vmax_x > orc_taus_float(seed)) {
+    if (v / vmax_x > cell_rng_float(rng)) {
       stat[1] += 1.0f;
       stat[2] += mag;
-      float b = 2.0f * orc_taus_float(seed) - 1.0f;
+      float b = 2.0f * cell_rng_float(rng) - 1.0f;
       float a = sqrtf(fmaf(-b, b, 1.0f));
-      float cc = 2 * ORC_PI_F * orc_taus_float(seed);
+      float cc = 2 * ORC_PI_F * cell_rng_float(rng);
       float ax = b * mag / 2.0f;
       float ay = a * mag * cosf(cc) / 2.0f;
       float az = a * mag * sinf(cc) / 2.0f;
@@ -254,15 +326,39 @@ static void collide_cell(const orc_sim* s, float* vel4, uint32_t c, const uint32
   maxrem[2 * c] = vmax_x;
   maxrem[2 * c + 1] = vmax_y;
   memcpy(stat4 + 4 * c, stat, 16);
-  memcpy(seeds + 4 * c, seed, 16);
 }
 
 void orc_collide(const orc_sim* s, float* vel4, const uint32_t* cse, float* maxrem, float* stat4,
                  uint32_t* seeds, float avg_conc, float dt) {
   long c;
 #pragma omp parallel for schedule(dynamic, 256)
-  for (c = 0; c < (long)s->cells; c++)
-    collide_cell(s, vel4, (uint32_t)c, cse, maxrem, stat4, seeds, avg_conc, dt);
+  for (c = 0; c < (long)s->cells; c++) {
+    orc_cell_rng r = {seeds + 4 * c, NULL, NULL};
+    collide_cell(s, vel4, (uint32_t)c, cse, maxrem, stat4, &r, avg_conc, dt);
+  }
+}
+
+/* The -mt collisions: cell c draws from twister c (state mt_state[21*c],
+ * parameters mt_cfg[4*c]), as ComputeBirdCollisionsDev does
+ * (kernels/dsmc_kernel.cu:1002-1089). */
+void orc_collide_mt(const orc_sim* s, float* vel4, const uint32_t* cse, float* maxrem, float* stat4,
+                    uint32_t* mt_state, const uint32_t* mt_cfg, float avg_conc, float dt) {
+  long c;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (c = 0; c < (long)s->cells; c++) {
+    orc_cell_rng r = {NULL, mt_state + 21 * c, mt_cfg + 4 * c};
+    collide_cell(s, vel4, (uint32_t)c, cse, maxrem, stat4, &r, avg_conc, dt);
+  }
+}
+
+/* InitMaximums, kernels/dsmc_kernel.cu:1104-1120: (sigma g)max from the
+ * settings and the remainder from one draw of the cell's twister. */
+void orc_init_maximums_mt(uint32_t cells, float max_rel_vel, uint32_t* mt_state,
+                          const uint32_t* mt_cfg, float* maxrem) {
+  for (uint32_t c = 0; c < cells; c++) {
+    maxrem[2 * c] = max_rel_vel;
+    maxrem[2 * c + 1] = orc_mt_float(mt_state + 21 * (size_t)c, mt_cfg + 4 * (size_t)c);
+  }
 }
 
 /* ---------------------------------------------------------------- move ---- */

@@ -53,6 +53,15 @@ typedef struct {
 uint32_t orc_taus_int(uint32_t s[4]);
 float orc_taus_float(uint32_t s[4]);
 
+/* Mersenne Twister variant of the -mt path (kernels/mtwister.cu:40-117):
+ * cfg = one 16-byte twister record (matrix_a, mask_b, mask_c, seed), st = 21
+ * words (iState, mti1, mt[19]). */
+uint32_t orc_mt_lcg(uint32_t a);
+void orc_mt_seed_chain(uint32_t seed, uint32_t* cfg, uint32_t n);
+void orc_mt_init(const uint32_t cfg[4], uint32_t st[21]);
+uint32_t orc_mt_int(uint32_t st[21], const uint32_t cfg[4]);
+float orc_mt_float(uint32_t st[21], const uint32_t cfg[4]);
+
 /* Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11). */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 
@@ -63,6 +72,13 @@ void orc_bounds_reorder(const orc_sim* s, uint32_t n, const uint32_t* keys, cons
                         uint32_t* cse);
 void orc_collide(const orc_sim* s, float* vel4, const uint32_t* cse, float* maxrem, float* stat4,
                  uint32_t* seeds, float avg_conc, float dt);
+/* ComputeBirdCollisionsDev (the -mt collisions, kernels/dsmc_kernel.cu:1002-1089):
+ * twister c per cell, 21 state words and 4 parameter words each. */
+void orc_collide_mt(const orc_sim* s, float* vel4, const uint32_t* cse, float* maxrem, float* stat4,
+                    uint32_t* mt_state, const uint32_t* mt_cfg, float avg_conc, float dt);
+/* InitMaximums (kernels/dsmc_kernel.cu:1104-1120). */
+void orc_init_maximums_mt(uint32_t cells, float max_rel_vel, uint32_t* mt_state,
+                          const uint32_t* mt_cfg, float* maxrem);
 void orc_move(const orc_sim* s, const orc_geom* g, float* pos4, float* vel4, uint32_t n, float dt);
 void orc_sample(const orc_sim* s, const float* vel4, const uint32_t* cse, float* cell_stats7);
 void orc_sample_f64(const orc_sim* s, const float* vel4, const uint32_t* cse, double* acc5);

@@ -1,5 +1,6 @@
-"""ctypes binding of the CPU oracle (liboracle.so) and of the reference's own
-kernels built headless (_ref/libdsmc_ref.so).
+"""ctypes binding of the CPU oracle (liboracle.so), of the reference's own
+kernels built headless (_ref/libdsmc_ref.so) and of the reference's twister
+code (_ref/libmt_ref.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
 bench.py's CPU-baseline leg, never by the product package.
@@ -64,6 +65,10 @@ def orc():
         L.orc_build_grid.restype = ctypes.c_long
         L.orc_tri_box_overlap.restype = ctypes.c_int
         L.orc_get_threads.restype = ctypes.c_int
+        L.orc_mt_lcg.restype = ctypes.c_uint32
+        L.orc_mt_lcg.argtypes = [ctypes.c_uint32]
+        L.orc_mt_int.restype = ctypes.c_uint32
+        L.orc_mt_float.restype = ctypes.c_float
         _orc = L
     return _orc
 
@@ -85,6 +90,66 @@ def ref():
         L.ref_build_grid.restype = ctypes.c_long
         _ref = L
     return _ref
+
+
+MT_REF_SO = os.path.join(HERE, "_ref", "libmt_ref.so")
+MT_DAT = os.path.join(HERE, "_ref", "MersenneTwister.dat")
+
+
+def mt_ref_available():
+    return os.path.exists(MT_REF_SO) and os.path.exists(MT_DAT)
+
+
+class MtStruct(ctypes.Structure):
+    """mt_struct of the reference's include/dci.h (the CPU twister)."""
+    _fields_ = [("aaa", ctypes.c_uint32), ("mm", ctypes.c_int), ("nn", ctypes.c_int),
+                ("rr", ctypes.c_int), ("ww", ctypes.c_int), ("wmask", ctypes.c_uint32),
+                ("umask", ctypes.c_uint32), ("lmask", ctypes.c_uint32), ("shift0", ctypes.c_int),
+                ("shift1", ctypes.c_int), ("shiftB", ctypes.c_int), ("shiftC", ctypes.c_int),
+                ("maskB", ctypes.c_uint32), ("maskC", ctypes.c_uint32), ("i", ctypes.c_int),
+                ("state", ctypes.POINTER(ctypes.c_uint32))]
+
+
+_mt_ref = None
+
+
+def mt_ref():
+    """The reference's twister code built unchanged (src/genmtrand.c and the
+    host function lcg_rand of kernels/mtwister.cu)."""
+    global _mt_ref
+    if _mt_ref is None:
+        if not os.path.exists(MT_REF_SO):
+            raise FileNotFoundError(MT_REF_SO)
+        L = ctypes.CDLL(MT_REF_SO)
+        L.genrand_mt.restype = ctypes.c_uint32
+        L.genrand_mt.argtypes = [ctypes.POINTER(MtStruct)]
+        L.sgenrand_mt.restype = None
+        L.sgenrand_mt.argtypes = [ctypes.c_uint32, ctypes.POINTER(MtStruct)]
+        lcg = getattr(L, "_Z8lcg_randm")  # unsigned long lcg_rand(unsigned long)
+        lcg.restype = ctypes.c_ulong
+        lcg.argtypes = [ctypes.c_ulong]
+        L.lcg_rand = lcg
+        _mt_ref = L
+    return _mt_ref
+
+
+def mt_records(path=MT_DAT):
+    """The twister records of data/MersenneTwister.dat, (count, 4) uint32:
+    matrix_a, mask_b, mask_c, seed (include/MersenneTwister.h:22-27)."""
+    return np.fromfile(path, dtype=np.uint32).reshape(-1, 4)
+
+
+def mt_draws(cfg, count):
+    """`count` draws of one twister through the oracle (InitTwisterFast, then
+    GetRandomIntegerFast); cfg holds its 4 parameter words."""
+    L = orc()
+    cfg = np.ascontiguousarray(cfg, dtype=np.uint32)
+    st = np.zeros(21, np.uint32)
+    L.orc_mt_init(p(cfg), p(st))
+    out = np.empty(count, np.uint32)
+    for k in range(count):
+        out[k] = L.orc_mt_int(p(st), p(cfg))
+    return out, st
 
 
 def sim_from(cfg_grid_min, cfg_grid_max, dim, fnum, cross_section, periodic="n", omega=0.5,
@@ -164,6 +229,24 @@ def collide(sim, vel4, cse, maxrem, stat4, seeds, avg_conc, dt):
     """In place on vel4, maxrem, stat4, seeds (numpy arrays)."""
     orc().orc_collide(ctypes.byref(sim), p(vel4), p(cse), p(maxrem), p(stat4), p(seeds),
                       ctypes.c_float(avg_conc), ctypes.c_float(dt))
+
+
+def collide_mt(sim, vel4, cse, maxrem, stat4, mt_state, mt_cfg, avg_conc, dt):
+    """The -mt collisions (ComputeBirdCollisionsDev), in place on vel4,
+    maxrem, stat4 and mt_state ((cells, 21) uint32); mt_cfg is (cells, 4)."""
+    orc().orc_collide_mt(ctypes.byref(sim), p(vel4), p(cse), p(maxrem), p(stat4), p(mt_state),
+                         p(np.ascontiguousarray(mt_cfg, np.uint32)), ctypes.c_float(avg_conc),
+                         ctypes.c_float(dt))
+
+
+def mt_states(mt_cfg):
+    """InitTwisterFast for every twister of mt_cfg ((count, 4) uint32)."""
+    cfg = np.ascontiguousarray(mt_cfg, np.uint32)
+    st = np.zeros((cfg.shape[0], 21), np.uint32)
+    L = orc()
+    for k in range(cfg.shape[0]):
+        L.orc_mt_init(p(cfg[k]), p(st[k]))
+    return st
 
 
 def geom_from(bbox, cell, dim, count, tri_ids, flags, verts, tris, normals):
