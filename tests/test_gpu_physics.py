@@ -39,7 +39,7 @@ def test_energy_conserved(cuda, rng, density):
     sol.close()
 
 
-@pytest.mark.parametrize("rng", ["taus", "philox"])
+    # the closed-box relaxation case: argon VHS, 200 K + 600 K halves, 16^3 cells, 100k particles
 def test_bimodal_relaxes_to_maxwellian(cuda, rng):
     # configs[0] of the workload list: argon VHS, 200 K + 600 K halves, 16^3 cells
     sol, n = box(1e20, rng=rng, omega=0.81, init="bimodal", temp=200.0, t2=600.0)
