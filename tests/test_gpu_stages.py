@@ -55,7 +55,7 @@ def test_cell_index_bit_exact(cuda, n):
 
 
 @pytest.mark.parametrize("n,nkeys,mode", [
-    (1, 1, "rand"), (2, 7, "rand"), (100000, 4096, "rand"), (131072, 65536, "rand"),
+    (0, 5, "rand"), (1, 1, "rand"), (2, 7, "rand"), (100000, 4096, "rand"), (131072, 65536, "rand"),
     (50000, 2048, "same"), (20000, 300, "nearly"), (70000, 10, "rand")])
 def test_sort_stable_bit_exact(cuda, n, nkeys, mode):
     rng = np.random.default_rng(n + nkeys)
