@@ -122,6 +122,28 @@ int ref_derived(unsigned* part_per_cell, float* cell_volume, float* cross_sectio
   return 0;
 }
 
+// settings_t::readFromFile (src/sim_settings.cpp:46-132) on `path`, with the
+// gas file opened relative to the working directory as the reference does.
+// f: grid min (3), max (3), density, fnum, temp, stream velocity (3), gas
+// mass, diameter, T_ref, cell size (3); i: grid dims (3), periodic character.
+// Host code only: no device work.
+int ref_read_settings(const char* path, float f[18], int i[4]) {
+  settings_t s;
+  s.readFromFile(path);
+  const float v[18] = {s.boundaries.min.x, s.boundaries.min.y, s.boundaries.min.z,
+                       s.boundaries.max.x, s.boundaries.max.y, s.boundaries.max.z,
+                       s.density, s.fnum, s.temp,
+                       s.streamVelocity.x, s.streamVelocity.y, s.streamVelocity.z,
+                       s.gas.molmass, s.gas.diameter, s.gas.Tref,
+                       s.cell_size.x, s.cell_size.y, s.cell_size.z};
+  std::memcpy(f, v, sizeof(v));
+  i[0] = s.grid_dim.x;
+  i[1] = s.grid_dim.y;
+  i[2] = s.grid_dim.z;
+  i[3] = s.periodicCondition;
+  return 0;
+}
+
 int ref_set_cell_state(const float* maxrem, const unsigned* seeds) {
   const uint cells = g_ref_settings.getCellsCount();
   if (maxrem) cudaMemcpy(maximums, maxrem, cells * sizeof(float2), cudaMemcpyHostToDevice);

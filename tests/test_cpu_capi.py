@@ -120,6 +120,28 @@ def test_reads_the_reference_configs(name):
     assert s.getCellsCount() in (9720, 32768)
 
 
+@pytest.mark.skipif(not (os.path.exists(REF) and O.ref_available()),
+                    reason="reference checkout or oracle/_ref not present")
+@pytest.mark.parametrize("name", ["config.xml", "config_500k.xml", "config_mln.xml"])
+def test_config_parse_matches_reference_parser(name, monkeypatch):
+    """Every value the reference's own settings_t::readFromFile
+    (src/sim_settings.cpp:46-132, built unchanged into oracle/_ref) reads from
+    its configuration and gas files, bit for bit; and the oracle's FP32 cell
+    size (InitSimulationProperties) equal to the reference's."""
+    s = cb.settings_t().readFromFile(os.path.join(REF, "data", name)).cfg
+    f = np.zeros(18, np.float32)
+    i = np.zeros(4, np.int32)
+    monkeypatch.chdir(REF)  # the reference opens the gas file relative to the working directory
+    assert O.ref().ref_read_settings(os.path.join("data", name).encode(), O.p(f), O.p(i)) == 0
+    ours = np.array(list(s.grid_min) + list(s.grid_max) + [s.density, s.fnum, s.temp] +
+                    list(s.stream_vel) + [s.gas_mass, s.gas_diam, s.gas_tref], np.float32)
+    assert np.array_equal(ours, f[:15])
+    assert list(s.grid_dim) == list(i[:3])
+    assert s.periodic == bytes([i[3]])
+    sim = O.sim_from(s.grid_min, s.grid_max, s.grid_dim, s.fnum, O.cross_section_of(s.gas_diam))
+    assert np.array_equal(np.array(sim.cell[:], np.float32), f[15:18])
+
+
 @pytest.mark.parametrize("level", [0, 1, 3])
 def test_icosphere(level):
     v, t = cb.mesh_icosphere(level, 0.1, (0.3, 0.3, 0.3))
