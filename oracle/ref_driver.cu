@@ -127,9 +127,7 @@ int ref_derived(unsigned* part_per_cell, float* cell_volume, float* cross_sectio
 // f: grid min (3), max (3), density, fnum, temp, stream velocity (3), gas
 // mass, diameter, T_ref, cell size (3); i: grid dims (3), periodic character.
 // Host code only: no device work.
-int ref_read_settings(const char* path, float f[18], int i[4]) {
-  settings_t s;
-  s.readFromFile(path);
+static void ref_settings_out(const settings_t& s, float* f, int* i) {
   const float v[18] = {s.boundaries.min.x, s.boundaries.min.y, s.boundaries.min.z,
                        s.boundaries.max.x, s.boundaries.max.y, s.boundaries.max.z,
                        s.density, s.fnum, s.temp,
@@ -141,6 +139,29 @@ int ref_read_settings(const char* path, float f[18], int i[4]) {
   i[1] = s.grid_dim.y;
   i[2] = s.grid_dim.z;
   i[3] = s.periodicCondition;
+}
+
+int ref_read_settings(const char* path, float f[18], int i[4]) {
+  settings_t s;
+  s.readFromFile(path);
+  ref_settings_out(s, f, i);
+  return 0;
+}
+
+// settings_t() then settings_t::readFromCmdLine (src/sim_settings.cpp:34-44,
+// 134-186) on argv.  f: the 18 values of ref_read_settings, then dt and the
+// run time; i: grid dims, periodic character, then benchmark, geometry, mt,
+// cpu.  Host code only.
+int ref_read_cmdline(int argc, char** argv, float f[20], int i[8]) {
+  settings_t s;
+  s.readFromCmdLine(argc, argv);
+  ref_settings_out(s, f, i);
+  f[18] = s.dt;
+  f[19] = s.maxRunTime;
+  i[4] = s.benchmark;
+  i[5] = s.geometry;
+  i[6] = s.mt;
+  i[7] = s.cpu;
   return 0;
 }
 

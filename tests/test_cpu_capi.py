@@ -142,6 +142,48 @@ def test_config_parse_matches_reference_parser(name, monkeypatch):
     assert np.array_equal(np.array(sim.cell[:], np.float32), f[15:18])
 
 
+@pytest.mark.skipif(not (os.path.exists(REF) and O.ref_available()),
+                    reason="reference checkout or oracle/_ref not present")
+@pytest.mark.parametrize("args", [
+    [],
+    ["-benchmark", "-no-geometry", "-density", "3e20", "-dt", "2.5e-6", "-run-for", "0.01"],
+    ["-f", "data/config_500k.xml", "-density", "7.3e19", "-benchmark"],
+    ["-density", "1e21", "-f", "data/config.xml", "-dt", "1e-5"],
+])
+def test_command_line_matches_reference_parser(args, monkeypatch):
+    """settings_t() and settings_t::readFromCmdLine (src/sim_settings.cpp:34-44,
+    134-186) of the reference, built unchanged, against this library's
+    command-line parse: defaults, flags in order, a -f file read where it
+    appears (later flags override it, earlier ones are overwritten)."""
+    monkeypatch.chdir(REF)
+    argv = ["prog"] + args
+    s = cb.settings_t().readFromCmdLine(argv)
+    c = s.cfg
+    f = np.zeros(20, np.float32)
+    i = np.zeros(8, np.int32)
+    arr = (ctypes.c_char_p * len(argv))(*[a.encode() for a in argv])
+    assert O.ref().ref_read_cmdline(len(argv), arr, O.p(f), O.p(i)) == 0
+    ours = np.array(list(c.grid_min) + list(c.grid_max) + [c.density, c.fnum, c.temp] +
+                    list(c.stream_vel), np.float32)
+    assert np.array_equal(ours, f[:12])
+    if any(a == "-f" for a in args):  # the gas is read from the file only
+        assert np.array_equal(np.array([c.gas_mass, c.gas_diam, c.gas_tref], np.float32), f[12:15])
+    assert list(c.grid_dim) == list(i[:3]) and c.periodic == bytes([i[3]])
+    assert np.float32(c.dt) == f[18] and np.float32(s.maxRunTime) == f[19]
+    # the flags set the same values; two defaults differ by design: there is
+    # no viewer to run instead of the benchmark loop, and mesh collisions are
+    # off until a mesh is set (the reference's main loads its built-in model)
+    if "-benchmark" in args:
+        assert c.benchmark == 1 and i[4] == 1
+    else:
+        assert c.benchmark == 1 and i[4] == 0
+    if "-no-geometry" in args:
+        assert c.geometry == 0 and i[5] == 0
+    else:
+        assert c.geometry == 0 and i[5] == 1
+    assert i[6] == 0 and i[7] == 0  # -mt and -cpu are not given
+
+
 @pytest.mark.parametrize("level", [0, 1, 3])
 def test_icosphere(level):
     v, t = cb.mesh_icosphere(level, 0.1, (0.3, 0.3, 0.3))
