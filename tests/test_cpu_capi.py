@@ -149,6 +149,7 @@ def test_config_parse_matches_reference_parser(name, monkeypatch):
     ["-benchmark", "-no-geometry", "-density", "3e20", "-dt", "2.5e-6", "-run-for", "0.01"],
     ["-f", "data/config_500k.xml", "-density", "7.3e19", "-benchmark"],
     ["-density", "1e21", "-f", "data/config.xml", "-dt", "1e-5"],
+    ["-cpu", "-run-for", "2.5", "-dt", "3.3e-6"],
 ])
 def test_command_line_matches_reference_parser(args, monkeypatch):
     """settings_t() and settings_t::readFromCmdLine (src/sim_settings.cpp:34-44,
@@ -181,7 +182,8 @@ def test_command_line_matches_reference_parser(args, monkeypatch):
         assert c.geometry == 0 and i[5] == 0
     else:
         assert c.geometry == 0 and i[5] == 1
-    assert i[6] == 0 and i[7] == 0  # -mt and -cpu are not given
+    assert i[6] == 0  # -mt is refused here (no GPU mode), so it is never given
+    assert i[7] == int("-cpu" in args)  # parsed and never read by the reference; ignored here
 
 
 @pytest.mark.parametrize("level", [0, 1, 3])
