@@ -165,6 +165,32 @@ int ref_read_cmdline(int argc, char** argv, float f[20], int i[8]) {
   return 0;
 }
 
+// The -mt twisters as GPUDSMCSolver::Init sets them up
+// (include/gpu_dsmc.inl:346-368): InitGPUTwisters on the parameter file at
+// `path` with `seed` (kernels/mtwister.cu:46-68), then InitMersenneTwisters
+// (kernels/dsmc_kernel.cu:548-569).
+int ref_mt_init(const char* path, unsigned seed) {
+  InitGPUTwisters(path, seed);
+  InitMersenneTwisters();
+  return ref_status();
+}
+
+// The first `count` twisters: parameters (matrix_a, mask_b, mask_c, seed)
+// and states (iState, mti1, mt[19]), either pointer may be null.
+int ref_mt_get(unsigned count, unsigned* cfg4, unsigned* state21) {
+  if (count > MT_RNG_COUNT) return -1;
+  if (cfg4) cudaMemcpyFromSymbol(cfg4, ds_MT, count * sizeof(mt_struct_stripped));
+  if (state21) cudaMemcpyFromSymbol(state21, ds_mtState, count * sizeof(mt_state));
+  return ref_status();
+}
+
+// ComputeBird with mt = true: ComputeBirdCollisionsDev
+// (kernels/dsmc_kernel.cu:1002-1089), cell c drawing from twister c.
+int ref_collide_mt(float4* vel, const uint2* cse, uint avg_conc, float dt) {
+  ComputeBird(vel, cse, 0, avg_conc, dt, true);
+  return ref_status();
+}
+
 int ref_set_cell_state(const float* maxrem, const unsigned* seeds) {
   const uint cells = g_ref_settings.getCellsCount();
   if (maxrem) cudaMemcpy(maximums, maxrem, cells * sizeof(float2), cudaMemcpyHostToDevice);

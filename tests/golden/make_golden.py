@@ -4,6 +4,7 @@ oracle/_ref/libdsmc_ref.so, needs a GPU) and its host geometry code.
 
 Usage (on a machine with a GPU and oracle/_ref built):
     python tests/golden/make_golden.py [OUTDIR]
+    python tests/golden/make_golden.py --only collide_mt [OUTDIR]
 
 Every fixture stores its seeded inputs and the reference's outputs; the CPU
 tests check the oracle against them (tests/test_cpu_oracle_golden.py).
@@ -193,5 +194,57 @@ def main(out):
     print("golden fixtures written to", out)
 
 
+def collide_mt(out):
+    """The -mt collisions (ComputeBirdCollisionsDev) on the case of
+    collide.npz, with the reference's twisters set up as its solver does:
+    data/MersenneTwister.dat (copied to oracle/_ref by `make -C oracle ref`)
+    and seed 999 (SEED, include/MersenneTwister.h:17)."""
+    os.makedirs(out, exist_ok=True)
+    R = O.ref()
+    dev = torch.device("cuda:0")
+    gmin, gmax, dim = (0.0, 0.0, 0.0), (0.8, 0.4, 0.4), (8, 4, 4)
+    mass, diam, tref, temp = 6.63e-26, 4.17e-10, 273.0, 300.0
+    d = ref_init(R, gmin, gmax, dim, 1e20, 1e15, temp, mass, diam, tref, "n")
+    n = 128 * 10
+    pos, vel = box_case(3, dim, gmin, gmax, n, vstd=400.0)
+    sim = O.sim_from(gmin, gmax, dim, 1e15, d["cross_section"])
+    k, i = O.cell_ids(sim, pos)
+    k, i = O.sort(k, i, sim.cells)
+    cse, sp, sv = O.bounds_reorder(sim, k, i, pos, vel)
+    mr = maxrem_init(5, 128, d["max_rel_vel"])
+    assert R.ref_mt_init(O.MT_DAT.encode(), 999) == 0
+    cfg = np.zeros((128, 4), np.uint32)
+    st0 = np.zeros((128, 21), np.uint32)
+    assert R.ref_mt_get(128, O.p(cfg), O.p(st0)) == 0
+    assert R.ref_set_cell_state(O.p(mr), None) == 0
+    assert R.ref_clear_stats() == 0
+    v_t = torch.from_numpy(sv.copy()).to(dev)
+    c_t = torch.from_numpy(cse.view(np.int32).copy()).to(dev)
+    dt = 4e-5
+    assert R.ref_collide_mt(P(v_t), P(c_t), 10, ctypes.c_float(dt)) == 0
+    st1 = np.zeros_like(st0)
+    assert R.ref_mt_get(128, None, O.p(st1)) == 0
+    mr_o = np.zeros_like(mr)
+    st4 = np.zeros((128, 4), np.float32)
+    R.ref_get_cell_state(O.p(mr_o), None, O.p(st4), None)
+    np.savez_compressed(os.path.join(out, "collide_mt.npz"), gmin=gmin, gmax=gmax, dim=dim, dt=dt,
+                        avg_conc=10.0, fnum=1e15, cross_section=d["cross_section"],
+                        cell_volume=d["cell_volume"], vel=sv, cse=cse, maxrem=mr, mt_cfg=cfg,
+                        mt_state=st0, vel_out=v_t.cpu().numpy(), maxrem_out=mr_o,
+                        mt_state_out=st1, stat4=st4)
+    print("collide_mt.npz written to", out)
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))
+    # make_golden.py [--only collide_mt] [OUTDIR]
+    args = sys.argv[1:]
+    only = None
+    if args[:1] == ["--only"]:
+        only, args = args[1], args[2:]
+    outdir = args[0] if args else os.path.dirname(os.path.abspath(__file__))
+    if only in (None, "collide_mt"):
+        if only is None:
+            main(outdir)
+        collide_mt(outdir)
+    else:
+        raise SystemExit(f"unknown fixture {only}")

@@ -13,6 +13,7 @@ one, which the golden vectors pin; here it is checked for conservation and
 for drawing exactly what the reference's loop draws.
 """
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -156,3 +157,34 @@ def test_init_maximums_draws_one_float_per_cell():
         u, s1 = O.mt_draws(cfg[c], 1)
         assert mr[c, 1] == (np.float32(u[0]) + np.float32(1.0)) / np.float32(4294967296.0)
         assert np.array_equal(s1, st[c])
+
+
+GOLDEN_MT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "collide_mt.npz")
+
+
+@pytest.mark.skipif(not os.path.exists(GOLDEN_MT),
+                    reason="collide_mt.npz is made on a GPU by tests/golden/make_golden.py --only collide_mt")
+def test_mt_collide_matches_reference_fixture():
+    """The reference's own -mt kernel on the collide.npz case: its twister set-up
+    (InitGPUTwisters seed chain, InitTwisterFast), and after ComputeBirdCollisionsDev
+    the twister states, counts and remainders bit-exact, velocities within 2e-6 of
+    the thermal scale (libm cosf/sinf here, __cosf/__sinf there)."""
+    d = np.load(GOLDEN_MT)
+    cfg = d["mt_cfg"]
+    chain = np.zeros((cfg.shape[0], 4), np.uint32)
+    O.orc().orc_mt_seed_chain(999, O.p(chain), cfg.shape[0])
+    assert np.array_equal(cfg[:, 3], chain[:, 3])
+    if O.mt_ref_available():
+        assert np.array_equal(cfg[:, :3], O.mt_records()[: cfg.shape[0], :3])
+    assert np.array_equal(O.mt_states(cfg), d["mt_state"])
+    sim = O.sim_from(d["gmin"], d["gmax"], d["dim"], float(d["fnum"]), float(d["cross_section"]))
+    vel = d["vel"].copy()
+    mr = d["maxrem"].copy()
+    st = d["mt_state"].copy()
+    st4 = np.zeros((sim.cells, 4), np.float32)
+    O.collide_mt(sim, vel, d["cse"], mr, st4, st, cfg, float(d["avg_conc"]), float(d["dt"]))
+    assert np.array_equal(st, d["mt_state_out"])
+    assert np.array_equal(st4[:, :2], d["stat4"][:, :2])
+    assert np.array_equal(mr[:, 1], d["maxrem_out"][:, 1])
+    assert np.allclose(mr[:, 0], d["maxrem_out"][:, 0], rtol=1e-6)
+    assert np.max(np.abs(vel[:, :3] - d["vel_out"][:, :3])) / (3 * 400.0) <= 2e-6
