@@ -13,6 +13,11 @@ cross-rank traffic is the reduction of the timings).
 
 --impl reference times the CPU restatement of the reference's step (oracle/,
 OpenMP over all host cores) on a bounded sample of the same workload.
+
+Both arms also report, under `legacy_dsmc_cpu`, the reference's own legacy
+2-D CPU solver (src/dsmc_cpu.cpp on its compile-time 30 x 18 grid, single
+thread) when oracle/_ref/dsmc_cpu_legacy is built: the only CPU solver the
+reference ships, reported beside the port, not in place of it.
 """
 import argparse
 import ctypes
