@@ -28,3 +28,23 @@ def cuda():
     assert torch.cuda.is_available(), "GPU tests need a CUDA device"
     torch.cuda.init()
     return torch.device("cuda:0")
+
+
+def pytest_collection_finish(session):
+    """With DSMC_CHECK_FIXTURES=1, fail collection when a test asks for an
+    argument that is neither a fixture nor a parameter (such a test would only
+    error at setup, on the GPU box)."""
+    if os.environ.get("DSMC_CHECK_FIXTURES") != "1":
+        return
+    missing = []
+    for item in session.items:
+        fi = getattr(item, "_fixtureinfo", None)
+        if fi is None:
+            continue
+        params = getattr(getattr(item, "callspec", None), "params", {})
+        for name in fi.names_closure:
+            if name == "request" or name in params or fi.name2fixturedefs.get(name):
+                continue
+            missing.append(f"{item.nodeid}: {name}")
+    if missing:
+        raise pytest.UsageError("unresolved test arguments:\n" + "\n".join(missing))

@@ -14,7 +14,8 @@ from cudadsmc_b200 import _capi
 from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+# the reference checkout, when the environment names one (tests that read it skip otherwise)
+REF = os.environ.get("DSMC_REFERENCE_DIR", "")
 
 
 def declared_functions():

@@ -39,9 +39,9 @@ def test_energy_conserved(cuda, rng, density):
     sol.close()
 
 
-    # the closed-box relaxation case: argon VHS, 200 K + 600 K halves, 16^3 cells, 100k particles
+@pytest.mark.parametrize("rng", ["taus", "philox"])
 def test_bimodal_relaxes_to_maxwellian(cuda, rng):
-    # configs[0] of the workload list: argon VHS, 200 K + 600 K halves, 16^3 cells
+    # the closed-box relaxation case: argon VHS, 200 K + 600 K halves, 16^3 cells, 100k particles
     sol, n = box(1e20, rng=rng, omega=0.81, init="bimodal", temp=200.0, t2=600.0)
     # n V / F_N = 24.41 per cell: the extension starts fill the fraction too
     assert abs(n - 100000) < 300
