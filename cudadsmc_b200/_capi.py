@@ -110,6 +110,7 @@ SIGNATURES = [
     ("dsmc_init_state", _I, [_P, _P, ctypes.POINTER(_U32)]),
     ("dsmc_upload_state", _I, [_P, _P, _P, _U32, _I]),
     ("dsmc_download_state", _I, [_P, _P, _P, ctypes.POINTER(_U32), _I]),
+    ("dsmc_read_keys", _I, [_P, _P, ctypes.POINTER(_U32)]),
     ("dsmc_set_cell_state", _I, [_P, _P, _P]),
     ("dsmc_get_cell_state", _I, [_P, _P, _P]),
     ("dsmc_step", _I, [_P, ctypes.c_float, _I]),

@@ -185,6 +185,18 @@ float vhs_gref_of(const dsmc_config& c) {
   return (float)(g0 * std::pow(std::tgamma(2.5 - w), -1.0 / (2.0 * w - 1.0)));
 }
 
+// The Philox mode's VHS coefficients: sigma(g) g = vhs_k 2^(vhs_c1 log2 g),
+// vhs_c1 = 2 - 2 omega, vhs_k = sigma_ref g_ref^(2 omega - 1), evaluated in
+// double and rounded once.
+void set_vhs_fast(dsmcb::StepParams& p, float cross_section, float omega, float gref) {
+  p.vhs_k = 0.f;
+  p.vhs_c1 = 0.f;
+  if (p.hard_sphere || !(gref > 0.f) || !(cross_section > 0.f)) return;
+  const double e = 2.0 * (double)omega - 1.0;
+  p.vhs_c1 = (float)(1.0 - e);
+  p.vhs_k = (float)((double)cross_section * std::pow((double)gref, e));
+}
+
 dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
   dsmcb::StepParams p{};
   p.grid = h->grid;
@@ -199,11 +211,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
   p.hard_sphere = std::fabs(h->cfg.gas_omega - 0.5f) < 1e-9f;
   p.vhs_exp = 2.f * h->cfg.gas_omega - 1.f;
   p.vhs_gref = h->vhs_gref;
-  if (!p.hard_sphere && h->vhs_gref > 0.f && h->cross_section > 0.f) {
-    const double e = 2.0 * (double)h->cfg.gas_omega - 1.0;
-    p.vhs_c1 = (float)(1.0 - e);
-    p.vhs_c0 = (float)(std::log2((double)h->cross_section) + e * std::log2((double)h->vhs_gref));
-  }
+  set_vhs_fast(p, h->cross_section, h->cfg.gas_omega, h->vhs_gref);
   p.ntc_local = h->cfg.ntc_local;
   p.rng_kind = h->cfg.rng;
   p.seed = make_uint2((uint32_t)h->cfg.seed, (uint32_t)(h->cfg.seed >> 32));
@@ -1146,6 +1154,20 @@ int dsmc_download_state(dsmc_handle* h, float* pos, float* vel, uint32_t* n_io, 
   return DSMC_OK;
 }
 
+int dsmc_read_keys(dsmc_handle* h, uint32_t* keys, uint32_t* n_io) {
+  if (!h || !n_io) return fail(h, DSMC_ERR_ARG, "null argument");
+  Meta m{};
+  int st = read_meta(h, m);
+  if (st) return st;
+  const uint32_t n = h->has_state ? m.n_alive + m.n_pending : 0;
+  const uint32_t cap = *n_io;
+  *n_io = n;
+  if (!keys) return DSMC_OK;
+  if (cap < n) return fail(h, DSMC_ERR_ARG, "output buffer too small");
+  CK(h, cudaMemcpy(keys, h->keys, (size_t)n * 4, cudaMemcpyDeviceToHost), "download keys");
+  return DSMC_OK;
+}
+
 int dsmc_set_cell_state(dsmc_handle* h, const float* maxrem, const uint32_t* seeds) {
   if (!h) return DSMC_ERR_ARG;
   if (maxrem)
@@ -1610,6 +1632,7 @@ int dsmc_stage_collide(const dsmc_collide_params* cp, float* u, float* v, float*
   p.hard_sphere = std::fabs(cp->omega - 0.5f) < 1e-9f;
   p.vhs_exp = 2.f * cp->omega - 1.f;
   p.vhs_gref = cp->vhs_gref;
+  set_vhs_fast(p, cp->cross_section, cp->omega, cp->vhs_gref);
   p.ntc_local = cp->ntc_local;
   p.rng_kind = cp->rng;
   p.seed = make_uint2((uint32_t)cp->seed, (uint32_t)(cp->seed >> 32));

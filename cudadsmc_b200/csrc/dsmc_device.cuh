@@ -206,22 +206,30 @@ constexpr int kTriStride = 3;
 // Ray/triangle test with a determinant threshold relative to the triangle's
 // size (the reference's absolute 1e-6 rejects near-grazing rays on small
 // triangles).
+// Rounding steps explicit (no contraction), the forms of dot_x/cross_x below.
+__device__ __forceinline__ float dot_x(float3 a, float3 b) {
+  return fmaf(a.z, b.z, fmaf(a.x, b.x, __fmul_rn(a.y, b.y)));
+}
+__device__ __forceinline__ float3 cross_x(float3 a, float3 b) {
+  return make_float3(fmaf(a.y, b.z, -__fmul_rn(a.z, b.y)), fmaf(a.z, b.x, -__fmul_rn(a.x, b.z)),
+                     fmaf(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
 __device__ __forceinline__ bool intersect_triangle_rel(float3 o, float3 d, float3 a, float3 b,
                                                        float3 c, float* t) {
-  float3 e1 = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
-  float3 e2 = make_float3(c.x - a.x, c.y - a.y, c.z - a.z);
-  float3 pv = make_float3(d.y * e2.z - d.z * e2.y, d.z * e2.x - d.x * e2.z, d.x * e2.y - d.y * e2.x);
-  float det = e1.x * pv.x + e1.y * pv.y + e1.z * pv.z;
-  float scale = (e1.x * e1.x + e1.y * e1.y + e1.z * e1.z) + (e2.x * e2.x + e2.y * e2.y + e2.z * e2.z);
-  if (fabsf(det) <= 1e-9f * scale) return false;
-  float inv = 1.0f / det;
-  float3 tv = make_float3(o.x - a.x, o.y - a.y, o.z - a.z);
-  float u = (tv.x * pv.x + tv.y * pv.y + tv.z * pv.z) * inv;
+  const float3 e1 = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
+  const float3 e2 = make_float3(c.x - a.x, c.y - a.y, c.z - a.z);
+  const float3 pv = cross_x(d, e2);
+  const float det = dot_x(e1, pv);
+  const float scale = dot_x(e1, e1) + dot_x(e2, e2);
+  if (fabsf(det) <= __fmul_rn(1e-9f, scale)) return false;
+  const float inv = 1.0f / det;
+  const float3 tv = make_float3(o.x - a.x, o.y - a.y, o.z - a.z);
+  const float u = __fmul_rn(dot_x(tv, pv), inv);
   if (u < 0.f || u > 1.f) return false;
-  float3 qv = make_float3(tv.y * e1.z - tv.z * e1.y, tv.z * e1.x - tv.x * e1.z, tv.x * e1.y - tv.y * e1.x);
-  float v = (d.x * qv.x + d.y * qv.y + d.z * qv.z) * inv;
+  const float3 qv = cross_x(tv, e1);
+  const float v = __fmul_rn(dot_x(d, qv), inv);
   if (v < 0.f || u + v > 1.f) return false;
-  *t = (e2.x * qv.x + e2.y * qv.y + e2.z * qv.z) * inv;
+  *t = __fmul_rn(dot_x(e2, qv), inv);
   return true;
 }
 
@@ -330,9 +338,10 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
         const uint32_t i = i0 + k;
         if (i >= se.y) break;
         // plane pre-test: both ends of the segment on one side -> no crossing
-        const float s0 = P[k].x * o.x + P[k].y * o.y + P[k].z * o.z - P[k].w;
-        const float s1 = s0 + dist * (P[k].x * d.x + P[k].y * d.y + P[k].z * d.z);
-        const float tol = 1e-7f * (fabsf(P[k].w) + 1.f);
+        const float3 pn = make_float3(P[k].x, P[k].y, P[k].z);
+        const float s0 = dot_x(pn, o) - P[k].w;
+        const float s1 = fmaf(dist, dot_x(pn, d), s0);
+        const float tol = __fmul_rn(1e-7f, fabsf(P[k].w) + 1.f);
         if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
         float4 A = __ldg(&G.tri[kTriStride * (size_t)i]);
         float4 B = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
@@ -413,21 +422,24 @@ __device__ __forceinline__ bool inside_mesh(const GeomView& G, float3 o) {
 // from (full accommodation at the wall temperature): normal speed from the
 // flux-weighted half-range Maxwellian, tangential components Gaussian.
 // r1, r2, r3: uniforms in (0, 1).  Out of line (walls are the cold path).
+// Rounding steps explicit (no contraction), so that a CPU restatement
+// evaluates the same steps (only logf and sincosf may differ in the last bit).
 static __device__ __noinline__ float3 diffuse_emit_r(float3 n_out, float vstd, float r1, float r2,
                                                      float r3) {
-  float vn = vstd * sqrtf(-2.0f * logf(r1));
-  float rad = vstd * sqrtf(-2.0f * logf(r2));
+  const float vn = __fmul_rn(vstd, sqrtf(__fmul_rn(-2.0f, logf(r1))));
+  const float rad = __fmul_rn(vstd, sqrtf(__fmul_rn(-2.0f, logf(r2))));
   float s, c;
-  sincosf(6.2831853f * r3, &s, &c);
-  float t1 = rad * c, t2 = rad * s;
+  sincosf(__fmul_rn(6.2831853f, r3), &s, &c);
+  const float t1 = __fmul_rn(rad, c), t2 = __fmul_rn(rad, s);
   // orthonormal tangent basis of n_out
-  float3 a = fabsf(n_out.x) < 0.9f ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
-  float3 e1 = normalize3(make_float3(a.y * n_out.z - a.z * n_out.y, a.z * n_out.x - a.x * n_out.z,
-                                     a.x * n_out.y - a.y * n_out.x));
-  float3 e2 = make_float3(n_out.y * e1.z - n_out.z * e1.y, n_out.z * e1.x - n_out.x * e1.z,
-                          n_out.x * e1.y - n_out.y * e1.x);
-  return make_float3(vn * n_out.x + t1 * e1.x + t2 * e2.x, vn * n_out.y + t1 * e1.y + t2 * e2.y,
-                     vn * n_out.z + t1 * e1.z + t2 * e2.z);
+  const float3 a = fabsf(n_out.x) < 0.9f ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
+  const float3 q = cross_x(a, n_out);
+  const float ql = sqrtf(dot_x(q, q));
+  const float3 e1 = ql > 0.f ? make_float3(q.x / ql, q.y / ql, q.z / ql) : q;
+  const float3 e2 = cross_x(n_out, e1);
+  return make_float3(fmaf(t2, e2.x, fmaf(t1, e1.x, __fmul_rn(vn, n_out.x))),
+                     fmaf(t2, e2.y, fmaf(t1, e1.y, __fmul_rn(vn, n_out.y))),
+                     fmaf(t2, e2.z, fmaf(t1, e1.z, __fmul_rn(vn, n_out.z))));
 }
 __device__ __forceinline__ float3 diffuse_emit(float3 n_out, float vstd, PhiloxStream& rng) {
   const float r1 = rng.uniform(), r2 = rng.uniform(), r3 = rng.uniform();

@@ -460,7 +460,7 @@ __global__ void k_init_fill(const __grid_constant__ InitParams p) {
 // fractional remainder), reserved after the particles already in the array.
 __global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* plan) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const float want = *p.remainder + p.inflow.number_flux * p.inflow.area * p.dt;
+  const float want = fmaf(__fmul_rn(p.inflow.number_flux, p.inflow.area), p.dt, *p.remainder);
   uint32_t k = want > 0.f ? (uint32_t)want : 0u;
   const uint32_t have = p.meta->n_alive + p.meta->n_pending;
   if (have + k > p.capacity) {
@@ -476,10 +476,11 @@ __global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* 
 
 // Inward normal speed of the drifting Maxwellian weighted by flux,
 // f(z) ~ z exp(-(z - s)^2) for z = v_n / c_mp > 0, by rejection from the
-// envelope (|y| + max(s,0)) exp(-y^2), y = z - s.
+// envelope (|y| + max(s,0)) exp(-y^2), y = z - s.  Rounding steps explicit
+// (no contraction).
 __device__ __forceinline__ float sample_flux_normal(float s, PhiloxStream& r) {
   const float sp = fmaxf(s, 0.f);
-  const float w_abs = 1.f / (1.f + sp * 1.7724539f);
+  const float w_abs = 1.f / fmaf(sp, 1.7724539f, 1.f);
   for (int it = 0; it < 64; it++) {
     float y;
     if (r.uniform() < w_abs) {
@@ -487,7 +488,7 @@ __device__ __forceinline__ float sample_flux_normal(float s, PhiloxStream& r) {
       if (r.uniform() < 0.5f) y = -y;
     } else {
       const float a = r.uniform(), b = r.uniform();
-      y = sqrtf(-logf(a)) * cospif(2.0f * b);  // N(0, 1/2)
+      y = __fmul_rn(sqrtf(-logf(a)), cospif(2.0f * b));  // N(0, 1/2)
     }
     const float z = s + y;
     if (z <= 0.f) continue;
@@ -520,20 +521,20 @@ __global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint
       float3 pos = make_float3(0, 0, 0), vel = pos;
       PhiloxStream r;
       r.init(p.seed, i, step, kPurposeInject + (uint32_t)face);
-      const float vn = sample_flux_normal(s, r) * cmp * sign;
+      const float vn = __fmul_rn(__fmul_rn(sample_flux_normal(s, r), cmp), sign);
       const float a1 = r.uniform(), a2 = r.uniform();
-      const float rad = p.inflow.vstd * sqrtf(-2.f * logf(a1));
+      const float rad = __fmul_rn(p.inflow.vstd, sqrtf(__fmul_rn(-2.f, logf(a1))));
       float sn, cs;
       sincospif(2.0f * a2, &sn, &cs);
       const int a_t1 = (ax + 1) % 3, a_t2 = (ax + 2) % 3;
       comp(vel, ax) = vn;
-      comp(vel, a_t1) = rad * cs + compc(p.inflow.stream, a_t1);
-      comp(vel, a_t2) = rad * sn + compc(p.inflow.stream, a_t2);
+      comp(vel, a_t1) = fmaf(rad, cs, compc(p.inflow.stream, a_t1));
+      comp(vel, a_t2) = fmaf(rad, sn, compc(p.inflow.stream, a_t2));
       comp(pos, ax) = (face & 1) ? compc(g.gmax, ax) : compc(g.gmin, ax);
-      comp(pos, a_t1) = compc(g.gmin, a_t1) + r.uniform() * (compc(g.gmax, a_t1) - compc(g.gmin, a_t1));
-      comp(pos, a_t2) = compc(g.gmin, a_t2) + r.uniform() * (compc(g.gmax, a_t2) - compc(g.gmin, a_t2));
-      const float frac = r.uniform() * p.dt;
-      pos.x += vel.x * frac; pos.y += vel.y * frac; pos.z += vel.z * frac;
+      comp(pos, a_t1) = fmaf(r.uniform(), compc(g.gmax, a_t1) - compc(g.gmin, a_t1), compc(g.gmin, a_t1));
+      comp(pos, a_t2) = fmaf(r.uniform(), compc(g.gmax, a_t2) - compc(g.gmin, a_t2), compc(g.gmin, a_t2));
+      const float frac = __fmul_rn(r.uniform(), p.dt);
+      pos.x = fmaf(vel.x, frac, pos.x); pos.y = fmaf(vel.y, frac, pos.y); pos.z = fmaf(vel.z, frac, pos.z);
       live = !(pos.x < g.gmin.x || pos.x > g.gmax.x || pos.y < g.gmin.y || pos.y > g.gmax.y ||
                pos.z < g.gmin.z || pos.z > g.gmax.z);
       if (live) key = cell_id3d(g, pos.x, pos.y, pos.z);

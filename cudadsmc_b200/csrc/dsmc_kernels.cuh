@@ -90,9 +90,9 @@ struct StepParams {
   int hard_sphere;
   float vhs_exp;   // 2*omega - 1
   float vhs_gref;
-  // Philox mode: sigma(g) g = 2^(vhs_c1 log2 g + vhs_c0), vhs_c1 = 1 - vhs_exp,
-  // vhs_c0 = log2(cross_section) + vhs_exp log2(vhs_gref)
-  float vhs_c0, vhs_c1;
+  // Philox mode: sigma(g) g = vhs_k 2^(vhs_c1 log2 g), vhs_c1 = 1 - vhs_exp,
+  // vhs_k = cross_section vhs_gref^vhs_exp (both rounded from double)
+  float vhs_k, vhs_c1;
   int ntc_local;
   int rng_kind;    // 0 HybridTaus per cell (reference), 1 Philox
   uint2 seed;

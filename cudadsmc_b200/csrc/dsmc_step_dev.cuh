@@ -141,12 +141,20 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 
 // sigma(g) g of the Philox mode: the VHS power law as
-// 2^((1 - e) log2 g + log2 sigma_ref + e log2 g_ref) with the hardware base-2
-// log and exponential (relative error about 1e-6, far below what an
-// acceptance test R < sigma g / (sigma g)max can resolve).
+// sigma_ref g_ref^e 2^((1 - e) log2 g) with the hardware base-2 log and
+// exponential (relative error about 1e-6, far below what an acceptance test
+// R < sigma g / (sigma g)max can resolve).  Every rounding step is explicit
+// (no contraction), so that a CPU restatement evaluates the same steps.
 __device__ __forceinline__ float sigma_g_fast(const StepParams& p, float mag) {
-  if (p.hard_sphere) return mag * p.cross_section;
-  return mag > 0.f ? ex2_approx(fmaf(p.vhs_c1, lg2_approx(mag), p.vhs_c0)) : 0.f;
+  if (p.hard_sphere) return __fmul_rn(mag, p.cross_section);
+  return mag > 0.f ? __fmul_rn(p.vhs_k, ex2_approx(__fmul_rn(p.vhs_c1, lg2_approx(mag)))) : 0.f;
+}
+
+// |a - b| of the Philox mode with explicit rounding: sqrt(dz^2 + (dx^2 + dy^2)),
+// each square-add fused.
+__device__ __forceinline__ float rel_speed(float3 a, float3 b) {
+  const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+  return sqrtf(fmaf(dz, dz, fmaf(dx, dx, __fmul_rn(dy, dy))));
 }
 
 // NTC collisions of one cell with the reference's arithmetic:
@@ -218,18 +226,22 @@ __device__ __forceinline__ void ntc_reference(const StepParams& p, int partCount
 // coefficient 0.5 fnum dt / V_c.
 __device__ __forceinline__ float ntc_fpc_fast(const StepParams& p, uint32_t n, float2 vm) {
   const float avg = p.ntc_local ? (float)(n - 1) : p.avg_conc;
-  return p.ntc_coef * (float)n * avg * vm.x + vm.y;
+  return fmaf(__fmul_rn(__fmul_rn(p.ntc_coef, (float)n), avg), vm.x, vm.y);
 }
 
 // Isotropic post-collision velocities (hard sphere / VHS), accurate angles.
+// Rounding steps are explicit (no contraction): cos chi = 2 R - 1,
+// sin chi = sqrt(1 - cos^2 chi), the azimuth from sincospi, g'/2 added to and
+// taken from the centre-of-mass velocity.
 __device__ __forceinline__ void scatter_pair(float3 v1, float3 v2, float mag, float r_cos,
                                              float r_phi, float3& o1, float3& o2) {
-  const float b = 2.0f * r_cos - 1.0f;
-  const float a = sqrtf(fmaxf(0.f, 1.f - b * b));
+  const float b = fmaf(2.0f, r_cos, -1.0f);
+  const float a = sqrtf(fmaxf(0.f, fmaf(-b, b, 1.f)));
   float sn, cn;
   sincospif(2.0f * r_phi, &sn, &cn);
   const float h = 0.5f * mag;
-  const float3 ang = make_float3(b * h, a * h * cn, a * h * sn);
+  const float ah = __fmul_rn(a, h);
+  const float3 ang = make_float3(__fmul_rn(b, h), __fmul_rn(ah, cn), __fmul_rn(ah, sn));
   const float3 cm = make_float3(0.5f * (v1.x + v2.x), 0.5f * (v1.y + v2.y), 0.5f * (v1.z + v2.z));
   o1 = make_float3(cm.x + ang.x, cm.y + ang.y, cm.z + ang.z);
   o2 = make_float3(cm.x - ang.x, cm.y - ang.y, cm.z - ang.z);
@@ -257,7 +269,7 @@ __device__ __forceinline__ uint32_t ntc_select_fast(const StepParams& p, uint32_
     uint32_t pj = pi + 1u + __umulhi(r.next(), n - 1u);
     if (pj >= n) pj -= n;
     const float3 v1 = acc.get(pi), v2 = acc.get(pj);
-    const float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
+    const float mag = rel_speed(v1, v2);
     const float v = sigma_g_fast(p, mag);
     if (v > r.uniform() * vm.x) {
       ncol++;
@@ -347,7 +359,7 @@ __device__ __forceinline__ float ntc_select_heavy_warp(const StepParams& p, uint
     float vv = 0.f;
     if (win) {
       const float3 v1 = acc.get(pi), v2 = acc.get(pj);
-      const float mag = length3(make_float3(v1.x - v2.x, v1.y - v2.y, v1.z - v2.z));
+      const float mag = rel_speed(v1, v2);
       vv = sigma_g_fast(p, mag);
       if (vv > rng.uniform() * vmax) {
         ncol++;
@@ -459,20 +471,20 @@ __device__ __forceinline__ bool face_axis(const StepParams& p, float& x, float& 
     return true;
   }
   if (kind == 0) {
-    x = 2.f * bound - x;
+    x = fmaf(2.f, bound, -x);
     vx = -vx;
     return true;
   }
   // diffuse wall: back to the crossing point, re-emit, fly the rest
   const float tau = vx != 0.f ? (x - bound) / vx : 0.f;
-  pos.x -= vel.x * tau; pos.y -= vel.y * tau; pos.z -= vel.z * tau;
+  pos.x = fmaf(-vel.x, tau, pos.x); pos.y = fmaf(-vel.y, tau, pos.y); pos.z = fmaf(-vel.z, tau, pos.z);
   float3 n_in = make_float3(0.f, 0.f, 0.f);
   const float s = (face & 1) ? -1.f : 1.f;
   if (axis == 0) { pos.x = bound; n_in.x = s; }
   else if (axis == 1) { pos.y = bound; n_in.y = s; }
   else { pos.z = bound; n_in.z = s; }
   vel = diffuse_emit(n_in, p.face_vstd[face], rng);
-  pos.x += vel.x * tau; pos.y += vel.y * tau; pos.z += vel.z * tau;
+  pos.x = fmaf(vel.x, tau, pos.x); pos.y = fmaf(vel.y, tau, pos.y); pos.z = fmaf(vel.z, tau, pos.z);
   return true;
 }
 
@@ -533,10 +545,9 @@ __device__ __forceinline__ bool apply_bc(const StepParams& p, float3& pos, float
 // cannot reach the body (flight_may_meet_body false), or without a body.
 __device__ __forceinline__ bool move_free(const StepParams& p, float3& pos, float3& vel,
                                           uint32_t gidx, uint32_t step) {
-  const float3 old_pos = pos;
-  pos.x = old_pos.x + vel.x * p.dt;
-  pos.y = old_pos.y + vel.y * p.dt;
-  pos.z = old_pos.z + vel.z * p.dt;
+  pos.x = fmaf(vel.x, p.dt, pos.x);
+  pos.y = fmaf(vel.y, p.dt, pos.y);
+  pos.z = fmaf(vel.z, p.dt, pos.z);
   PhiloxStream rng;
   rng.init(p.seed, gidx, step, kPurposeWall);
   return apply_bc(p, pos, vel, rng);
@@ -569,9 +580,9 @@ __device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, fl
 __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& pos, float3& vel,
                                                    uint32_t gidx, uint32_t step, bool pretested) {
   float3 old_pos = pos;
-  pos.x = old_pos.x + vel.x * p.dt;
-  pos.y = old_pos.y + vel.y * p.dt;
-  pos.z = old_pos.z + vel.z * p.dt;
+  pos.x = fmaf(vel.x, p.dt, old_pos.x);
+  pos.y = fmaf(vel.y, p.dt, old_pos.y);
+  pos.z = fmaf(vel.z, p.dt, old_pos.z);
   PhiloxStream rng;
   rng.init(p.seed, gidx, step, kPurposeWall);
   if (p.has_geom && p.geom.nearest) {
@@ -580,7 +591,7 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
     const GeomView& G = p.geom;
     for (uint32_t b = 0; b < kCollisionLimit; b++) {
       const float3 seg = make_float3(pos.x - old_pos.x, pos.y - old_pos.y, pos.z - old_pos.z);
-      const float dist = length3(seg);
+      const float dist = sqrtf(fmaf(seg.z, seg.z, fmaf(seg.x, seg.x, __fmul_rn(seg.y, seg.y))));
       if (!(dist > 1e-12f)) break;
       // a path shorter than the start cell's clearance cannot reach the body
       if (!(pretested && b == 0)) {
@@ -590,7 +601,7 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
         if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
       }
       const float idist = 1.f / dist;
-      const float3 d = make_float3(seg.x * idist, seg.y * idist, seg.z * idist);
+      const float3 d = make_float3(__fmul_rn(seg.x, idist), __fmul_rn(seg.y, idist), __fmul_rn(seg.z, idist));
       float t;
       uint32_t e;
       if (!nearest_wall_hit(G, old_pos, d, dist, &t, &e)) break;
@@ -599,22 +610,23 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
       // the mesh is closed with outward normals: a face reached from its
       // back side holds a particle inside the body (left over from a fill of
       // a cell the body covers in part), which is removed
-      if ((d.x * n.x + d.y * n.y + d.z * n.z) > 0.f) return false;
-      const float side = 1.f;
-      const float3 n_out = make_float3(side * n.x, side * n.y, side * n.z);
-      const float3 hp = make_float3(old_pos.x + d.x * t + n_out.x * 1e-6f,
-                                    old_pos.y + d.y * t + n_out.y * 1e-6f,
-                                    old_pos.z + d.z * t + n_out.z * 1e-6f);
+      if (fmaf(d.z, n.z, fmaf(d.x, n.x, __fmul_rn(d.y, n.y))) > 0.f) return false;
+      // the hit point, set off the wall by 1e-6 m along the outward normal
+      const float3 hp = make_float3(fmaf(n.x, 1e-6f, fmaf(d.x, t, old_pos.x)),
+                                    fmaf(n.y, 1e-6f, fmaf(d.y, t, old_pos.y)),
+                                    fmaf(n.z, 1e-6f, fmaf(d.z, t, old_pos.z)));
       const float rest = dist - t;
       if (G.diffuse) {
-        const float speed = length3(vel);
-        vel = diffuse_emit(n_out, G.wall_vstd, rng);
+        const float speed = sqrtf(fmaf(vel.z, vel.z, fmaf(vel.x, vel.x, __fmul_rn(vel.y, vel.y))));
+        vel = diffuse_emit(n, G.wall_vstd, rng);
         const float tau = speed > 0.f ? rest / speed : 0.f;
-        pos = make_float3(hp.x + vel.x * tau, hp.y + vel.y * tau, hp.z + vel.z * tau);
+        pos = make_float3(fmaf(vel.x, tau, hp.x), fmaf(vel.y, tau, hp.y), fmaf(vel.z, tau, hp.z));
       } else {
-        vel = reflect3(vel, n);
-        const float3 r = normalize3(vel);
-        pos = make_float3(hp.x + r.x * rest, hp.y + r.y * rest, hp.z + r.z * rest);
+        const float vn2 = 2.f * fmaf(vel.z, n.z, fmaf(vel.x, n.x, __fmul_rn(vel.y, n.y)));
+        vel = make_float3(fmaf(-vn2, n.x, vel.x), fmaf(-vn2, n.y, vel.y), fmaf(-vn2, n.z, vel.z));
+        const float sp = sqrtf(fmaf(vel.z, vel.z, fmaf(vel.x, vel.x, __fmul_rn(vel.y, vel.y))));
+        const float3 r = sp > 0.f ? make_float3(vel.x / sp, vel.y / sp, vel.z / sp) : vel;
+        pos = make_float3(fmaf(r.x, rest, hp.x), fmaf(r.y, rest, hp.y), fmaf(r.z, rest, hp.z));
       }
       old_pos = hp;
     }

@@ -268,6 +268,16 @@ class DSMCSolver:
                     "DownloadState")
         return p, v
 
+    def ReadKeys(self):
+        """Next-step cell key of every particle slot (0xffffffff: left the
+        domain), in the order of DownloadState."""
+        n = ctypes.c_uint32(0)
+        self._check(lib().dsmc_read_keys(self.h, None, ctypes.byref(n)), "ReadKeys")
+        k = np.zeros(n.value, np.uint32)
+        n2 = ctypes.c_uint32(n.value)
+        self._check(lib().dsmc_read_keys(self.h, _ptr(k), ctypes.byref(n2)), "ReadKeys")
+        return k
+
     def SetCellState(self, maxrem=None, seeds=None):
         m = None if maxrem is None else np.ascontiguousarray(maxrem, np.float32)
         s = None if seeds is None else np.ascontiguousarray(seeds, np.uint32)

@@ -231,6 +231,13 @@ int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out)
  * reference's particles_state_t.  Upload resets the cell order. */
 int dsmc_upload_state(dsmc_handle* h, const float* pos, const float* vel, uint32_t n, int soa);
 int dsmc_download_state(dsmc_handle* h, float* pos, float* vel, uint32_t* n, int soa);
+/* The cell key of every particle slot that dsmc_download_state returns, in
+ * the same order: the cell the particle sits in for the next step's sort, or
+ * 0xffffffff for a particle that left the domain (outflow) or was found
+ * inside the body.  The reference keeps its keys (gridHashes,
+ * include/gpu_dsmc.inl:352-359) internal; this exposes them for parity
+ * checks. */
+int dsmc_read_keys(dsmc_handle* h, uint32_t* keys, uint32_t* n);
 /* Per-cell collision state: (sigma*g)max and remainder (float2 per cell,
  * kernels/dsmc_kernel.cu:131) and HybridTaus seeds (uint4 per cell, :124). */
 int dsmc_set_cell_state(dsmc_handle* h, const float* maxrem, const uint32_t* seeds);

@@ -101,6 +101,72 @@ long orc_build_grid(const float* verts, uint32_t nverts, const uint32_t* tris, u
                     const int dim[3], float bbox[6], float cell[3], uint32_t* count,
                     uint32_t* tri_ids, long cap, uint8_t* flags);
 
+/* ---- The extension mode (fast_oracle.c): Philox streams, VHS, warp-collided
+ * dense cells, nearest wall crossings with diffuse walls, per-face
+ * boundaries, inflow.  No counterpart in the reference. */
+typedef struct {
+  uint32_t key[2];     /* Philox key: the run's 64-bit seed, low word first */
+  uint32_t step;       /* timestep counter (Philox counter word 2) */
+  float ntc_coef;      /* 0.5 F_N dt / V_c, rounded to float */
+  float avg_conc;      /* particles per cell of the reference NTC (ntc_local = 0) */
+  int ntc_local;       /* 1: N_c - 1 */
+  int hard_sphere;
+  float cross_section; /* hard sphere: sigma g = g cross_section */
+  float vhs_k, vhs_c1; /* VHS: sigma g = vhs_k 2^(vhs_c1 log2 g) */
+  uint32_t heavy_min;  /* pair count from which a cell is collided by a warp */
+  uint32_t warp_cap;   /* cells holding more particles are collided by one lane */
+  float tie_rel;       /* relative margin of an acceptance flagged as a near tie */
+} orc_fast;
+
+/* NTC collisions of every cell in the sorted SoA velocities (in place).
+ * cell_info (optional): per cell the pair count, the collisions, the path
+ * (0 none, 1 lane, 2 warp, 3 lane for a cell above warp_cap) and the near
+ * ties; sum_g_out (optional): sum of the colliding pairs' relative speeds. */
+void orc_collide_fast(const orc_fast* f, float* u, float* v, float* w, const uint32_t* start,
+                      uint32_t ncells, float* maxrem, uint32_t* cell_info, double* sum_g_out);
+
+typedef struct {
+  float gmin[3];
+  float gmax[3];
+  float cell[3];
+  uint32_t dim[3];
+  int face_kind[6];    /* -x,+x,-y,+y,-z,+z: 0 specular, 1 diffuse, 2 outflow, 3 periodic, 4 inflow */
+  float face_vstd[6];  /* sqrt(k T_face / m) */
+  float dt;
+  uint32_t key[2];
+  uint32_t step;
+  uint32_t ntris;      /* 0: no body */
+  const float* tri;    /* 9 floats per triangle: the three vertices */
+  const float* plane;  /* 4 floats per triangle: unit normal, offset (orc_tri_planes) */
+  int wall_diffuse;
+  float wall_vstd;
+  float amb_rel;       /* relative margin of a crossing flagged as ambiguous */
+} orc_fast_move;
+
+/* Flights of n particles (SoA, in place); gidx0 + i is particle i's wall
+ * stream.  live[i] = 0: the particle left the domain or was inside the body;
+ * amb[i] = 1: a crossing within the margin (see fast_oracle.c). */
+void orc_move_fast(const orc_fast_move* m, float* x, float* y, float* z, float* u, float* v,
+                   float* w, uint32_t n, uint32_t gidx0, uint8_t* live, uint8_t* amb);
+void orc_tri_planes(const float* tri9, uint32_t ntris, float* plane4);
+
+typedef struct {
+  int face;
+  float number_flux;   /* simulator particles per unit area per second */
+  float area;
+  float stream[3];
+  float vstd;
+} orc_inflow;
+
+/* The injection count of one step (k_inject_plan), remainder updated. */
+uint32_t orc_inject_plan(const orc_inflow* in, float dt, float* remainder, uint32_t max_k);
+/* One step's injection through an inflow face: returns the count k (at most
+ * max_k) and writes the particles to x..w[0, k). */
+uint32_t orc_inject_fast(const orc_inflow* in, const float gmin[3], const float gmax[3], float dt,
+                         const uint32_t key[2], uint32_t step, float* remainder, uint32_t max_k,
+                         float* x, float* y, float* z, float* u, float* v, float* w, uint8_t* amb,
+                         float tie_rel);
+
 int orc_set_threads(int n);
 int orc_get_threads(void);
 

@@ -49,8 +49,9 @@ _orc = None
 
 
 def ensure_built():
-    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(
-            os.path.join(HERE, "dsmc_oracle.c")):
+    srcs = [os.path.join(HERE, f) for f in ("dsmc_oracle.c", "fast_oracle.c", "dsmc_oracle.h")]
+    if not os.path.exists(ORACLE_SO) or os.path.getmtime(ORACLE_SO) < max(
+            os.path.getmtime(f) for f in srcs):
         subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
 
 
@@ -69,6 +70,8 @@ def orc():
         L.orc_mt_lcg.argtypes = [ctypes.c_uint32]
         L.orc_mt_int.restype = ctypes.c_uint32
         L.orc_mt_float.restype = ctypes.c_float
+        L.orc_inject_fast.restype = ctypes.c_uint32
+        L.orc_inject_plan.restype = ctypes.c_uint32
         _orc = L
     return _orc
 
@@ -334,3 +337,253 @@ def set_threads(n):
 
 def threads():
     return orc().orc_get_threads()
+
+
+# ---------------------------------------------------------------------------
+# The extension mode (fast_oracle.c): Philox streams, VHS, warp-collided dense
+# cells, nearest wall crossings with diffuse walls, per-face boundaries and
+# inflow.  No counterpart in the reference.
+
+DEAD = 0xFFFFFFFF
+
+
+class OrcFast(ctypes.Structure):
+    _fields_ = [("key", ctypes.c_uint32 * 2), ("step", ctypes.c_uint32),
+                ("ntc_coef", ctypes.c_float), ("avg_conc", ctypes.c_float),
+                ("ntc_local", ctypes.c_int), ("hard_sphere", ctypes.c_int),
+                ("cross_section", ctypes.c_float), ("vhs_k", ctypes.c_float),
+                ("vhs_c1", ctypes.c_float), ("heavy_min", ctypes.c_uint32),
+                ("warp_cap", ctypes.c_uint32), ("tie_rel", ctypes.c_float)]
+
+
+class OrcFastMove(ctypes.Structure):
+    _fields_ = [("gmin", c_f3), ("gmax", c_f3), ("cell", c_f3), ("dim", c_u3),
+                ("face_kind", ctypes.c_int * 6), ("face_vstd", ctypes.c_float * 6),
+                ("dt", ctypes.c_float), ("key", ctypes.c_uint32 * 2), ("step", ctypes.c_uint32),
+                ("ntris", ctypes.c_uint32), ("tri", _P), ("plane", _P),
+                ("wall_diffuse", ctypes.c_int), ("wall_vstd", ctypes.c_float),
+                ("amb_rel", ctypes.c_float)]
+
+
+class OrcInflow(ctypes.Structure):
+    _fields_ = [("face", ctypes.c_int), ("number_flux", ctypes.c_float), ("area", ctypes.c_float),
+                ("stream", c_f3), ("vstd", ctypes.c_float)]
+
+
+def seed_words(seed):
+    return [int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF]
+
+
+def vhs_fast_coeffs(cross_section, omega, gref):
+    """(vhs_k, vhs_c1) of sigma g = vhs_k 2^(vhs_c1 log2 g), from double."""
+    e = 2.0 * float(np.float32(omega)) - 1.0
+    return (float(np.float32(float(cross_section) * float(gref) ** e)), float(np.float32(1.0 - e)))
+
+
+def fast_params(seed, step, fnum, dt, cell_volume, cross_section, omega=0.5, vhs_gref=0.0,
+                avg_conc=0.0, ntc_local=1, heavy_min=8, warp_cap=128, tie_rel=4e-6):
+    f = OrcFast()
+    f.key[:] = seed_words(seed)
+    f.step = int(step)
+    f.ntc_coef = float(np.float32(0.5 * float(np.float32(fnum)) * float(np.float32(dt)) /
+                                  float(np.float32(cell_volume))))
+    f.avg_conc = float(avg_conc)
+    f.ntc_local = int(ntc_local)
+    f.hard_sphere = int(abs(float(np.float32(omega)) - 0.5) < 1e-9)
+    f.cross_section = float(cross_section)
+    if not f.hard_sphere:
+        f.vhs_k, f.vhs_c1 = vhs_fast_coeffs(cross_section, omega, vhs_gref)
+    f.heavy_min = int(heavy_min)
+    f.warp_cap = int(warp_cap)
+    f.tie_rel = float(tie_rel)
+    return f
+
+
+def collide_fast(f, u, v, w, start, maxrem):
+    """NTC collisions in place on the sorted velocities u, v, w (float32) and
+    maxrem ((cells, 2) float32).  Returns (per cell: pairs, collisions, path,
+    near ties) and the sum of the colliding pairs' relative speeds."""
+    ncells = len(start) - 1
+    info = np.zeros((ncells, 4), np.uint32)
+    sg = ctypes.c_double(0.0)
+    st = np.ascontiguousarray(start, np.uint32)
+    orc().orc_collide_fast(ctypes.byref(f), p(u), p(v), p(w), p(st), ncells, p(maxrem), p(info),
+                           ctypes.byref(sg))
+    return info, sg.value
+
+
+def tri_planes(tri9):
+    t = np.ascontiguousarray(tri9, np.float32).reshape(-1, 9)
+    out = np.zeros((t.shape[0], 4), np.float32)
+    orc().orc_tri_planes(p(t), t.shape[0], p(out))
+    return out
+
+
+def triangles_of(verts, tris):
+    v = np.asarray(verts, np.float32).reshape(-1, 3)
+    t = np.asarray(tris, np.int64).reshape(-1, 3)
+    return np.ascontiguousarray(v[t].reshape(-1, 9))
+
+
+def fast_move_params(sim, face_kind, face_vstd, dt, seed, step, tri9=None, wall_diffuse=1,
+                     wall_vstd=0.0, amb_rel=1e-5):
+    m = OrcFastMove()
+    m.gmin[:] = list(sim.gmin)
+    m.gmax[:] = list(sim.gmax)
+    m.cell[:] = list(sim.cell)
+    m.dim[:] = list(sim.dim)
+    m.face_kind[:] = [int(k) for k in face_kind]
+    m.face_vstd[:] = [float(x) for x in face_vstd]
+    m.dt = float(dt)
+    m.key[:] = seed_words(seed)
+    m.step = int(step)
+    m.wall_diffuse = int(wall_diffuse)
+    m.wall_vstd = float(wall_vstd)
+    m.amb_rel = float(amb_rel)
+    if tri9 is not None and len(tri9):
+        t = np.ascontiguousarray(tri9, np.float32).reshape(-1, 9)
+        pl = tri_planes(t)
+        m._keep = (t, pl)
+        m.ntris = t.shape[0]
+        m.tri, m.plane = p(t), p(pl)
+    else:
+        m.ntris = 0
+    return m
+
+
+def move_fast(m, st6, gidx0=0):
+    """Flights in place on st6 ((6, n) float32, rows x y z u v w).  Returns
+    (live, ambiguous) per particle."""
+    n = st6.shape[1]
+    live = np.zeros(n, np.uint8)
+    amb = np.zeros(n, np.uint8)
+    rows = [np.ascontiguousarray(st6[k]) for k in range(6)]
+    orc().orc_move_fast(ctypes.byref(m), *[p(r) for r in rows], n, int(gidx0), p(live), p(amb))
+    for k in range(6):
+        st6[k] = rows[k]
+    return live.astype(bool), amb.astype(bool)
+
+
+def inflow_of(face, number_flux, area, stream, vstd):
+    i = OrcInflow()
+    i.face, i.number_flux, i.area = int(face), float(number_flux), float(area)
+    i.stream[:] = [float(x) for x in stream]
+    i.vstd = float(vstd)
+    return i
+
+
+def inject_fast(inflow, sim, dt, seed, step, remainder, max_k, tie_rel=1e-5):
+    """One step's injection through one face.  Returns ((6, k) state, ambiguous,
+    new remainder)."""
+    rem = ctypes.c_float(remainder)
+    gmin = np.array(list(sim.gmin), np.float32)
+    gmax = np.array(list(sim.gmax), np.float32)
+    key = np.array(seed_words(seed), np.uint32)
+    buf = [np.zeros(max(int(max_k), 1), np.float32) for _ in range(6)]
+    amb = np.zeros(max(int(max_k), 1), np.uint8)
+    k = orc().orc_inject_fast(ctypes.byref(inflow), p(gmin), p(gmax), ctypes.c_float(dt), p(key),
+                              int(step), ctypes.byref(rem), int(max_k), *[p(b) for b in buf],
+                              p(amb), ctypes.c_float(tie_rel))
+    return np.stack([b[:k] for b in buf]), amb[:k].astype(bool), rem.value
+
+
+def inject_plan_chain(inflow, dt, steps, remainder=0.0):
+    """The injection remainder after `steps` steps from `remainder` (the
+    count of each step from k_inject_plan's arithmetic)."""
+    rem = ctypes.c_float(remainder)
+    ks = []
+    for _ in range(int(steps)):
+        ks.append(orc().orc_inject_plan(ctypes.byref(inflow), ctypes.c_float(dt), ctypes.byref(rem),
+                                        0xFFFFFFFF))
+    return rem.value, ks
+
+
+def library_inflows(settings_cfg):
+    """The inflow faces as the library derives them from a configuration
+    (number flux of a drifting Maxwellian through each inflow face, in
+    simulator particles, evaluated in double and rounded to float)."""
+    import math
+    c = settings_cfg
+    vstd = math.sqrt(1.3806e-23 * float(np.float32(c.temp)) / float(np.float32(c.gas_mass)))
+    cmp = math.sqrt(2.0) * vstd
+    out = []
+    for f in range(6):
+        if c.face_kind[f] != 4:
+            continue
+        ax = f >> 1
+        sign = -1.0 if f & 1 else 1.0
+        un = sign * float(np.float32(c.stream_vel[ax]))
+        s = un / cmp
+        flux = float(np.float32(c.density)) * cmp / (2.0 * math.sqrt(math.pi)) * (
+            math.exp(-s * s) + math.sqrt(math.pi) * s * (1.0 + math.erf(s)))
+        a1, a2 = (ax + 1) % 3, (ax + 2) % 3
+        area = (float(np.float32(np.float32(c.grid_max[a1]) - np.float32(c.grid_min[a1]))) *
+                float(np.float32(np.float32(c.grid_max[a2]) - np.float32(c.grid_min[a2]))))
+        out.append(inflow_of(f, np.float32(flux / float(np.float32(c.fnum))), np.float32(area),
+                             [float(np.float32(x)) for x in c.stream_vel], np.float32(vstd)))
+    return out
+
+
+def keys_of(sim, st6, live=None):
+    """Cell ids (GetCellID3D) of the positions in st6; DEAD where not live."""
+    n = st6.shape[1]
+    pos4 = np.zeros((n, 4), np.float32)
+    pos4[:, :3] = st6[:3].T
+    keys, _ = cell_ids(sim, pos4)
+    if live is not None:
+        keys = np.where(live, keys, np.uint32(DEAD)).astype(np.uint32)
+    return keys
+
+
+def near_cell_face(sim, st6, rel=1e-5):
+    """Particles within rel of a cell size from a cell face (their key may
+    flip with a last-bit difference of the position)."""
+    pos = st6[:3].astype(np.float64)
+    lo = np.array(list(sim.gmin), np.float64)[:, None]
+    cs = np.array(list(sim.cell), np.float64)[:, None]
+    fr = (pos - lo) / cs
+    return np.any(np.abs(fr - np.round(fr)) < rel, axis=0)
+
+
+def step_fast(f, m, sim, st6, keys, maxrem, inflows=(), inj_rem=None, max_total=None):
+    """One timestep of the extension mode, composed from the restated stages
+    in the order the library runs them: stable sort by cell (removed
+    particles dropped), NTC collisions, flights (gidx = sorted slot), next
+    keys, then the inflow faces' particles appended (plan + fill per face).
+    Returns a dict with the new state, keys, maxrem, remainders, per-cell info
+    and the near-tie / ambiguity masks over the new slots."""
+    keys = np.asarray(keys, np.uint32)
+    alive = np.nonzero(keys != DEAD)[0]
+    order = alive[np.argsort(keys[alive], kind="stable")]
+    nk = keys[order]
+    counts = np.bincount(nk, minlength=sim.cells)
+    start = np.zeros(sim.cells + 1, np.uint32)
+    start[1:] = np.cumsum(counts)
+    S = np.ascontiguousarray(st6[:, order], np.float32)
+    mr = np.ascontiguousarray(maxrem, np.float32).copy()
+    u, v, w = (np.ascontiguousarray(S[k]) for k in (3, 4, 5))
+    info, sum_g = collide_fast(f, u, v, w, start, mr)
+    S[3], S[4], S[5] = u, v, w
+    tie_cell = info[:, 3] > 0
+    tie_slot = np.repeat(tie_cell, counts)
+    live, amb = move_fast(m, S)
+    nkeys = keys_of(sim, S, live)
+    amb = amb | (live & near_cell_face(sim, S))
+    parts, pkeys, pamb = [S], [nkeys], [amb | tie_slot]
+    rems = dict(inj_rem or {})
+    total = S.shape[1]
+    for inflow in inflows:
+        cap = (max_total - total) if max_total is not None else 1 << 26
+        st, ia, r = inject_fast(inflow, sim, m.dt, f.key[0] | (f.key[1] << 32), f.step,
+                                rems.get(inflow.face, 0.0), cap)
+        rems[inflow.face] = r
+        inside = np.all((st[:3] >= np.array(list(sim.gmin), np.float32)[:, None]) &
+                        (st[:3] <= np.array(list(sim.gmax), np.float32)[:, None]), axis=0)
+        parts.append(st)
+        pkeys.append(keys_of(sim, st, inside))
+        pamb.append(ia | near_cell_face(sim, st))
+        total += st.shape[1]
+    return {"state": np.concatenate(parts, axis=1), "keys": np.concatenate(pkeys),
+            "maxrem": mr, "inj_rem": rems, "info": info, "sum_g": sum_g, "start": start,
+            "n_alive": int(len(order)), "ambiguous": np.concatenate(pamb), "tie_cell": tie_cell,
+            "order": order}
