@@ -161,14 +161,35 @@ def build_solver(wl, seed_offset=0):
 # ------------------------------------------------------------------ clocks ---
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every millisecond from a thread (the region can be a
+    few milliseconds long), nvidia-smi at 100 ms where NVML is not usable.
+    Read-only: nothing here changes a setting of the GPU."""
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    BITS = [0x8, 0x40, 0x20, 0x4]  # nvmlClocksEventReason* of the same names
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, period_s=0.001):
         self.idx = gpu_index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, max MHz, reason bits)
+        self.stop = threading.Event()
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(int(self.idx))
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self._poll_once()
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nvml = None
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -182,11 +203,36 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll_once(self):
+        p = self.nvml
+        mhz = p.nvmlDeviceGetClockInfo(self.h, p.NVML_CLOCK_SM)
+        try:
+            bits = p.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        except AttributeError:
+            bits = p.nvmlDeviceGetCurrentClocksThrottleReasons(self.h)
+        self.samples.append((float(mhz), float(self.max_mhz), int(bits)))
+
+    def _poll(self):
+        while not self.stop.is_set():
+            try:
+                self._poll_once()
+            except Exception:
+                return
+            self.stop.wait(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=2)
+            try:
+                self._poll_once()
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -196,67 +242,84 @@ class ClockSampler:
 
     def summary(self):
         mhz, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 7:
-                continue
-            try:
-                mhz.append(float(f[0]))
-                mx = float(f[1])
-            except ValueError:
-                continue
-            for k, nm in enumerate(names):
-                if f[3 + k].lower().startswith("active"):
-                    reasons.add(nm)
+        if self.samples:
+            for m, x, bits in self.samples:
+                mhz.append(m)
+                mx = x
+                for nm, b in zip(self.NAMES, self.BITS):
+                    if bits & b:
+                        reasons.add(nm)
+            src = f"NVML every {self.period * 1e3:.0f} ms"
+        else:
+            for ln in self.lines:
+                f = [x.strip() for x in ln.split(",")]
+                if len(f) < 7:
+                    continue
+                try:
+                    mhz.append(float(f[0]))
+                    mx = float(f[1])
+                except ValueError:
+                    continue
+                for k, nm in enumerate(self.NAMES):
+                    if f[3 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            src = "nvidia-smi every 100 ms"
         return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(mhz)}
+                "reasons": sorted(reasons), "samples": len(mhz), "source": src}
 
 
 # ------------------------------------------------------------- CPU oracle ---
 
-def cpu_oracle_sample(wl, budget_s=12.0, max_threads=None):
-    """The oracle's reference step (OpenMP) on a bounded sample of the
-    workload: an x-slab of its cells with its free-stream fill (closed slab
-    walls, the mesh specular, HybridTaus, the workload's VHS exponent).
-    Returns (particle-timesteps/s, threads, description)."""
+def cpu_oracle_sample(wl, budget_s=12.0, max_threads=None, warmup=1, max_steps=50):
+    """The oracle's restatement of the reference step (OpenMP over the host
+    cores) on the workload's own grid, particle count and body: the
+    reference's free-stream fill (part_per_cell per cell, cells covered by
+    the body included), HybridTaus NTC with the workload's VHS exponent, the
+    reference's first-hit specular body, and its closed-box boundary functor.
+    The reference expresses neither inflow/outflow faces nor diffuse walls
+    nor Philox streams; those three are its closest counterparts.  The mesh
+    comes from oracle/meshes.py, so the product library is not loaded.
+    `warmup` untimed steps, then timed steps until budget_s or max_steps.
+    Returns (particle-timesteps/s, threads, description, particles, steps,
+    seconds)."""
     from oracle import oracle as O
+    from oracle import meshes as OM
     if max_threads:
         O.set_threads(max_threads)
     s = wl["settings"]
     dim = list(s["grid_dim"])
     gmin, gmax = np.asarray(s["grid_min"], np.float64), np.asarray(s["grid_max"], np.float64)
-    cell = (gmax - gmin) / np.asarray(dim)
-    nx = max(1, min(dim[0], 16))
-    x0 = dim[0] // 3
-    sub_min = gmin.copy()
-    sub_max = gmax.copy()
-    sub_min[0] = gmin[0] + x0 * cell[0]
-    sub_max[0] = sub_min[0] + nx * cell[0]
-    sub_dim = (nx, dim[1], dim[2])
-    import math as _m
     w = s.get("gas_omega", 0.5)
     gref = 0.0
     if abs(w - 0.5) > 1e-9:
-        gref = _m.sqrt(2 * KB * s["gas_tref"] / (0.5 * s["gas_mass"])) * _m.gamma(2.5 - w) ** (-1 / (2 * w - 1))
-    sim = O.sim_from(sub_min, sub_max, sub_dim, s["fnum"], O.cross_section_of(s["gas_diam"]), "n", w, gref)
+        gref = math.sqrt(2 * KB * s["gas_tref"] / (0.5 * s["gas_mass"])) * math.gamma(2.5 - w) ** (-1 / (2 * w - 1))
+    sim = O.sim_from(gmin, gmax, dim, s["fnum"], O.cross_section_of(s["gas_diam"]), "n", w, gref)
     ppc = int(np.float32(s["density"]) * np.float32(sim.cell_volume) / np.float32(s["fnum"]))
     rng = np.random.default_rng(1)
     n = ppc * sim.cells
     pos = np.zeros((n, 4), np.float32)
     vel = np.zeros((n, 4), np.float32)
-    pos[:, :3] = rng.uniform(sub_min, sub_max, (n, 3))
+    # ppc particles uniform in every cell (GenerateUniformVelocitiesDevBlocks' fill)
+    cell_idx = np.repeat(np.arange(sim.cells, dtype=np.int64), ppc)
+    cx = cell_idx % dim[0]
+    cy = (cell_idx // dim[0]) % dim[1]
+    cz = cell_idx // (dim[0] * dim[1])
+    cs = np.asarray(list(sim.cell), np.float64)
+    pos[:, 0] = gmin[0] + (cx + rng.uniform(0, 1, n)) * cs[0]
+    pos[:, 1] = gmin[1] + (cy + rng.uniform(0, 1, n)) * cs[1]
+    pos[:, 2] = gmin[2] + (cz + rng.uniform(0, 1, n)) * cs[2]
+    pos[:, 3] = 1.0
+    del cell_idx, cx, cy, cz
     vstd = math.sqrt(KB * s["temp"] / s["gas_mass"])
     vel[:, :3] = rng.normal(0, vstd, (n, 3)) + np.asarray(s.get("stream_vel", (0, 0, 0)))
     geom = None
     m = wl["mesh"]
     if m is not None:
-        import cudadsmc_b200 as cb
         if m["kind"] == "capsule":
-            v, t = cb.mesh_capsule(m["nose_radius"], m["cone_deg"], m["length"], m["nose_center"],
-                                   m["ntarget"], m["seed"])
+            v, t = OM.capsule(m["nose_radius"], m["cone_deg"], m["length"], m["nose_center"],
+                              m["ntarget"], m["seed"])
         else:
-            v, t = cb.mesh_icosphere(m["level"], m["radius"], m["center"])
+            v, t = OM.icosphere(m["level"], m["radius"], m["center"])
         bbox, gc, count, ids, flags = O.build_grid(v, t, m["grid"])
         nrm = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
         nrm = (nrm / np.linalg.norm(nrm, axis=1, keepdims=True)).astype(np.float32)
@@ -267,14 +330,19 @@ def cpu_oracle_sample(wl, budget_s=12.0, max_threads=None):
     mr[:, 1] = rng.uniform(0, 1, sim.cells)
     st4 = np.zeros((sim.cells, 4), np.float32)
     dt = s["dt"]
+    for _ in range(max(0, int(warmup))):
+        pos, vel, _ = O.step(sim, geom, pos, vel, dt, float(ppc), mr, st4, seeds)
     steps, t_total = 0, 0.0
-    while t_total < budget_s and steps < 50:
+    while steps < 1 or (t_total < budget_s and steps < max_steps):
         t0 = time.perf_counter()
         pos, vel, _ = O.step(sim, geom, pos, vel, dt, float(ppc), mr, st4, seeds)
         t_total += time.perf_counter() - t0
         steps += 1
-    desc = (f"oracle reference step on an x-slab of the workload ({sub_dim[0]}x{sub_dim[1]}x{sub_dim[2]} cells, "
-            f"{n} particles, {steps} steps, {O.threads()} threads)")
+    desc = (f"oracle restatement of the reference step on the full workload grid ({dim[0]}x{dim[1]}x"
+            f"{dim[2]} cells, {n} particles, {int(warmup)} untimed + {steps} timed steps, "
+            f"{O.threads()} threads); closest reference physics: closed specular box for the "
+            f"inflow/outflow faces, first-hit specular body for the diffuse nearest-hit wall, "
+            f"HybridTaus for Philox")
     return n * steps / t_total, O.threads(), desc, n, steps, t_total
 
 
@@ -621,10 +689,11 @@ def run_reference(args):
     wl = WORKLOADS[args.workload]()
     if wl.get("members"):
         wl = dict(wl, settings=wl["members"][0]["settings"])
-    budget = max(10.0, min(120.0, 4.0 * (args.steps + args.warmup)))
+    budget = max(10.0, min(90.0, 4.0 * args.steps))
     from oracle import oracle as O
     O.set_threads(os.cpu_count() or 1)
-    v, cores, desc, n, steps, tt = cpu_oracle_sample(wl, budget_s=budget)
+    v, cores, desc, n, steps, tt = cpu_oracle_sample(wl, budget_s=budget, warmup=min(args.warmup, 2),
+                                                     max_steps=args.steps)
     out = {"metric": "particle-timesteps/s", "value": v, "unit": "particle-timesteps/s", "n_gpus": 1,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": tt / steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -282,9 +282,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     const bool mine = lane >= C.cur && lane < C.cur + C.k;
     const uint32_t s0 = A.s - C.base, nc = A.e - A.s;  // meaningful for `mine`
     const bool ne = mine && nc > 0;
+    const uint32_t ne_idx = __popc(__ballot_sync(kFull, ne) & ((1u << lane) - 1u));
     if (!C.giant && C.n) {
-      const unsigned ne_mask = __ballot_sync(kFull, ne);
-      if (ne) S.cr[__popc(ne_mask & ((1u << lane) - 1u))] = s0 | ((s0 + nc) << 16);
+      if (ne) S.cr[ne_idx] = s0 | ((s0 + nc) << 16);
       const uint32_t par = (phase >> C.buf) & 1u;
       bool ok = mbar_wait_bounded(&S.mbar[C.buf], par);
       phase ^= 1u << C.buf;
@@ -331,6 +331,34 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       // number of smaller origs there (element j of the chunk sits at
       // ORA[j + off]).
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][6]);
+      if (do_fixup) {
+        // Descents of orig inside the chunk.  A cell without one is in stable
+        // order already (its particles took their tickets in one or a few
+        // increasing runs, the common case) and a slot's rank there is its
+        // position; only cells with a descent count smaller origs.  The flag
+        // goes to bit 31 of the cell's range entry.
+        uint32_t dw[CAPW / 32];
+#pragma unroll
+        for (int k = 0; k < CAPW / 32; k++) {
+          const uint32_t t = 32u * k + lane;
+          dw[k] = __ballot_sync(kFull, t > 0 && t < n && OR[t - 1] > OR[t]);
+        }
+        if (ne && nc > 1) {
+          bool unsorted = false;
+          const uint32_t lo_b = s0 + 1u, hi_b = s0 + nc;
+#pragma unroll
+          for (int k = 0; k < CAPW / 32; k++) {
+            const uint32_t w0 = 32u * k;
+            const uint32_t l = max(lo_b, w0), h = min(hi_b, w0 + 32u);
+            if (l < h) {
+              const uint32_t m = (uint32_t)(((1ull << (h - w0)) - 1ull) & ~((1ull << (l - w0)) - 1ull));
+              unsorted |= (dw[k] & m) != 0u;
+            }
+          }
+          if (unsorted) S.cr[ne_idx] |= 0x80000000u;
+        }
+        __syncwarp();
+      }
       for (uint32_t b0 = 0; b0 < n; b0 += 32) {
         const uint32_t t = b0 + lane;
         const uint32_t my = t < n ? OR[t] : 0u;
@@ -344,14 +372,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
           const uint32_t before = __popc(__ballot_sync(kFull, ne && s0 < b0));
           if (t < n) {
             const uint32_t ab = S.cr[before + __popc(starts & (0xffffffffu >> (31u - lane))) - 1u];
-            const uint32_t a = ab & 0xffffu, b = ab >> 16;
-            const uint32_t lo = a + off, hi = b + off;
-            uint32_t rank = 0;
-            // one element per step: the lanes of a cell read the same word
-            // (a broadcast), and lanes of different cells only differ in the
-            // trip count (a 16-byte form with edge cases diverged in both)
-            for (uint32_t j = lo; j < hi; j++) rank += (uint32_t)(ORA[j] < my);
-            pos = a + rank;
+            if (ab >> 31) {
+              const uint32_t a = ab & 0xffffu, b = (ab >> 16) & 0x7fffu;
+              const uint32_t lo = a + off, hi = b + off;
+              uint32_t rank = 0;
+              // one element per step: the lanes of a cell read the same word
+              // (a broadcast), and lanes of different cells only differ in
+              // the trip count (a 16-byte form with edge cases diverged in
+              // both)
+              for (uint32_t j = lo; j < hi; j++) rank += (uint32_t)(ORA[j] < my);
+              pos = a + rank;
+            }
           }
         }
         if (t < n) {

@@ -39,3 +39,24 @@ def test_planted_collision_rate_is_rejected(base):
     r = _compare(base, pair_scale=1.5)
     assert not F.agree(r)
     assert min(r["mean_z2_per_field"]) > 1.6  # every field carries it
+
+
+@pytest.fixture(scope="module")
+def base_fast():
+    return S.oracle_replicas_fast(1, REPLICAS, SETTLE, STEPS)
+
+
+def test_fast_mode_independent_runs_agree_and_planted_wall_is_rejected(base_fast):
+    """The extension-mode flow (inflow/outflow, VHS, diffuse 300 K sphere):
+    independent oracle runs agree; a wall at 450 K and 1.5x the NTC pairs are
+    rejected."""
+    other = S.oracle_replicas_fast(1001, REPLICAS, SETTLE, STEPS)
+    r = F.compare(base_fast, other, STEPS, S.MASS, MIN_COUNT)
+    assert r["cells"] > 3000
+    assert F.agree(r), r["mean_z2_per_field"]
+    hot = S.oracle_replicas_fast(1001, REPLICAS, SETTLE, STEPS, wall_temp=450.0)
+    r = F.compare(base_fast, hot, STEPS, S.MASS, MIN_COUNT)
+    assert not F.agree(r), r["mean_z2_per_field"]
+    pairs = S.oracle_replicas_fast(1001, REPLICAS, SETTLE, STEPS, pair_scale=1.5)
+    r = F.compare(base_fast, pairs, STEPS, S.MASS, MIN_COUNT)
+    assert not F.agree(r), r["mean_z2_per_field"]

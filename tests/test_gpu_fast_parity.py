@@ -133,8 +133,17 @@ def test_collide_philox_matches_oracle(cuda, omega):
         assert np.allclose(mr_g[ok, 0], mr_o[ok, 0], rtol=4e-6, atol=0)
     slot_ok = np.repeat(ok, counts)
     speed = np.linalg.norm(vo.astype(np.float64), axis=0)
-    err = np.max(np.abs(vg - vo), axis=0)[slot_ok] / np.maximum(speed[slot_ok], 1.0)
-    assert err.max() <= 1e-6, err.max()
+    err = np.max(np.abs(vg - vo), axis=0) / np.maximum(speed, 1.0)
+    # the FP32 bound is per collision: a particle of a dense cell takes part
+    # in many collisions of one pass (each rounds sincospi's last bit apart),
+    # so the bound scales with the collisions per particle of its cell
+    per_particle = np.maximum(1.0, 2.0 * info[:, 1] / np.maximum(counts, 1))
+    bound = 1e-6 * np.repeat(per_particle, counts)
+    light = np.repeat(per_particle <= 1.0, counts)
+    print(f"velocity error / speed: light cells {err[slot_ok & light].max():.2e}, "
+          f"all {err[slot_ok].max():.2e} (bound up to {bound.max():.1e})")
+    assert err[slot_ok & light].max() <= 1e-6
+    assert np.all(err[slot_ok] <= bound[slot_ok])
     changed = np.any(vg != vel, axis=0)
     assert changed.mean() > 0.3
     # momentum and energy of every cell conserved to FP32 rounding
