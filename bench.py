@@ -646,6 +646,7 @@ def run_e2e(args, wl, rank, world, dev, variant):
     state = sol.DownloadState()  # the initial state, as a host would provide it
     host = torch.from_numpy(state).pin_memory()
     tot = torch.zeros((2, 24), dtype=torch.uint8).pin_memory()
+    fields_host = torch.zeros((sol.Info().cells, 5), dtype=torch.float64).pin_memory()
     ev = [torch.cuda.Event(), torch.cuda.Event()]
     dt = wl["settings"]["dt"]
     # as many steps as the device-timed region: a run uploads its state once
@@ -669,7 +670,7 @@ def run_e2e(args, wl, rank, world, dev, variant):
             totals = sol.TotalsFromBytes(tot[(i - 1) % 2].numpy())
     ev[(k - 1) % 2].synchronize()
     totals = sol.TotalsFromBytes(tot[(k - 1) % 2].numpy())
-    fields = sol.Fields()
+    fields = sol.Fields(out=fields_host.numpy())
     t1 = time.perf_counter()
     pst = sol.Info().particle_steps - i0
     assert totals[1] > 0 and totals[0] >= totals[1]

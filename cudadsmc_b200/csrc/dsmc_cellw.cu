@@ -43,17 +43,22 @@ using namespace dev;
 constexpr uint32_t kWarpTile = 32;  // cells per warp tile, one per lane
 constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach the body
 
-template <int CAPW>
+// DIRECT: the order kernel reads each particle's state straight into
+// registers and stores it to its sorted slot (no shared-memory copy of the
+// state); only orig is staged.  Otherwise the state is gathered into shared
+// memory by asynchronous copies and written out after the pair counts.
+template <int CAPW, bool DIRECT = false>
 struct __align__(16) WarpSmem {
-  float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
+  static constexpr int kOrig = DIRECT ? 0 : 6;  // orig's row in part
+  float part[2][DIRECT ? 1 : 7][CAPW + 8];  // (x y z u v w) orig of a chunk, double buffered
   uint4 lbuf[2 * kWarpTile];   // light-cell list entries not yet in the global list
   uint32_t cr[kWarpTile];      // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
   unsigned long long mbar[2];
 };
 
-template <int CAPW, int WARPS>
+template <int CAPW, int WARPS, bool DIRECT = false>
 constexpr size_t collide_smem_bytes() {
-  return WARPS * sizeof(WarpSmem<CAPW>);
+  return WARPS * sizeof(WarpSmem<CAPW, DIRECT>);
 }
 
 // A tile of 32 cells as the lanes see it: lane L holds the start and end of
@@ -120,8 +125,9 @@ __device__ __forceinline__ WChunk make_wchunk(const WTile& T, uint32_t cur, int 
 // into buffer c.buf.  The library's buffers carry 16 bytes of slack, so the
 // whole 16-byte aligned cover of [base, base + n) is copied (at most CAPW + 6
 // elements).
-template <int CAPW>
-__device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>& S, const WChunk& c) {
+template <int CAPW, bool DIRECT>
+__device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW, DIRECT>& S,
+                                             const WChunk& c) {
   const uint32_t ia = c.base & ~3u, ib = (c.base + c.n + 3u) & ~3u;
   const uint32_t bytes = (ib - ia) * 4u;
   const uint32_t lane = lane_id();
@@ -129,7 +135,7 @@ __device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>
   __syncwarp();
   if (lane == 0) {
     fence_proxy_async();
-    bulk_g2s(S.part[c.buf][6], p.in_orig + ia, bytes, &S.mbar[c.buf]);
+    bulk_g2s(S.part[c.buf][WarpSmem<CAPW, DIRECT>::kOrig], p.in_orig + ia, bytes, &S.mbar[c.buf]);
   }
 }
 
@@ -216,11 +222,12 @@ __device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint
 
 // ---------------------------------------------------- order + pair counts ----
 
-template <int CAPW, int WARPS, int MINB>
+template <int CAPW, int WARPS, int MINB, bool DIRECT>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  WarpSmem<CAPW>& S = reinterpret_cast<WarpSmem<CAPW>*>(smem_raw)[warp];
+  using Smem = WarpSmem<CAPW, DIRECT>;
+  Smem& S = reinterpret_cast<Smem*>(smem_raw)[warp];
   const bool do_fixup = (p.flags & kDoFixup) != 0;
   const bool do_collide = (p.flags & kDoCollide) != 0;
   const bool taus = p.rng_kind == 0;
@@ -316,13 +323,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       }
     } else if (C.n > 0) {
       const uint32_t off = C.base & 3u;
-      float* X = S.part[C.buf][0] + off;
-      float* Y = S.part[C.buf][1] + off;
-      float* Z = S.part[C.buf][2] + off;
-      float* U = S.part[C.buf][3] + off;
-      float* V = S.part[C.buf][4] + off;
-      float* W = S.part[C.buf][5] + off;
-      const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][6] + off);
+      float* X = S.part[C.buf][DIRECT ? 0 : 0] + off;
+      float* Y = S.part[C.buf][DIRECT ? 0 : 1] + off;
+      float* Z = S.part[C.buf][DIRECT ? 0 : 2] + off;
+      float* U = S.part[C.buf][DIRECT ? 0 : 3] + off;
+      float* V = S.part[C.buf][DIRECT ? 0 : 4] + off;
+      float* W = S.part[C.buf][DIRECT ? 0 : 5] + off;
+      const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig] + off);
       const uint32_t base = C.base, n = C.n;
       // A: each particle's sorted position, sorted = (cell, orig), then the
       // gather of its state through orig straight to that position
@@ -330,7 +337,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       // The origs are distinct, so a particle's rank in its cell is the
       // number of smaller origs there (element j of the chunk sits at
       // ORA[j + off]).
-      const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][6]);
+      const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig]);
+      // DIRECT: the previous group's state, stored after this group's loads
+      // are issued (so that its load latency overlaps this group's rank)
+      float qx = 0.f, qy = 0.f, qz = 0.f, qu = 0.f, qv = 0.f, qw = 0.f;
+      uint32_t qpos = 0;
+      bool qval = false;
       if (do_fixup) {
         // Descents of orig inside the chunk.  A cell without one is in stable
         // order already (its particles took their tickets in one or a few
@@ -385,7 +397,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
             }
           }
         }
-        if (t < n) {
+        if (DIRECT) {
+          float lx = 0.f, ly = 0.f, lz = 0.f, lu = 0.f, lv = 0.f, lw = 0.f;
+          if (t < n) {
+            lx = __ldg(p.in.x + my); ly = __ldg(p.in.y + my); lz = __ldg(p.in.z + my);
+            lu = __ldg(p.in.u + my); lv = __ldg(p.in.v + my); lw = __ldg(p.in.w + my);
+          }
+          if (qval) {
+            const uint32_t g = base + qpos;
+            p.mid.x[g] = qx; p.mid.y[g] = qy; p.mid.z[g] = qz;
+            p.mid.u[g] = qu; p.mid.v[g] = qv; p.mid.w[g] = qw;
+          }
+          qx = lx; qy = ly; qz = lz; qu = lu; qv = lv; qw = lw;
+          qpos = pos;
+          qval = t < n;
+        } else if (t < n) {
           cp_async4(X + pos, p.in.x + my);
           cp_async4(Y + pos, p.in.y + my);
           cp_async4(Z + pos, p.in.z + my);
@@ -409,13 +435,23 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      cp_async_wait_all();
-      __syncwarp();
-      // C: the chunk, now in sorted order, to the mid arrays
-      for (uint32_t q = lane; q < n; q += 32) {
-        const uint32_t g = base + q;
-        p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
-        p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
+      if (DIRECT) {
+        // the last group's state
+        if (qval) {
+          const uint32_t g = base + qpos;
+          p.mid.x[g] = qx; p.mid.y[g] = qy; p.mid.z[g] = qz;
+          p.mid.u[g] = qu; p.mid.v[g] = qv; p.mid.w[g] = qw;
+        }
+        __syncwarp();
+      } else {
+        cp_async_wait_all();
+        __syncwarp();
+        // C: the chunk, now in sorted order, to the mid arrays
+        for (uint32_t q = lane; q < n; q += 32) {
+          const uint32_t g = base + q;
+          p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
+          p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
+        }
       }
     }
     __syncwarp();
@@ -784,20 +820,20 @@ struct LaunchShapeW {
   int per_sm = 0;
 };
 
-template <int CAPW, int WARPS, int MINB>
+template <int CAPW, int WARPS, int MINB, bool DIRECT = false>
 cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   LaunchShapeW& ls = cache[dev & 7];
-  const size_t smem = collide_smem_bytes<CAPW, WARPS>();
+  const size_t smem = collide_smem_bytes<CAPW, WARPS, DIRECT>();
   if (ls.device != dev) {
-    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB>,
+    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB, DIRECT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB, DIRECT>,
                                                       WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -808,7 +844,7 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  k_order_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
+  k_order_w<CAPW, WARPS, MINB, DIRECT><<<grid, WARPS * 32, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -904,16 +940,18 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 }  // namespace
 
 // Split variants (cell_kernel_variants() numbers them after the fused
-// CTA-wide ones): (particles per warp chunk, warps per CTA, register cap) of
-// the order kernel and the flight kernel's form (8 warps per CTA): 0 (256, 4,
-// 128; one particle per lane, 80 registers), 1 (128, 4, 128; one, 80), 2
-// (128, 8, 80; pairs, 80), 3 (128, 4, 80; pairs, 64).  The mesh kernel runs
-// at 64 registers (more warps to cover its chains of L2 loads).
-int cell_kernel_w_variants() { return 4; }
+// CTA-wide ones): (particles per warp chunk, warps per CTA, CTAs per SM the
+// registers are capped for) of the order kernel and the flight kernel's form
+// (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 4;
+// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs); 4-7 the order kernel's
+// direct form (state loaded into registers and stored to its sorted slot,
+// only orig staged in shared memory), one particle per lane in the flight
+// kernel: 4 (128, 4, 4), 5 (128, 4, 6), 6 (128, 8, 4), 7 (256, 4, 6).
+int cell_kernel_w_variants() { return 8; }
 
 int cell_kernel_w_capacity(int v) {
-  static const int caps[4] = {256, 128, 128, 128};
-  return caps[v < 0 || v > 3 ? 1 : v];
+  static const int caps[8] = {256, 128, 128, 128, 128, 128, 128, 256};
+  return caps[v < 0 || v > 7 ? 1 : v];
 }
 
 uint32_t cell_kernel_w_tile() { return kWarpTile; }
@@ -925,6 +963,10 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         case 0: return launch_order_w<256, 4, 4>(p, stream);
         case 2: return launch_order_w<128, 8, 3>(p, stream);
         case 3: return launch_order_w<128, 4, 6>(p, stream);
+        case 4: return launch_order_w<128, 4, 4, true>(p, stream);
+        case 5: return launch_order_w<128, 4, 6, true>(p, stream);
+        case 6: return launch_order_w<128, 8, 4, true>(p, stream);
+        case 7: return launch_order_w<256, 4, 6, true>(p, stream);
         default: return launch_order_w<128, 4, 4>(p, stream);
       }
     case 1:

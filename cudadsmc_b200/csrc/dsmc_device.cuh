@@ -105,6 +105,43 @@ using PhiloxStreamInline = PhiloxStreamT<true>;
 // (cvt.rzi.u32.f32: truncation, saturation, NaN -> 0).
 __device__ __forceinline__ uint32_t f2u(float f) { return (uint32_t)f; }
 
+// Loads of the body's geometry (triangle grid, planes, vertices, clearance
+// table) with the L2 eviction priority evict_last: these 10-20 MB are read
+// by a few percent of the particles every step, after streaming kernels have
+// passed several hundred MB through L2; with normal priority they were
+// evicted every step and each dependent step of a traversal paid a DRAM
+// round trip.
+__device__ __forceinline__ uint64_t l2_keep() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ float4 geo_ld(const float4* a) {
+  float4 r;
+  asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+      : "l"(a), "l"(l2_keep()));
+  return r;
+}
+__device__ __forceinline__ uint2 geo_ld(const uint2* a) {
+  uint2 r;
+  asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(r.x), "=r"(r.y) : "l"(a), "l"(l2_keep()));
+  return r;
+}
+__device__ __forceinline__ float geo_ld(const float* a) {
+  float r;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(a), "l"(l2_keep()));
+  return r;
+}
+__device__ __forceinline__ uint32_t geo_ld(const uint32_t* a) {
+  uint32_t r;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(a), "l"(l2_keep()));
+  return r;
+}
+__device__ __forceinline__ void geo_prefetch(const void* a) {
+  asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(a));
+}
+
 struct GridGeom {
   float3 gmin, gmax, cell;
   uint3 dim;
@@ -298,7 +335,7 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
       if (more) {
         // the walk's own stepping rule
         const uint32_t c = ((uint32_t)pidx[2] * g.dim.y + (uint32_t)pidx[1]) * g.dim.x + (uint32_t)pidx[0];
-        pse[k] = __ldg(&G.start_end[c]);
+        pse[k] = geo_ld(&G.start_end[c]);
         np = k + 1;
         const float texit = fminf(ptmax[0], fminf(ptmax[1], ptmax[2]));
         if (texit > t1) {
@@ -314,10 +351,10 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
 #pragma unroll
     for (int k = 0; k < kAhead; k++) {
       if (k < np && pse[k].x < pse[k].y) {
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(G.plane + pse[k].x));
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(G.tri + kTriStride * (size_t)pse[k].x));
+        geo_prefetch(G.plane + pse[k].x);
+        geo_prefetch(G.tri + kTriStride * (size_t)pse[k].x);
         if (kTriStride * (pse[k].y - pse[k].x) > 8u)  // stays inside the cell's entries
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(G.tri + kTriStride * (size_t)pse[k].x + 8));
+          geo_prefetch(G.tri + kTriStride * (size_t)pse[k].x + 8);
       }
     }
   }
@@ -326,13 +363,13 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
   const int max_iter = dm[0] + dm[1] + dm[2] + 3;
   for (int it = 0; it < max_iter; it++) {
     uint32_t c = ((uint32_t)idx[2] * g.dim.y + (uint32_t)idx[1]) * g.dim.x + (uint32_t)idx[0];
-    const uint2 se = __ldg(&G.start_end[c]);
+    const uint2 se = geo_ld(&G.start_end[c]);
     for (uint32_t i0 = se.x; i0 < se.y; i0 += 8) {
       // the planes of up to 8 of the cell's triangles in one round of loads
       float4 P[8];
 #pragma unroll
       for (int k = 0; k < 8; k++)
-        P[k] = i0 + k < se.y ? __ldg(&G.plane[i0 + k]) : make_float4(0.f, 0.f, 0.f, 1.f);
+        P[k] = i0 + k < se.y ? geo_ld(&G.plane[i0 + k]) : make_float4(0.f, 0.f, 0.f, 1.f);
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const uint32_t i = i0 + k;
@@ -343,9 +380,9 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
         const float s1 = fmaf(dist, dot_x(pn, d), s0);
         const float tol = __fmul_rn(1e-7f, fabsf(P[k].w) + 1.f);
         if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
-        float4 A = __ldg(&G.tri[kTriStride * (size_t)i]);
-        float4 B = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
-        float4 C = __ldg(&G.tri[kTriStride * (size_t)i + 2]);
+        float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
+        float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
+        float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
         float t;
         if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
                                    make_float3(C.x, C.y, C.z), &t) &&
@@ -396,12 +433,12 @@ __device__ __forceinline__ bool inside_mesh(const GeomView& G, float3 o) {
   for (int it = 0; it < max_iter; it++) {
     const uint32_t c = ((uint32_t)idx[2] * g.dim.y + (uint32_t)idx[1]) * g.dim.x + (uint32_t)idx[0];
     const float texit = fminf(tmax[0], fminf(tmax[1], tmax[2]));
-    if (__ldg(&G.flags[c]) != 0) {
-      const uint2 se = __ldg(&G.start_end[c]);
+    if (geo_ld(&G.flags[c]) != 0) {
+      const uint2 se = geo_ld(&G.start_end[c]);
       for (uint32_t i = se.x; i < se.y; i++) {
-        const float4 A = __ldg(&G.tri[kTriStride * (size_t)i]);
-        const float4 B = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
-        const float4 C = __ldg(&G.tri[kTriStride * (size_t)i + 2]);
+        const float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
+        const float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
+        const float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
         float t;
         if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
                                    make_float3(C.x, C.y, C.z), &t) &&
@@ -452,15 +489,15 @@ __device__ __forceinline__ float3 diffuse_emit(float3 n_out, float vstd, PhiloxS
 __device__ __forceinline__ bool collide_with_geometry(const GeomView& G, float3* pos, float3* vel,
                                                       float3* old_pos, uint32_t cellid,
                                                       PhiloxStream* rng) {
-  uint2 idx_stend = __ldg(&G.start_end[cellid]);
+  uint2 idx_stend = geo_ld(&G.start_end[cellid]);
   float3 dir = normalize3(*vel);
   float t, u, v;
   float dist = distance3(*old_pos, *pos);
   if (dist < kPathEps) return false;
   for (uint32_t i = idx_stend.x; i < idx_stend.y; i++) {
-    float4 a = __ldg(&G.tri[kTriStride * (size_t)i]);
-    float4 b = __ldg(&G.tri[kTriStride * (size_t)i + 1]);
-    float4 c = __ldg(&G.tri[kTriStride * (size_t)i + 2]);
+    float4 a = geo_ld(&G.tri[kTriStride * (size_t)i]);
+    float4 b = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
+    float4 c = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
     float3 v1 = make_float3(a.x, a.y, a.z), v2 = make_float3(b.x, b.y, b.z),
            v3 = make_float3(c.x, c.y, c.z);
     if (intersect_triangle(*old_pos, dir, v1, v2, v3, &t, &u, &v)) {

@@ -387,6 +387,35 @@ __global__ void k_sample_cells(const float* __restrict__ u, const float* __restr
   }
 }
 
+// Per-cell fields (n, ux, uy, uz, T), cell-major, from the FP64 sampling sums
+// (5 x cells, SoA) of ns passes: ProcessAndOutputStatistics' arithmetic
+// (kernels/dsmc_base.cu:104-163) in double with every rounding step explicit,
+// the same steps as the host code; with fields == 0 the sums themselves,
+// transposed to cell-major.
+__global__ void k_cell_fields(const double* __restrict__ acc, uint32_t cells, double fnum,
+                              double cell_volume, uint32_t ns, double mass, int fields,
+                              double* __restrict__ out) {
+  const double k3 = 3.0 * 1.3806e-23;
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+    const double N = acc[c], a1 = acc[(size_t)cells + c], a2 = acc[2 * (size_t)cells + c],
+                 a3 = acc[3 * (size_t)cells + c], a4 = acc[4 * (size_t)cells + c];
+    double* o = out + 5 * (size_t)c;
+    if (!fields) {
+      o[0] = N; o[1] = a1; o[2] = a2; o[3] = a3; o[4] = a4;
+      continue;
+    }
+    o[0] = ns ? __ddiv_rn(__dmul_rn(fnum, N), __dmul_rn(cell_volume, (double)ns)) : 0.0;
+    if (N > 0) {
+      const double ux = __ddiv_rn(a1, N), uy = __ddiv_rn(a2, N), uz = __ddiv_rn(a3, N);
+      const double u2 = __dadd_rn(__dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy)), __dmul_rn(uz, uz));
+      o[1] = ux; o[2] = uy; o[3] = uz;
+      o[4] = __ddiv_rn(__dmul_rn(mass, __dsub_rn(__ddiv_rn(a4, N), u2)), k3);
+    } else {
+      o[1] = o[2] = o[3] = o[4] = 0.0;
+    }
+  }
+}
+
 // ------------------------------------------------------------ init fill ----
 
 // Initial population: part_per_cell particles per cell at uniform positions
@@ -656,6 +685,13 @@ cudaError_t launch_bounds_reorder(const uint32_t* keys, const uint32_t* idx, uin
   const uint32_t grid = grid_for(n, 256, 8);
   k_bounds_reorder<<<grid, 256, 0, stream>>>(keys, idx, n, ncells, (uint2*)cse, s, d,
                                              (src && dst) ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cell_fields(const double* acc, uint32_t cells, double fnum, double cell_volume,
+                               uint32_t ns, double mass, int fields, double* out, cudaStream_t stream) {
+  k_cell_fields<<<grid_for(cells, 256, 8), 256, 0, stream>>>(acc, cells, fnum, cell_volume, ns, mass,
+                                                            fields, out);
   return cudaGetLastError();
 }
 

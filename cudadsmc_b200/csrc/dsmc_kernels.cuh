@@ -186,6 +186,10 @@ cudaError_t launch_bounds_reorder(const uint32_t* keys, const uint32_t* idx, uin
                                   uint32_t ncells, uint32_t* cse, const float* const src[6],
                                   float* const dst[6], cudaStream_t stream);
 // acc[field * fstride + cell * cstride] += sums (field 0..4: n, u, v, w, |v|^2)
+// Per-cell fields (or, with fields == 0, the sums) cell-major from the FP64
+// sampling sums.
+cudaError_t launch_cell_fields(const double* acc, uint32_t cells, double fnum, double cell_volume,
+                               uint32_t ns, double mass, int fields, double* out, cudaStream_t stream);
 cudaError_t launch_sample_cells(const float* u, const float* v, const float* w,
                                 const uint32_t* start, uint32_t cells, double* acc,
                                 size_t fstride, size_t cstride, cudaStream_t stream);

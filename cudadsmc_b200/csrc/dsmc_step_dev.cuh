@@ -521,13 +521,13 @@ __device__ __forceinline__ bool flight_may_meet_body(const StepParams& p, float3
     const uint32_t cc = coll_cell_id(G.cgrid, pos);
     if (cc != kNone) {
       const float dist = length3(make_float3(e.x - pos.x, e.y - pos.y, e.z - pos.z));
-      return !(dist < __ldg(&G.clear[cc]));
+      return !(dist < geo_ld(&G.clear[cc]));
     }
     return path_box_meets_grid(G.grid, pos, e);
   }
   const uint32_t sc = coll_cell_id(G.grid, pos);
   const uint32_t ec = coll_cell_id(G.grid, e);
-  return (sc != kNone && __ldg(&G.flags[sc]) != 0) || (ec != kNone && __ldg(&G.flags[ec]) != 0);
+  return (sc != kNone && geo_ld(&G.flags[sc]) != 0) || (ec != kNone && geo_ld(&G.flags[ec]) != 0);
 }
 
 // The boundaries after the flight: the reference's functors or the per-face
@@ -559,7 +559,7 @@ __device__ __forceinline__ bool move_free(const StepParams& p, float3& pos, floa
 // decision from it (the same arithmetic as flight_may_meet_body).
 __device__ __forceinline__ float defer_lookup(const StepParams& p, float3 pos) {
   const uint32_t cc = coll_cell_id(p.geom.cgrid, pos);
-  return cc == kNone ? -1.f : __ldg(&p.geom.clear[cc]);
+  return cc == kNone ? -1.f : geo_ld(&p.geom.clear[cc]);
 }
 __device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, float3 vel, float clr) {
   const float3 e = make_float3(pos.x + vel.x * p.dt, pos.y + vel.y * p.dt, pos.z + vel.z * p.dt);
@@ -596,7 +596,7 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
       // a path shorter than the start cell's clearance cannot reach the body
       if (!(pretested && b == 0)) {
         const uint32_t cc = coll_cell_id(G.cgrid, old_pos);
-        if (cc != kNone && dist < __ldg(&G.clear[cc])) break;
+        if (cc != kNone && dist < geo_ld(&G.clear[cc])) break;
         // a path outside the geometry grid whose box misses the grid's box
         if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
       }
@@ -605,7 +605,7 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
       float t;
       uint32_t e;
       if (!nearest_wall_hit(G, old_pos, d, dist, &t, &e)) break;
-      const float4 P = __ldg(&G.plane[e]);
+      const float4 P = geo_ld(&G.plane[e]);
       const float3 n = make_float3(P.x, P.y, P.z);
       // the mesh is closed with outward normals: a face reached from its
       // back side holds a particle inside the body (left over from a fill of
@@ -639,11 +639,11 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
       st_cubid = coll_cell_id(G.grid, old_pos);
       end_cubid = coll_cell_id(G.grid, pos);
       if (st_cubid != kNone) {
-        if (__ldg(&G.flags[st_cubid]) != 0)
+        if (geo_ld(&G.flags[st_cubid]) != 0)
           collProcessed = collide_with_geometry(G, &pos, &vel, &old_pos, st_cubid, &rng);
       }
       if (!collProcessed && st_cubid != end_cubid && end_cubid != kNone) {
-        if (__ldg(&G.flags[end_cubid]) != 0)
+        if (geo_ld(&G.flags[end_cubid]) != 0)
           collProcessed = collide_with_geometry(G, &pos, &vel, &old_pos, end_cubid, &rng);
       }
     } while (collProcessed && i++ < kCollisionLimit);

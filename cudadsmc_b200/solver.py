@@ -143,9 +143,10 @@ class DSMCSolver:
         return v.value, cap.value
 
     def Autotune(self, dt, steps=10):
-        """Times every cell-kernel variant on real timesteps (the run advances
-        by KernelVariantCount() * (steps + 2) steps) and keeps the fastest;
-        returns (best, ms per step of each variant)."""
+        """Times every split cell-kernel variant (4 and up) on real timesteps
+        (the run advances by (KernelVariantCount() - 4) * (steps + 2) steps)
+        and keeps the fastest; returns (best, ms per step of each variant, 0
+        for the fused variants 0-3, which are not timed)."""
         best = ctypes.c_int(0)
         ms = np.zeros(KernelVariantCount(), np.float32)
         self._check(lib().dsmc_autotune(self.h, dt, int(steps), ctypes.byref(best), _ptr(ms)),
@@ -176,9 +177,13 @@ class DSMCSolver:
         self._check(lib().dsmc_read_cell_sums(self.h, _ptr(s), ctypes.byref(ns)), "SampleStatistics")
         return s, self.Totals(), ns.value
 
-    def Fields(self):
-        """Per-cell n, ux, uy, uz, T [cells, 5] from the FP64 samples."""
-        f = np.zeros((self.settings.getCellsCount(), 5), np.float64)
+    def Fields(self, out=None):
+        """Per-cell n, ux, uy, uz, T [cells, 5] from the FP64 samples (into
+        `out`, a C-contiguous float64 array of that shape, when given: pinned
+        host memory makes the copy faster)."""
+        f = out if out is not None else np.zeros((self.settings.getCellsCount(), 5), np.float64)
+        if f.dtype != np.float64 or f.size != 5 * self.settings.getCellsCount() or not f.flags.c_contiguous:
+            raise ValueError("Fields(out=...) needs a C-contiguous float64 array of cells x 5")
         self._check(lib().dsmc_read_fields(self.h, _ptr(f)), "Fields")
         return f
 

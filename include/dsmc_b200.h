@@ -255,9 +255,11 @@ int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps);
 /* Launch shape of the step's cell kernel (no counterpart in the reference,
  * whose kernels use fixed block sizes).  Variants 0-3 are a CTA-wide kernel:
  * 0 = 512 threads per CTA and up to 2048 particles per shared-memory chunk,
- * 1 = 256/1024, 2 = 128/512, 3 = 64/256.  Variants 4-7 are a kernel whose
- * warps each work through their own tiles of 32 cells, with chunks of up to
- * 256 (4) or 128 (5-7) particles per warp; 5 is the default.  Results do not
+ * 1 = 256/1024, 2 = 128/512, 3 = 64/256.  Variants 4-11 are split kernels
+ * whose warps each work through their own tiles of 32 cells, with chunks of
+ * up to 256 (4, 11) or 128 (5-10) particles per warp; 8-11 load each
+ * particle's state into registers and store it to its sorted slot, 4-7
+ * stage it in shared memory; 5 is the default.  Results do not
  * depend on the variant, except in the Philox mode for a cell holding more
  * particles than the chunk (it is then collided by one thread instead of one
  * warp, a different but equivalent stream of draws).  Changing it drops the
@@ -267,10 +269,11 @@ int dsmc_get_kernel_variant(dsmc_handle* h, int* variant, int* chunk_capacity);
 /* Number of cell-kernel variants (valid variants are 0 .. count-1). */
 int dsmc_kernel_variant_count(void);
 /* Times `steps` graph-replayed timesteps (after 2 warm-up steps) of every
- * variant and keeps the fastest.  These are real timesteps of the run: the
- * simulation advances by count * (steps + 2) steps, count =
- * dsmc_kernel_variant_count().  ms_per_step (optional) receives count times
- * in milliseconds.  Blocks until done. */
+ * split variant (4 .. count-1, count = dsmc_kernel_variant_count()) and keeps
+ * the fastest.  These are real timesteps of the run: the simulation advances
+ * by (count - 4) * (steps + 2) steps.  ms_per_step (optional) receives count
+ * times in milliseconds (0 for the fused variants 0-3, which are not timed).
+ * Blocks until done. */
 int dsmc_autotune(dsmc_handle* h, float dt, int steps, int* best, float* ms_per_step);
 
 /* Batches (no counterpart in the reference, which runs one solver per
@@ -293,7 +296,7 @@ int dsmc_batch_set_stream(dsmc_batch* b, void* stream);
 int dsmc_batch_step(dsmc_batch* b, const float* dt, int nsteps);
 /* Synchronises the batch stream and reports the members' device error flags. */
 int dsmc_batch_sync(dsmc_batch* b);
-/* dsmc_autotune for every member (each advances by count * (steps + 2) steps);
+/* dsmc_autotune for every member (each advances by (count - 4) * (steps + 2) steps);
  * variants (optional) receives the chosen variant per member. */
 int dsmc_batch_autotune(dsmc_batch* b, const float* dt, int steps, int* variants);
 

@@ -128,10 +128,9 @@ def test_collide_philox_matches_oracle(cuda, omega):
     assert np.array_equal(mr_g[:, 1], mr_o[:, 1])
     ok = ~tie
     assert np.array_equal(st[ok, 1].astype(np.int64), info[ok, 1].astype(np.int64))
-    if abs(omega - 0.5) < 1e-9:
-        assert np.array_equal(mr_g[:, 0], mr_o[:, 0])
-    else:
-        assert np.allclose(mr_g[ok, 0], mr_o[ok, 0], rtol=4e-6, atol=0)
+    # (sigma g)max: the largest sigma g of the pass, from velocities that
+    # earlier collisions of the cell left an ulp apart
+    assert np.allclose(mr_g[ok, 0], mr_o[ok, 0], rtol=4e-6, atol=0)
     slot_ok = np.repeat(ok, counts)
     # relative to the velocity scale of the particle's cell (the rms speed
     # there before the pass: a collision rounds on that scale, whatever the
@@ -320,7 +319,7 @@ def test_inflow_injection_matches_oracle(cuda):
     sol.close()
 
 
-@pytest.mark.parametrize("variant", [5, 0])
+@pytest.mark.parametrize("variant", [5, 9, 0])
 def test_step_matches_oracle(cuda, variant):
     """Whole timesteps of a sphere flow in the capsule workload's mode: the
     GPU steps 12 times to develop the flow, then each of three more steps is
