@@ -113,11 +113,15 @@ SIGNATURES = [
     ("dsmc_read_keys", _I, [_P, _P, ctypes.POINTER(_U32)]),
     ("dsmc_set_cell_state", _I, [_P, _P, _P]),
     ("dsmc_get_cell_state", _I, [_P, _P, _P]),
+    ("dsmc_set_twisters", _I, [_P, _P, _P, _I]),
+    ("dsmc_get_twisters", _I, [_P, _P]),
+    ("dsmc_read_twisters", _I, [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_uint32, _P]),
     ("dsmc_step", _I, [_P, ctypes.c_float, _I]),
     ("dsmc_step_graph", _I, [_P, ctypes.c_float, _I]),
     ("dsmc_init_from_fields", _I, [_P, _P, _P]),
     ("dsmc_gemm_bf16", _I, [_I, _I, _I, _P, _I, _I, _P, _I, _I, _P, _I, ctypes.c_float, _P, _I, _P,
                             _I, _I, _P]),
+    ("dsmc_gemm_check", _I, [_P]),
     ("dsmc_gelu_backward", _I, [_P, _P, _P, _P, ctypes.c_size_t, _P]),
     ("dsmc_colsum", _I, [_P, _I, _I, _I, _P, _P]),
     ("dsmc_mse_grad", _I, [_P, _P, ctypes.c_size_t, ctypes.c_float, _P, _P, _P, _P, _P]),

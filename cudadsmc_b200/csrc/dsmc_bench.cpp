@@ -7,6 +7,9 @@
 //   -move X Y Z           translate the mesh (reference: 0 0 -3)
 //   -steps N              run N steps instead of -run-for
 //   -stats FILE           statistics output (default statistics.txt)
+//   -mt                   the reference's Mersenne-Twister collisions, twister
+//                         records from data/MersenneTwister.dat (the reference's path)
+//   -mt-file FILE         another twister parameter file
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -19,8 +22,22 @@
 
 int main(int argc, char** argv) {
   try {
+    // -mt and -mt-file are taken here; the settings parser sees the rest
+    bool mt = false;
+    std::string mt_file = "data/MersenneTwister.dat";
+    std::vector<char*> rest;
+    for (int i = 0; i < argc; i++) {
+      if (i > 0 && !strcmp(argv[i], "-mt")) {
+        mt = true;
+      } else if (i > 0 && !strcmp(argv[i], "-mt-file") && i + 1 < argc) {
+        mt = true;
+        mt_file = argv[++i];
+      } else {
+        rest.push_back(argv[i]);
+      }
+    }
     dsmc_b200::settings_t s;
-    s.readFromCmdLine(argc, argv);
+    s.readFromCmdLine((int)rest.size(), rest.data());
     std::string raw, stats = "statistics.txt";
     bool ico = false;
     float ico_r = 0.1f, ico_c[3] = {0, 0, 0}, mv[3] = {0, 0, 0};
@@ -72,6 +89,7 @@ int main(int argc, char** argv) {
     cudaEventCreate(&b);
     cudaEventRecord(a);
     uint32_t n = solver.InitSystemState(s.cfg.stream_vel);
+    if (mt) solver.UseTwisters(mt_file.c_str());
     cudaEventRecord(b);
     cudaEventSynchronize(b);
     float ms = 0;

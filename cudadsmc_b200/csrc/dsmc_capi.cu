@@ -37,6 +37,11 @@ struct dsmc_handle {
   uint32_t* tile_sum = nullptr;
   float2* maxrem = nullptr;
   uint4* seeds = nullptr;
+  // -mt mode (dsmc_set_twisters): per cell a Mersenne Twister, 21 state
+  // words and one parameter record; the NTC selections draw from it
+  uint32_t* mt_state = nullptr;
+  uint4* mt_cfg = nullptr;
+  bool mt_on = false;
   double* acc = nullptr;
   double* cellbuf = nullptr;  // per-cell fields / sums, cell-major, for readback (on first use)
   Meta* meta = nullptr;
@@ -171,8 +176,11 @@ void free_all(dsmc_handle* h) {
   }
   void* ps[] = {h->orig, h->ntc_list, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
                 h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse,
-                h->gtri, h->gplane};
+                h->gtri, h->gplane, h->mt_state, h->mt_cfg};
   for (void* p : ps) cudaFree(p);
+  h->mt_state = nullptr;
+  h->mt_cfg = nullptr;
+  h->mt_on = false;
 }
 
 SoA soa_of(float* const a[6]) { return SoA{a[0], a[1], a[2], a[3], a[4], a[5]}; }
@@ -375,6 +383,7 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
     static const int slot[5] = {2, 7, 4, 5, 6};
     for (int stage = 0; stage < 5; stage++) {
       e = timed(h, slot[stage], [&] {
+        if (stage == 1 && h->mt_on) return dsmcb::launch_ntc_mt(p, h->mt_state, h->mt_cfg, h->stream);
         return dsmcb::launch_split_stage(p, h->variant - 4, stage, h->stream);
       });
       if (e) return e;
@@ -388,6 +397,9 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
     }
     if (fork) return cudaStreamWaitEvent(h->stream, h->ev_join, 0);
   } else {
+    // the -mt selections exist for the split kernels only (dsmc_set_twisters
+    // selects one)
+    if (h->mt_on) return cudaErrorInvalidValue;
     e = timed(h, 2, [&] { return dsmcb::launch_cell(p, h->stream); });
     if (e) return e;
   }
@@ -1189,6 +1201,70 @@ int dsmc_get_cell_state(dsmc_handle* h, float* maxrem, uint32_t* seeds) {
   return DSMC_OK;
 }
 
+// InitGPUTwisters + InitMersenneTwisters (kernels/mtwister.cu:46-68,
+// kernels/dsmc_kernel.cu:548-569) and InitMaximums (:1104-1120) for the
+// handle's cells; the -mt collisions (ComputeBirdCollisionsDev, :1002-1089)
+// from then on.
+int dsmc_set_twisters(dsmc_handle* h, const uint32_t* cfg4, const uint32_t* state21,
+                      int init_maximums) {
+  if (!h || !cfg4) return DSMC_ERR_ARG;
+  if (h->cfg.rng != DSMC_RNG_TAUS)
+    return fail(h, DSMC_ERR_CONFIG, "the -mt collisions replace the reference RNG mode (rng taus)");
+  if (state21)
+    for (uint32_t c = 0; c < h->cells; c++)
+      if (state21[21 * (size_t)c] >= 19u)
+        return fail(h, DSMC_ERR_ARG, "twister state: iState must be below 19");
+  if (!h->mt_state) {
+    CK(h, cudaMalloc(&h->mt_state, (size_t)h->cells * 21 * sizeof(uint32_t)), "twister states");
+    CK(h, cudaMalloc(&h->mt_cfg, (size_t)h->cells * sizeof(uint4)), "twister parameters");
+  }
+  CK(h, cudaMemcpyAsync(h->mt_cfg, cfg4, (size_t)h->cells * sizeof(uint4), cudaMemcpyHostToDevice,
+                        h->stream), "twister parameters");
+  if (init_maximums) {
+    // the reference's order (include/gpu_dsmc.inl:363-367): InitBirdData's
+    // InitMaximums draws from the twister states before InitMersenneTwisters
+    // initialises them, i.e. from zeroed states, so every remainder is
+    // (0 + 1) / 2^32
+    CK(h, cudaMemsetAsync(h->mt_state, 0, (size_t)h->cells * 21 * sizeof(uint32_t), h->stream),
+       "twister states");
+    CK(h, dsmcb::launch_mt_maximums(h->mt_cfg, h->mt_state, h->maxrem, h->max_rel_vel, h->cells,
+                                    h->stream), "InitMaximums");
+  }
+  if (state21)
+    CK(h, cudaMemcpyAsync(h->mt_state, state21, (size_t)h->cells * 21 * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice, h->stream), "twister states");
+  else
+    CK(h, dsmcb::launch_mt_init(h->mt_cfg, h->mt_state, h->cells, h->stream), "twister init");
+  CK(h, cudaStreamSynchronize(h->stream), "twisters");
+  if (!dsmcb::cell_kernel_is_warp(h->variant)) apply_variant(h, 5);
+  h->mt_on = true;
+  drop_graph(h);
+  return DSMC_OK;
+}
+
+int dsmc_read_twisters(const char* path, uint32_t seed, uint32_t count, uint32_t* cfg4) {
+  if (!path || (count && !cfg4)) return DSMC_ERR_ARG;
+  std::ifstream f(path, std::ios::binary);
+  if (!f) return DSMC_ERR_IO;
+  f.read(reinterpret_cast<char*>(cfg4), (std::streamsize)count * 16);
+  if (!f) return DSMC_ERR_IO;
+  uint64_t s = seed;
+  for (uint32_t i = 0; i < count; i++) {
+    s = (s * 279470273ull) % 4294967291ull;
+    cfg4[4 * (size_t)i + 3] = (uint32_t)s;
+  }
+  return DSMC_OK;
+}
+
+int dsmc_get_twisters(dsmc_handle* h, uint32_t* state21) {
+  if (!h || !state21) return DSMC_ERR_ARG;
+  if (!h->mt_on) return fail(h, DSMC_ERR_STATE, "no twisters set (dsmc_set_twisters)");
+  CK(h, cudaStreamSynchronize(h->stream), "sync");
+  CK(h, cudaMemcpy(state21, h->mt_state, (size_t)h->cells * 21 * sizeof(uint32_t),
+                   cudaMemcpyDeviceToHost), "twister states");
+  return DSMC_OK;
+}
+
 int dsmc_step(dsmc_handle* h, float dt, int nsteps) {
   if (!h || nsteps < 0) return DSMC_ERR_ARG;
   if (!h->has_state) return fail(h, DSMC_ERR_STATE, "dsmc_step before dsmc_init_state/upload");
@@ -1270,6 +1346,8 @@ int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps) {
 
 int dsmc_set_kernel_variant(dsmc_handle* h, int variant) {
   if (!h || variant < 0 || variant >= dsmcb::cell_kernel_variants()) return DSMC_ERR_ARG;
+  if (h->mt_on && !dsmcb::cell_kernel_is_warp(variant))
+    return fail(h, DSMC_ERR_CONFIG, "the -mt collisions run with the split kernels (variants 4 and up)");
   apply_variant(h, variant);
   return DSMC_OK;
 }

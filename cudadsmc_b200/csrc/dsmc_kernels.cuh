@@ -186,6 +186,15 @@ cudaError_t launch_bounds_reorder(const uint32_t* keys, const uint32_t* idx, uin
                                   uint32_t ncells, uint32_t* cse, const float* const src[6],
                                   float* const dst[6], cudaStream_t stream);
 // acc[field * fstride + cell * cstride] += sums (field 0..4: n, u, v, w, |v|^2)
+// The -mt collisions (dsmc_mt.cu): twister set-up (InitTwisterFast for
+// twisters [0, n)), InitMaximums, and the NTC selections of the listed cells
+// drawn from each cell's twister in place of k_ntc_w's.
+cudaError_t launch_mt_init(const uint4* cfg, uint32_t* state, uint32_t n, cudaStream_t stream);
+cudaError_t launch_mt_maximums(const uint4* cfg, uint32_t* state, float2* maxrem, float max_rel_vel,
+                               uint32_t n, cudaStream_t stream);
+cudaError_t launch_ntc_mt(const StepParams& p, uint32_t* mt_state, const uint4* mt_cfg,
+                          cudaStream_t stream);
+
 // Per-cell fields (or, with fields == 0, the sums) cell-major from the FP64
 // sampling sums.
 cudaError_t launch_cell_fields(const double* acc, uint32_t cells, double fnum, double cell_volume,

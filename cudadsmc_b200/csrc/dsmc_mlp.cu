@@ -8,12 +8,16 @@
 #include <cstdint>
 
 #include "dsmc_b200.h"
+#include "dsmc_bulk.cuh"
+#include "dsmc_umma.cuh"
+
+// Set by a GEMM whose wait on its tensor-core work ran out (a second);
+// dsmc_gemm_check reports and clears it.
+__device__ unsigned int g_gemm_failed = 0;
 
 namespace {
 
 using bf16 = __nv_bfloat16;
-
-constexpr int kBM = 128, kBN = 128, kBK = 32, kPadK = 40;
 
 struct GemmArgs {
   int m, n, k;
@@ -28,7 +32,7 @@ struct GemmArgs {
   int act;  // 0 none, 1 GELU
   bf16* cb;
   int ldcb;
-  int kchunk;  // K range per blockIdx.z (multiple of kBK)
+  int kchunk;  // K range per blockIdx.z (multiple of the tile's K step)
 };
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678f)); }
@@ -36,122 +40,123 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return 0.5f * (1.f + erff(z * 0.70710678f)) + z * 0.39894228f * expf(-0.5f * z * z);
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+// Operand tile of rows [r0, r0 + 128) and k in [k0, k0 + 64) into `dst`:
+// TRANS false - stored rows x k (k contiguous, K-major in shared memory);
+// TRANS true - stored k x rows (rows contiguous, MN-major).
+template <bool TRANS>
+__device__ __forceinline__ void umma_load_tile(const bf16* src, int ld, int rows, int r0, int k0, int kend,
+                                               bf16* dst) {
+  using namespace dsmcb::umma;
+  unsigned char* d = reinterpret_cast<unsigned char*>(dst);
+  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+  for (int it = 0; it < (kBM * kBK / 8) / kThreads; it++) {
+    const int c = threadIdx.x + it * kThreads;
+    if (!TRANS) {
+      const int r = c >> 3, kc = c & 7;
+      const int gr = r0 + r, gk = k0 + kc * 8;
+      uint4 v = zero;
+      if (gr < rows && gk < kend) v = *reinterpret_cast<const uint4*>(src + (size_t)gr * ld + gk);
+      *reinterpret_cast<uint4*>(d + kmajor_off((uint32_t)r, (uint32_t)(kc * 8))) = v;
+    } else {
+      const int kk = c >> 4, rc = c & 15;
+      const int gk = k0 + kk, gr = r0 + rc * 8;
+      uint4 v = zero;
+      if (gk < kend && gr < rows) v = *reinterpret_cast<const uint4*>(src + (size_t)gk * ld + gr);
+      *reinterpret_cast<uint4*>(d + mnmajor_off((uint32_t)(rc * 8), (uint32_t)kk)) = v;
+    }
+  }
 }
 
-// C[m x n] (+)= A[m x k] B[k x n].  AT: A is stored k x m (row-major), so the
-// product uses its transpose; BT: B is stored n x k.  A 128x128 tile per CTA,
-// 8 warps of 64x32, K in steps of 32 through shared memory ([m][k] and [n][k]
-// so that every fragment pair is one 32-bit load).
+// C [m x n] (+)= A [m x k] B [k x n] on the tensor cores (tcgen05.mma, the
+// accumulator in TMEM): see dsmc_umma.cuh for the tile, the stages and the
+// operand layouts.  AT: A is stored k x m (row-major), so the product uses
+// its transpose; BT: B is stored n x k.
 template <bool AT, bool BT>
-__global__ void __launch_bounds__(256) k_gemm(const GemmArgs g) {
-  __shared__ __align__(16) bf16 As[kBM][kPadK];
-  __shared__ __align__(16) bf16 Bs[kBN][kPadK];
+__global__ void __launch_bounds__(dsmcb::umma::kThreads, 1) k_gemm_tc(const GemmArgs g) {
+  using namespace dsmcb::umma;
+  using namespace dsmcb::dev;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem& S = *reinterpret_cast<Smem*>(smem_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
   const int kbeg = blockIdx.z * g.kchunk;
   const int kend = min(g.k, kbeg + g.kchunk);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 2, wn = warp & 3;
-  float acc[4][4][4];
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
-  const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
-
-  for (int kb = kbeg; kb < kend; kb += kBK) {
-#pragma unroll
-    for (int it = 0; it < 2; it++) {
-      const int idx = tid + it * 256;
-      if (!AT) {
-        const int r = idx >> 2, kv = (idx & 3) * 8;
-        const int gm = m0 + r, gk = kb + kv;
-        uint4 v = zero;
-        if (gm < g.m && gk < kend) v = *reinterpret_cast<const uint4*>(g.a + (size_t)gm * g.lda + gk);
-        *reinterpret_cast<uint4*>(&As[r][kv]) = v;
-      } else {
-        const int kk = idx >> 4, mv = (idx & 15) * 8;
-        const int gk = kb + kk, gm = m0 + mv;
-        uint4 v = zero;
-        if (gk < kend && gm < g.m) v = *reinterpret_cast<const uint4*>(g.a + (size_t)gk * g.lda + gm);
-        const bf16* e = reinterpret_cast<const bf16*>(&v);
-#pragma unroll
-        for (int j = 0; j < 8; j++) As[mv + j][kk] = e[j];
-      }
-      if (BT) {
-        const int r = idx >> 2, kv = (idx & 3) * 8;
-        const int gn = n0 + r, gk = kb + kv;
-        uint4 v = zero;
-        if (gn < g.n && gk < kend) v = *reinterpret_cast<const uint4*>(g.b + (size_t)gn * g.ldb + gk);
-        *reinterpret_cast<uint4*>(&Bs[r][kv]) = v;
-      } else {
-        const int kk = idx >> 4, nv = (idx & 15) * 8;
-        const int gk = kb + kk, gn = n0 + nv;
-        uint4 v = zero;
-        if (gk < kend && gn < g.n) v = *reinterpret_cast<const uint4*>(g.b + (size_t)gk * g.ldb + gn);
-        const bf16* e = reinterpret_cast<const bf16*>(&v);
-#pragma unroll
-        for (int j = 0; j < 8; j++) Bs[nv + j][kk] = e[j];
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < kBK; kk += 16) {
-      uint32_t af[4][4], bfr[4][2];
-      const int c = kk + (lane & 3) * 2;
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int r = wm * 64 + i * 16 + (lane >> 2);
-        af[i][0] = *reinterpret_cast<const uint32_t*>(&As[r][c]);
-        af[i][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][c]);
-        af[i][2] = *reinterpret_cast<const uint32_t*>(&As[r][c + 8]);
-        af[i][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][c + 8]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int nn = wn * 32 + j * 8 + (lane >> 2);
-        bfr[j][0] = *reinterpret_cast<const uint32_t*>(&Bs[nn][c]);
-        bfr[j][1] = *reinterpret_cast<const uint32_t*>(&Bs[nn][c + 8]);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], af[i], bfr[j]);
-    }
-    __syncthreads();
+  const int ktiles = (kend - kbeg + kBK - 1) / kBK;
+  if (tid == 0) {
+    mbar_init(&S.mbar[0], 1);
+    mbar_init(&S.mbar[1], 1);
+    fence_mbar_init();
   }
-
+  if (warp == 0) tmem_alloc(&S.tmem_base, kTmemCols);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = S.tmem_base;
+  const uint32_t idesc = instr_desc(AT ? 1u : 0u, BT ? 0u : 1u);
+  uint32_t phase0 = 0, phase1 = 0;  // parity of each stage's next completion
+  bool ok = true;
+  for (int kt = 0; kt < ktiles; kt++) {
+    const int s = kt & 1;
+    // the stage's MMAs of tile kt - 2 must have read it before it is refilled
+    if (kt >= 2) {
+      uint32_t& ph = s ? phase1 : phase0;
+      ok = mbar_wait_bounded(&S.mbar[s], ph) && ok;
+      ph ^= 1u;
+    }
+    const int k0 = kbeg + kt * kBK;
+    umma_load_tile<AT>(g.a, g.lda, g.m, m0, k0, kend, S.a[s]);
+    umma_load_tile<!BT>(g.b, g.ldb, g.n, n0, k0, kend, S.b[s]);
+    fence_proxy_async();  // the tiles, written by the generic proxy, are read by the tensor cores
+    __syncthreads();
+    if (tid == 0) {
+      fence_after_sync();
+      const uint32_t a0 = su32(S.a[s]), b0 = su32(S.b[s]);
+#pragma unroll
+      for (int j = 0; j < kBK / 16; j++)
+        mma(tmem, smem_desc(a0 + 2u * kLbo * j), smem_desc(b0 + 2u * kLbo * j), idesc,
+            (kt > 0 || j > 0) ? 1u : 0u);
+      commit(&S.mbar[s]);
+    }
+  }
+  // the last commit completes after every MMA of the tile
+  {
+    const int sl = (ktiles - 1) & 1;
+    ok = mbar_wait_bounded(&S.mbar[sl], sl ? phase1 : phase0) && ok;
+  }
+  fence_after_sync();
   const bool split = gridDim.z > 1;
+  const int row = m0 + 32 * warp + lane;
+#pragma unroll 1
+  for (int q = 0; q < kBN / 32; q++) {
+    float v[32];
+    ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(32 * q), v);
+    if (row >= g.m) continue;
 #pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const int row = m0 + wm * 64 + i * 16 + (lane >> 2) + (h >> 1) * 8;
-        const int col = n0 + wn * 32 + j * 8 + (lane & 3) * 2 + (h & 1);
-        if (row >= g.m || col >= g.n) continue;
-        const float v = acc[i][j][h];
-        if (split) {
-          atomicAdd(&g.c[(size_t)row * g.ldc + col], v);
-          continue;
-        }
-        float z = v;
-        if (g.bias) z += g.bias[col];
-        if (g.c) {
-          float* cp = &g.c[(size_t)row * g.ldc + col];
-          if (g.beta != 0.f) z += g.beta * *cp;
-          *cp = z;
-        }
-        if (g.cb) g.cb[(size_t)row * g.ldcb + col] = __float2bfloat16(g.act == 1 ? gelu(z) : z);
+    for (int j = 0; j < 32; j++) {
+      const int col = n0 + 32 * q + j;
+      if (col >= g.n) continue;
+      if (split) {
+        atomicAdd(&g.c[(size_t)row * g.ldc + col], v[j]);
+        continue;
       }
+      float z = v[j];
+      if (g.bias) z += g.bias[col];
+      if (g.c) {
+        float* cp = &g.c[(size_t)row * g.ldc + col];
+        if (g.beta != 0.f) z += g.beta * *cp;
+        *cp = z;
+      }
+      if (g.cb) g.cb[(size_t)row * g.ldcb + col] = __float2bfloat16(g.act == 1 ? gelu(z) : z);
+    }
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after_sync();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+  if (!ok && tid == 0) atomicOr(&g_gemm_failed, 1u);
 }
 
 __global__ void k_gelu_backward(const float* z, const float* dh, float* dz, bf16* dzb, size_t n) {
@@ -240,6 +245,24 @@ unsigned grid_1d(size_t n) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
+// Shared memory per CTA: the tiles, padded to kTcSmemReserve so that every
+// address a descriptor of this kernel can form stays inside the allocation.
+constexpr int kTcSmemReserve = 200 * 1024;
+
+template <bool AT, bool BT>
+void launch_tc(dim3 grid, const GemmArgs& g, cudaStream_t s) {
+  static bool attr = false;
+  const int smem = (int)sizeof(dsmcb::umma::Smem) > kTcSmemReserve ? (int)sizeof(dsmcb::umma::Smem)
+                                                                   : kTcSmemReserve;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_gemm_tc<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+      return;
+    attr = true;
+  }
+  k_gemm_tc<AT, BT><<<grid, dsmcb::umma::kThreads, smem, s>>>(g);
+}
+
 }  // namespace
 
 extern "C" {
@@ -260,17 +283,30 @@ int dsmc_gemm_bf16(int m, int n, int k, const void* a, int lda, int a_trans, con
   g.c = c; g.ldc = ldc; g.beta = beta;
   g.bias = bias; g.act = act;
   g.cb = static_cast<bf16*>(c_bf16); g.ldcb = ldcb;
+  using dsmcb::umma::kBK;
+  using dsmcb::umma::kBM;
+  using dsmcb::umma::kBN;
   const int ksteps = (k + kBK - 1) / kBK;
   const int per = (ksteps + split_k - 1) / split_k;
   g.kchunk = per * kBK;
   const int splits = (k + g.kchunk - 1) / g.kchunk;
   const dim3 grid((n + kBN - 1) / kBN, (m + kBM - 1) / kBM, splits);
   cudaStream_t s = (cudaStream_t)stream;
-  if (!a_trans && !b_trans) k_gemm<false, false><<<grid, 256, 0, s>>>(g);
-  else if (!a_trans && b_trans) k_gemm<false, true><<<grid, 256, 0, s>>>(g);
-  else if (a_trans && !b_trans) k_gemm<true, false><<<grid, 256, 0, s>>>(g);
-  else k_gemm<true, true><<<grid, 256, 0, s>>>(g);
+  if (!a_trans && !b_trans) launch_tc<false, false>(grid, g, s);
+  else if (!a_trans && b_trans) launch_tc<false, true>(grid, g, s);
+  else if (a_trans && !b_trans) launch_tc<true, false>(grid, g, s);
+  else launch_tc<true, true>(grid, g, s);
   return cudaGetLastError() == cudaSuccess ? DSMC_OK : DSMC_ERR_CUDA;
+}
+
+int dsmc_gemm_check(void* stream) {
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return DSMC_ERR_CUDA;
+  unsigned int f = 0;
+  if (cudaMemcpyFromSymbol(&f, g_gemm_failed, sizeof(f)) != cudaSuccess) return DSMC_ERR_CUDA;
+  if (!f) return DSMC_OK;
+  f = 0;
+  if (cudaMemcpyToSymbol(g_gemm_failed, &f, sizeof(f)) != cudaSuccess) return DSMC_ERR_CUDA;
+  return DSMC_ERR_DEVICE;
 }
 
 int dsmc_gelu_backward(const float* z, const float* dh, float* dz, void* dz_bf16, size_t n,

@@ -283,6 +283,22 @@ class DSMCSolver:
         self._check(lib().dsmc_read_keys(self.h, _ptr(k), ctypes.byref(n2)), "ReadKeys")
         return k
 
+    def SetTwisters(self, cfg4, state21=None, init_maximums=False):
+        """The -mt collisions (ComputeBirdCollisionsDev): cfg4 (cells, 4)
+        twister records (read_twisters), state21 (cells, 21) twister states or
+        None to initialise them from their seeds; init_maximums also sets
+        (sigma g)max and draws the remainders from the twisters
+        (InitMaximums)."""
+        c = np.ascontiguousarray(cfg4, np.uint32)
+        st = None if state21 is None else np.ascontiguousarray(state21, np.uint32)
+        self._check(lib().dsmc_set_twisters(self.h, _ptr(c), _ptr(st), int(init_maximums)),
+                    "SetTwisters")
+
+    def GetTwisters(self):
+        st = np.zeros((self.settings.getCellsCount(), 21), np.uint32)
+        self._check(lib().dsmc_get_twisters(self.h, _ptr(st)), "GetTwisters")
+        return st
+
     def SetCellState(self, maxrem=None, seeds=None):
         m = None if maxrem is None else np.ascontiguousarray(maxrem, np.float32)
         s = None if seeds is None else np.ascontiguousarray(seeds, np.uint32)
@@ -350,6 +366,15 @@ class DSMCBatch:
         v = np.zeros(len(self.solvers), np.int32)
         self._check(lib().dsmc_batch_autotune(self.b, _ptr(d), int(steps), _ptr(v)), "Autotune")
         return [int(x) for x in v]
+
+
+def read_twisters(path, count, seed=999):
+    """InitGPUTwisters' host part: the first `count` twister records of a
+    parameter file (data/MersenneTwister.dat), seeds from the lcg chain
+    started at `seed` (the reference uses SEED = 999).  (count, 4) uint32."""
+    cfg = np.zeros((count, 4), np.uint32)
+    check(lib().dsmc_read_twisters(str(path).encode(), seed, count, _ptr(cfg)), "read_twisters")
+    return cfg
 
 
 def KernelVariantCount():

@@ -105,7 +105,9 @@ int dsmc_config_default(dsmc_config* cfg);
 int dsmc_config_read_xml(const char* path, dsmc_config* cfg);
 
 /* settings_t::readFromCmdLine (src/sim_settings.cpp:134-186): -f, -benchmark,
- * -no-geometry, -mt (rejected: not supported), -density, -dt, -run-for. */
+ * -no-geometry, -density, -dt, -run-for.  -mt is rejected here: the -mt
+ * collisions need the twister file, which the caller loads with
+ * dsmc_read_twisters and hands to dsmc_set_twisters (dsmc_bench does this). */
 int dsmc_config_from_args(int argc, const char* const* argv, dsmc_config* cfg, float* run_for);
 
 /* CreateSolver(SolverGPU) + DSMCSolver::Init (kernels/dsmc_base.cu:43-47,
@@ -238,6 +240,26 @@ int dsmc_download_state(dsmc_handle* h, float* pos, float* vel, uint32_t* n, int
  * include/gpu_dsmc.inl:352-359) internal; this exposes them for parity
  * checks. */
 int dsmc_read_keys(dsmc_handle* h, uint32_t* keys, uint32_t* n);
+/* The -mt collisions (ComputeBirdCollisionsDev, kernels/dsmc_kernel.cu:1002-1089):
+ * cell c draws its NTC pairs and angles from Mersenne Twister c, the variant of
+ * kernels/mtwister.cu:30-117.  cfg4: per cell (matrix_a, mask_b, mask_c, seed),
+ * as dsmc_read_twisters returns them; state21: per cell (iState, mti1, mt[19]),
+ * or NULL to initialise each twister from its seed (InitTwisterFast,
+ * kernels/mtwister.cu:108-117).  init_maximums: also set (sigma g)max and the
+ * remainders as the reference's start does: InitMaximums (kernels/dsmc_kernel.cu:
+ * 1104-1120) runs before the twisters are initialised (include/gpu_dsmc.inl:363-367)
+ * and draws from zeroed states, so every remainder is (0 + 1) / 2^32.
+ * Needs the reference RNG mode (rng taus) and the split kernels (variants 4
+ * and up; a fused variant is replaced by 5).  The twisters are not part of
+ * snapshots. */
+int dsmc_set_twisters(dsmc_handle* h, const uint32_t* cfg4, const uint32_t* state21,
+                      int init_maximums);
+int dsmc_get_twisters(dsmc_handle* h, uint32_t* state21);
+/* InitGPUTwisters' host part (kernels/mtwister.cu:46-68): the first `count`
+ * 16-byte records of a twister parameter file (data/MersenneTwister.dat), each
+ * seed replaced by the next value of the chain seed <- seed * 279470273 mod
+ * 4294967291 started from `seed` (SEED = 999 in the reference). */
+int dsmc_read_twisters(const char* path, uint32_t seed, uint32_t count, uint32_t* cfg4);
 /* Per-cell collision state: (sigma*g)max and remainder (float2 per cell,
  * kernels/dsmc_kernel.cu:131) and HybridTaus seeds (uint4 per cell, :124). */
 int dsmc_set_cell_state(dsmc_handle* h, const float* maxrem, const uint32_t* seeds);
@@ -441,7 +463,8 @@ int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint
 
 /* --- Warm-start surrogate kernels (no counterpart in the reference) ---
  * Device pointers, asynchronous on `stream`.  BF16 operands, FP32
- * accumulation.  dsmc_gemm_bf16: c = A B (+ bias) (+ beta c) for an m x n
+ * accumulation; the GEMM runs on the tensor cores (tcgen05.mma, its
+ * accumulator in tensor memory), 128 x 128 tiles.  dsmc_gemm_bf16: c = A B (+ bias) (+ beta c) for an m x n
  * result; a_trans = 1 reads A stored k x m, b_trans = 1 reads B stored n x k
  * (row-major, leading dimensions lda/ldb/ldc/ldcb in elements).  act = 1
  * applies GELU: c keeps the pre-activation, c_bf16 (optional) receives the
@@ -452,6 +475,10 @@ int dsmc_stage_sample(const float* u, const float* v, const float* w, const uint
 int dsmc_gemm_bf16(int m, int n, int k, const void* a, int lda, int a_trans, const void* b, int ldb,
                    int b_trans, float* c, int ldc, float beta, const float* bias, int act, void* c_bf16,
                    int ldcb, int split_k, void* stream);
+/* Synchronises `stream` and reports whether a dsmc_gemm_bf16 launch since
+ * the last check gave up waiting on its tensor-core work (DSMC_ERR_DEVICE;
+ * its output is then incomplete); clears the flag. */
+int dsmc_gemm_check(void* stream);
 /* dz = dh * GELU'(z), in FP32 and/or BF16. */
 int dsmc_gelu_backward(const float* z, const float* dh, float* dz, void* dz_bf16, size_t n,
                        void* stream);

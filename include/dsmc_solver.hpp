@@ -95,6 +95,15 @@ class DSMCSolver {
     check(dsmc_init_state(h_, streamVel, &n), h_, "InitSystemState");
     return n;
   }
+  // The reference's -mt start (include/gpu_dsmc.inl:341-368): twister records
+  // of `path` with SEED's chain, InitMaximums, then InitMersenneTwisters; the
+  // collisions draw from the cells' twisters from then on.
+  void UseTwisters(const char* path, uint32_t seed = 999) {
+    std::vector<uint32_t> cfg(4 * (size_t)settings_.getCellsCount());
+    check(dsmc_read_twisters(path, seed, settings_.getCellsCount(), cfg.data()), nullptr,
+          "UseTwisters (twister file)");
+    check(dsmc_set_twisters(h_, cfg.data(), nullptr, 1), h_, "UseTwisters");
+  }
   void RunSimulationStep(float dt) { check(dsmc_step(h_, dt, 1), h_, "RunSimulationStep"); }
   void DoBenchmark(uint32_t itn, float dt) {
     check(dsmc_step_graph(h_, dt, (int)itn), h_, "DoBenchmark");

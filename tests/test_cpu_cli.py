@@ -28,10 +28,18 @@ def _config(tmp_path):
     return "cfg.xml"
 
 
-def test_mt_flag_is_refused_with_a_message(tmp_path):
-    r = _run(["-mt"], tmp_path)
+def test_mt_flag_is_taken_by_the_driver(tmp_path):
+    """-mt reaches the driver (the settings parser alone rejects it); without
+    a GPU the run stops at Init, before the twister file is read."""
+    import torch
+    cfg = _config(tmp_path)
+    r = _run(["-f", cfg, "-mt", "-mt-file", "missing.dat", "-steps", "1"], tmp_path)
     assert r.returncode == 1
-    assert "Exception: readFromCmdLine" in r.stderr and "-mt" in r.stderr
+    assert "readFromCmdLine" not in r.stderr
+    if torch.cuda.is_available():
+        assert "UseTwisters (twister file)" in r.stderr
+    else:
+        assert "Exception: Init: CUDA error" in r.stderr
 
 
 def test_missing_config_is_an_io_error(tmp_path):

@@ -188,3 +188,18 @@ def test_mt_collide_matches_reference_fixture():
     assert np.array_equal(mr[:, 1], d["maxrem_out"][:, 1])
     assert np.allclose(mr[:, 0], d["maxrem_out"][:, 0], rtol=1e-6)
     assert np.max(np.abs(vel[:, :3] - d["vel_out"][:, :3])) / (3 * 400.0) <= 2e-6
+
+
+@needs_mt_ref
+def test_library_reads_twister_records_as_the_reference():
+    """dsmc_read_twisters: InitGPUTwisters' host part (records of the file,
+    seeds from the lcg chain of SEED = 999)."""
+    import cudadsmc_b200 as cb
+    cfg = cb.read_twisters(O.MT_DAT, 3000)
+    recs = O.mt_records()[:3000]
+    assert np.array_equal(cfg[:, :3], recs[:, :3])
+    chain = np.zeros((3000, 4), np.uint32)
+    O.orc().orc_mt_seed_chain(999, O.p(chain), 3000)
+    assert np.array_equal(cfg[:, 3], chain[:, 3])
+    with pytest.raises(cb.DsmcError):
+        cb.read_twisters(O.MT_DAT, 70000)  # beyond the file's 65,536 records
