@@ -43,22 +43,18 @@ using namespace dev;
 constexpr uint32_t kWarpTile = 32;  // cells per warp tile, one per lane
 constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach the body
 
-// DIRECT: the order kernel reads each particle's state straight into
-// registers and stores it to its sorted slot (no shared-memory copy of the
-// state); only orig is staged.  Otherwise the state is gathered into shared
-// memory by asynchronous copies and written out after the pair counts.
-template <int CAPW, bool DIRECT = false>
+template <int CAPW>
 struct __align__(16) WarpSmem {
-  static constexpr int kOrig = DIRECT ? 0 : 6;  // orig's row in part
-  float part[2][DIRECT ? 1 : 7][CAPW + 8];  // (x y z u v w) orig of a chunk, double buffered
+  static constexpr int kOrig = 6;  // orig's row in part
+  float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
   uint4 lbuf[2 * kWarpTile];   // light-cell list entries not yet in the global list
   uint32_t cr[kWarpTile];      // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
   unsigned long long mbar[2];
 };
 
-template <int CAPW, int WARPS, bool DIRECT = false>
+template <int CAPW, int WARPS>
 constexpr size_t collide_smem_bytes() {
-  return WARPS * sizeof(WarpSmem<CAPW, DIRECT>);
+  return WARPS * sizeof(WarpSmem<CAPW>);
 }
 
 // A tile of 32 cells as the lanes see it: lane L holds the start and end of
@@ -125,9 +121,8 @@ __device__ __forceinline__ WChunk make_wchunk(const WTile& T, uint32_t cur, int 
 // into buffer c.buf.  The library's buffers carry 16 bytes of slack, so the
 // whole 16-byte aligned cover of [base, base + n) is copied (at most CAPW + 6
 // elements).
-template <int CAPW, bool DIRECT>
-__device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW, DIRECT>& S,
-                                             const WChunk& c) {
+template <int CAPW>
+__device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>& S, const WChunk& c) {
   const uint32_t ia = c.base & ~3u, ib = (c.base + c.n + 3u) & ~3u;
   const uint32_t bytes = (ib - ia) * 4u;
   const uint32_t lane = lane_id();
@@ -135,7 +130,7 @@ __device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW,
   __syncwarp();
   if (lane == 0) {
     fence_proxy_async();
-    bulk_g2s(S.part[c.buf][WarpSmem<CAPW, DIRECT>::kOrig], p.in_orig + ia, bytes, &S.mbar[c.buf]);
+    bulk_g2s(S.part[c.buf][WarpSmem<CAPW>::kOrig], p.in_orig + ia, bytes, &S.mbar[c.buf]);
   }
 }
 
@@ -222,11 +217,16 @@ __device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint
 
 // ---------------------------------------------------- order + pair counts ----
 
-template <int CAPW, int WARPS, int MINB, bool DIRECT>
+// PIPE: a chunk's sorted state is written out one chunk later, after the
+// next chunk's gathers are issued, so that the gathers' memory latency
+// overlaps the other work of the warp (the state buffers are double
+// buffered; cp.async groups track the chunks).  Otherwise each chunk waits
+// for its own gathers before it is written.
+template <int CAPW, int WARPS, int MINB, bool PIPE>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  using Smem = WarpSmem<CAPW, DIRECT>;
+  using Smem = WarpSmem<CAPW>;
   Smem& S = reinterpret_cast<Smem*>(smem_raw)[warp];
   const bool do_fixup = (p.flags & kDoFixup) != 0;
   const bool do_collide = (p.flags & kDoCollide) != 0;
@@ -256,6 +256,34 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
   uint32_t lcnt = 0;   // entries in S.lbuf
   WChunk C;
   C.valid = 0;
+  // PIPE: the chunk whose gathers are in flight and whose write is pending
+  uint32_t q_base = 0, q_n = 0, q_buf = 0;
+  bool q_valid = false;
+  // writes chunk (base, n) from state buffer b to the mid arrays
+  auto write_chunk = [&](uint32_t b, uint32_t base, uint32_t n) {
+    const uint32_t o = base & 3u;
+    const float* X = S.part[b][0] + o;
+    const float* Y = S.part[b][1] + o;
+    const float* Z = S.part[b][2] + o;
+    const float* U = S.part[b][3] + o;
+    const float* V = S.part[b][4] + o;
+    const float* W = S.part[b][5] + o;
+    for (uint32_t q = lane; q < n; q += 32) {
+      const uint32_t g = base + q;
+      p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
+      p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
+    }
+  };
+  // the pending chunk once all of this lane's gathers have landed
+  auto flush_pending = [&]() {
+    if (PIPE && q_valid) {
+      cp_async_wait_all();
+      __syncwarp();
+      write_chunk(q_buf, q_base, q_n);
+      __syncwarp();
+      q_valid = false;
+    }
+  };
   // (sigma g)max and remainder of a chunk's cells, loaded one chunk ahead
   float2 mr_c = make_float2(0.f, 0.f);
   auto load_cell_state = [&](const WChunk& K, uint32_t tile, float2& mr) {
@@ -297,6 +325,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       phase ^= 1u << C.buf;
       if (!__all_sync(kFull, ok)) {
         if (lane == 0 && p.meta) atomicOr(&p.meta->error, kErrTimeout);
+        flush_pending();
         // this chunk's and the next chunk's copies may still be in flight:
         // let them land (again bounded) before the shared memory goes away
         mbar_wait_bounded(&S.mbar[C.buf], par);
@@ -307,6 +336,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     __syncwarp();
 
     if (C.giant) {
+      // the buffer after this chunk's is the pending chunk's: write it first
+      flush_pending();
       giant_order_warp(p, C.base, C.base + C.n);
       if (do_collide) {
         // the giant cell's pair count, from lane C.cur's (sigma g)max
@@ -322,13 +353,16 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
                      make_uint4(gc, C.base, C.n, M));
       }
     } else if (C.n > 0) {
+      // the pending chunk sits in this chunk's buffer when an empty chunk
+      // came between them: write it before the gathers land there
+      if (PIPE && q_valid && q_buf == (uint32_t)C.buf) flush_pending();
       const uint32_t off = C.base & 3u;
-      float* X = S.part[C.buf][DIRECT ? 0 : 0] + off;
-      float* Y = S.part[C.buf][DIRECT ? 0 : 1] + off;
-      float* Z = S.part[C.buf][DIRECT ? 0 : 2] + off;
-      float* U = S.part[C.buf][DIRECT ? 0 : 3] + off;
-      float* V = S.part[C.buf][DIRECT ? 0 : 4] + off;
-      float* W = S.part[C.buf][DIRECT ? 0 : 5] + off;
+      float* X = S.part[C.buf][0] + off;
+      float* Y = S.part[C.buf][1] + off;
+      float* Z = S.part[C.buf][2] + off;
+      float* U = S.part[C.buf][3] + off;
+      float* V = S.part[C.buf][4] + off;
+      float* W = S.part[C.buf][5] + off;
       const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig] + off);
       const uint32_t base = C.base, n = C.n;
       // A: each particle's sorted position, sorted = (cell, orig), then the
@@ -338,11 +372,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       // number of smaller origs there (element j of the chunk sits at
       // ORA[j + off]).
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig]);
-      // DIRECT: the previous group's state, stored after this group's loads
-      // are issued (so that its load latency overlaps this group's rank)
-      float qx = 0.f, qy = 0.f, qz = 0.f, qu = 0.f, qv = 0.f, qw = 0.f;
-      uint32_t qpos = 0;
-      bool qval = false;
       if (do_fixup) {
         // Descents of orig inside the chunk.  A cell without one is in stable
         // order already (its particles took their tickets in one or a few
@@ -397,21 +426,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
             }
           }
         }
-        if (DIRECT) {
-          float lx = 0.f, ly = 0.f, lz = 0.f, lu = 0.f, lv = 0.f, lw = 0.f;
-          if (t < n) {
-            lx = __ldg(p.in.x + my); ly = __ldg(p.in.y + my); lz = __ldg(p.in.z + my);
-            lu = __ldg(p.in.u + my); lv = __ldg(p.in.v + my); lw = __ldg(p.in.w + my);
-          }
-          if (qval) {
-            const uint32_t g = base + qpos;
-            p.mid.x[g] = qx; p.mid.y[g] = qy; p.mid.z[g] = qz;
-            p.mid.u[g] = qu; p.mid.v[g] = qv; p.mid.w[g] = qw;
-          }
-          qx = lx; qy = ly; qz = lz; qu = lu; qv = lv; qw = lw;
-          qpos = pos;
-          qval = t < n;
-        } else if (t < n) {
+        if (t < n) {
           cp_async4(X + pos, p.in.x + my);
           cp_async4(Y + pos, p.in.y + my);
           cp_async4(Z + pos, p.in.z + my);
@@ -435,23 +450,25 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      if (DIRECT) {
-        // the last group's state
-        if (qval) {
-          const uint32_t g = base + qpos;
-          p.mid.x[g] = qx; p.mid.y[g] = qy; p.mid.z[g] = qz;
-          p.mid.u[g] = qu; p.mid.v[g] = qv; p.mid.w[g] = qw;
+      if (PIPE) {
+        // C of the previous chunk, whose gathers were issued one chunk ago
+        // (at most this chunk's group still in flight); this chunk's write
+        // is pending until the next chunk's gathers are issued
+        cp_async_commit();
+        if (q_valid) {
+          cp_async_wait_group1();
+          __syncwarp();
+          write_chunk(q_buf, q_base, q_n);
         }
-        __syncwarp();
+        q_valid = true;
+        q_base = base;
+        q_n = n;
+        q_buf = C.buf;
       } else {
         cp_async_wait_all();
         __syncwarp();
         // C: the chunk, now in sorted order, to the mid arrays
-        for (uint32_t q = lane; q < n; q += 32) {
-          const uint32_t g = base + q;
-          p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
-          p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
-        }
+        write_chunk(C.buf, base, n);
       }
     }
     __syncwarp();
@@ -464,6 +481,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     C = N;
     mr_c = mr_n;
   }
+  flush_pending();
   if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
   __shared__ unsigned long long s_red[WARPS];
   if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
@@ -820,20 +838,20 @@ struct LaunchShapeW {
   int per_sm = 0;
 };
 
-template <int CAPW, int WARPS, int MINB, bool DIRECT = false>
+template <int CAPW, int WARPS, int MINB, bool PIPE = false>
 cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   LaunchShapeW& ls = cache[dev & 7];
-  const size_t smem = collide_smem_bytes<CAPW, WARPS, DIRECT>();
+  const size_t smem = collide_smem_bytes<CAPW, WARPS>();
   if (ls.device != dev) {
-    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB, DIRECT>,
+    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB, PIPE>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB, DIRECT>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB, PIPE>,
                                                       WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -844,7 +862,7 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  k_order_w<CAPW, WARPS, MINB, DIRECT><<<grid, WARPS * 32, smem, stream>>>(p);
+  k_order_w<CAPW, WARPS, MINB, PIPE><<<grid, WARPS * 32, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -944,9 +962,9 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 // registers are capped for) of the order kernel and the flight kernel's form
 // (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 4;
 // one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs); 4-7 the order kernel's
-// direct form (state loaded into registers and stored to its sorted slot,
-// only orig staged in shared memory), one particle per lane in the flight
-// kernel: 4 (128, 4, 4), 5 (128, 4, 6), 6 (128, 8, 4), 7 (256, 4, 6).
+// pipelined form (a chunk written out after the next chunk's gathers are
+// issued), one particle per lane in the flight
+// kernel: 4 (128, 4, 4), 5 (128, 4, 6), 6 (128, 8, 3), 7 (256, 4, 4).
 int cell_kernel_w_variants() { return 8; }
 
 int cell_kernel_w_capacity(int v) {
@@ -965,8 +983,8 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         case 3: return launch_order_w<128, 4, 6>(p, stream);
         case 4: return launch_order_w<128, 4, 4, true>(p, stream);
         case 5: return launch_order_w<128, 4, 6, true>(p, stream);
-        case 6: return launch_order_w<128, 8, 4, true>(p, stream);
-        case 7: return launch_order_w<256, 4, 6, true>(p, stream);
+        case 6: return launch_order_w<128, 8, 3, true>(p, stream);
+        case 7: return launch_order_w<256, 4, 4, true>(p, stream);
         default: return launch_order_w<128, 4, 4>(p, stream);
       }
     case 1:

@@ -36,7 +36,8 @@ std::atomic<unsigned char*> g_scratch_addr[kMaxDevices];
 std::mutex g_scratch_mutex;
 
 // Device address of the scratch on the current device, looked up once per
-// device.
+// device and kept for the life of the process (a device reset would move the
+// array: the header tells callers not to use this entry point after one).
 cudaError_t scratch_address(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

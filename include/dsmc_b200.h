@@ -388,7 +388,10 @@ int dsmc_stage_sort(uint32_t* keys, uint32_t* vals, uint32_t n, uint32_t nkeys,
  * Limits: n <= DSMC_SORT_STATIC_MAX_N and nkeys <= DSMC_SORT_STATIC_MAX_KEYS;
  * larger sizes return DSMC_ERR_CAPACITY before any device work.
  * The scratch address is looked up once per device on the first call there;
- * make that first call outside any stream capture.  Every call zeroes the
+ * make that first call outside any stream capture.  The address is kept for
+ * the life of the process: after a reset of the device (cudaDeviceReset, or
+ * a reset of its primary context) the array may sit elsewhere, so a process
+ * that resets a device must not call this entry point on it again.  Every call zeroes the
  * scratch counters it needs on `stream` itself, so nothing has to be cleared
  * beforehand.  All calls on one device share the scratch: calls that may
  * overlap (different streams or host threads without ordering between them)

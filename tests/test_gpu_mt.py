@@ -56,15 +56,23 @@ def test_mt_steps_vs_oracle(cuda, steps):
                            dt, steps)
     same_cells = np.all(st_g == mts, axis=1).mean()
     same_part = np.all(pg[:, :3] == po[:, :3], axis=1).mean()
+    # the collisions drew exactly the same numbers (identical twister states:
+    # the same pairs, acceptances and angles); velocities differ in the last
+    # bits where the kernels' __cosf/__sinf and the oracle's libm cosf/sinf
+    # round apart, each collision by about an ulp, and positions by that
+    # times dt
+    scale = 3 * 400.0
+    dv = np.max(np.abs(vg[:, :3] - vo[:, :3]), axis=1) / scale
+    dp = np.max(np.abs(pg[:, :3] - po[:, :3]), axis=1)
     print(f"-mt, {steps} steps: cells with identical twister state {same_cells:.6f}, "
-          f"particles with identical position {same_part:.6f}")
-    assert same_cells >= 0.999
+          f"particles with identical position {same_part:.6f}, max velocity error {dv.max():.2e}, "
+          f"max position error {dp.max():.2e} m")
+    assert same_cells == 1.0
+    assert np.mean(dv <= 2e-6 * steps) >= 0.999
+    assert np.mean(dp <= 1e-6 + 2e-6 * steps * scale * dt) >= 0.999
     if steps == 1:
-        assert same_part > 0.999
-        assert np.max(np.abs(vg[:, :3] - vo[:, :3])) / (3 * 400.0) <= 2e-6
+        assert dv.max() <= 2e-6
         assert np.array_equal(mr_g[:, 1], mr_o[:, 1])  # remainders
-    else:
-        assert same_part > 0.99
     assert sol.Totals()[1] > 0
     sol.close()
 

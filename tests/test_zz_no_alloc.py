@@ -1,7 +1,11 @@
 """dsmc_stage_sort_static (the stage sort on the library's static scratch,
 allocating nothing) against dsmc_stage_sort on the same inputs, two calls in a
 row with different sizes so that state left by the first call would show in
-the second.  Collected last so that it also runs after every other GPU test."""
+the second, and allocating nothing on the second call (free device memory and
+the default stream-ordered pool unchanged).  Collected last so that it also
+runs after every other GPU test."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -28,16 +32,51 @@ def _case(seed, n, nkeys):
     return keys, vals
 
 
+class _DeviceMemory:
+    """Free device memory (cudaMemGetInfo) and the default stream-ordered
+    pool's used bytes (cudaMemPoolAttrUsedMemCurrent / High) of the current
+    device, read through the CUDA runtime the library itself loads."""
+
+    def __init__(self):
+        self.rt = ctypes.CDLL("libcudart.so.12")
+
+    def read(self):
+        free, total = ctypes.c_size_t(), ctypes.c_size_t()
+        assert self.rt.cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+        dev = ctypes.c_int()
+        assert self.rt.cudaGetDevice(ctypes.byref(dev)) == 0
+        pool = ctypes.c_void_p()
+        assert self.rt.cudaDeviceGetDefaultMemPool(ctypes.byref(pool), dev) == 0
+        used, high = ctypes.c_uint64(), ctypes.c_uint64()
+        assert self.rt.cudaMemPoolGetAttribute(pool, 7, ctypes.byref(used)) == 0  # UsedMemCurrent
+        assert self.rt.cudaMemPoolGetAttribute(pool, 8, ctypes.byref(high)) == 0  # UsedMemHigh
+        return free.value, used.value, high.value
+
+
 def test_static_sort_matches_stage_sort_twice_in_a_row(cuda):
     cases = [(11, 300000, 100000), (12, 70000, 5000)]
+    inputs = [(seed, nkeys) + _case(seed, n, nkeys) for seed, n, nkeys in cases]
+    # every device buffer of the two calls exists before they run, and the
+    # memory readings around the second call see only what it allocates
+    # (the first call on a device may load the library's module, which
+    # reserves the static scratch)
+    dev_in = [(_u32(keys, cuda), _u32(vals, cuda),
+               torch.full((nkeys + 1,), -1, dtype=torch.int32, device=cuda))
+              for _, nkeys, keys, vals in inputs]
+    torch.cuda.synchronize()
+    mem = _DeviceMemory()
     outs = []
-    for seed, n, nkeys in cases:
-        keys, vals = _case(seed, n, nkeys)
-        kt, vt = _u32(keys, cuda), _u32(vals, cuda)
-        st = torch.full((nkeys + 1,), -1, dtype=torch.int32, device=cuda)
+    before = None
+    for (seed, nkeys, keys, vals), (kt, vt, st) in zip(inputs, dev_in):
+        if outs:
+            torch.cuda.synchronize()
+            before = mem.read()
         stages.sort_static(kt, vt, nkeys, cell_start=st)
         outs.append((keys, vals, nkeys, kt, vt, st))
     torch.cuda.synchronize()
+    after = mem.read()
+    # the call allocated nothing: neither device memory nor pool memory
+    assert after == before, (before, after)
     for keys, vals, nkeys, kt, vt, st in outs:
         kr, vr = _u32(keys, cuda), _u32(vals, cuda)
         sr = torch.zeros(nkeys + 1, dtype=torch.int32, device=cuda)
