@@ -245,15 +245,10 @@ unsigned grid_1d(size_t n) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-// Shared memory per CTA: the tiles, padded to kTcSmemReserve so that every
-// address a descriptor of this kernel can form stays inside the allocation.
-constexpr int kTcSmemReserve = 200 * 1024;
-
 template <bool AT, bool BT>
 void launch_tc(dim3 grid, const GemmArgs& g, cudaStream_t s) {
   static bool attr = false;
-  const int smem = (int)sizeof(dsmcb::umma::Smem) > kTcSmemReserve ? (int)sizeof(dsmcb::umma::Smem)
-                                                                   : kTcSmemReserve;
+  const int smem = (int)sizeof(dsmcb::umma::Smem);
   if (!attr) {
     if (cudaFuncSetAttribute(k_gemm_tc<AT, BT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
         cudaSuccess)
