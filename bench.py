@@ -627,7 +627,57 @@ def run_batch(args, rank, world):
     batch.close()
     for s in sols:
         s.close()
+    out["single_instance_same_size"] = single_same_size(args, int(sum(n_now)), len(sols), stream)
+    sv = out["single_instance_same_size"]["value"]
+    out["single_instance_same_size"]["batch_over_single"] = value / max(world, 1) / sv
     return out
+
+
+def single_same_size(args, particles, members, stream):
+    """One sphere flow as large as the whole ensemble (the members' cells
+    together, 256 x 128 x 128 for 64 members of 64 x 32 x 32, and their
+    particles together), stepped with the same kernels: the throughput a
+    batch could reach if its members' per-step launches cost nothing beyond
+    their particles' work, the bound a persistent batched kernel would aim
+    at."""
+    import torch
+    import cudadsmc_b200 as cb
+    f = max(1, round(members ** (1.0 / 3.0)))
+    dim = (64 * f, 32 * f, 32 * f)
+    dom = (1.2, 0.6, 0.6)
+    cells = dim[0] * dim[1] * dim[2]
+    cell_v = (dom[0] / dim[0]) * (dom[1] / dim[1]) * (dom[2] / dim[2])
+    T, m = 200.0, ARGON["gas_mass"]
+    a = math.sqrt(5.0 / 3.0 * KB * T / m)
+    cmp = math.sqrt(2 * KB * T / m)
+    u, nd = 6.0 * a, 1e20
+    st = dict(grid_min=(0, 0, 0), grid_max=dom, grid_dim=dim, density=nd,
+              fnum=nd * cell_v / (particles / cells), temp=T, stream_vel=(u, 0.0, 0.0),
+              dt=0.2 * min(dom[k] / dim[k] for k in range(3)) / (u + 3 * cmp), rng="philox",
+              ntc_local=1, sample_every=100, init_kind="maxwell", wall_diffuse=1, wall_temp=400.0,
+              capacity_factor=1.6, seed=77, geom_nearest=1,
+              face_kind={"-x": "inflow", "+x": "outflow", "-y": "outflow", "+y": "outflow",
+                         "-z": "outflow", "+z": "outflow"}, **ARGON)
+    sol = cb.DSMCSolver().Init(cb.settings_t().set(**st))
+    v, t = cb.mesh_icosphere(3, 0.1, (0.4, 0.3, 0.3))
+    sol.SetModel(v, t, (8 * f, 8 * f, 8 * f))
+    sol.SetStream(stream.cuda_stream)
+    sol.InitSystemState()
+    dt = st["dt"]
+    sol.StepGraph(dt, max(3, args.warmup))
+    sol.Sync()
+    k = max(3, args.steps // 4)
+    p0 = sol.Info().particle_steps
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    sol.StepGraph(dt, k)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    res = {"value": (sol.Info().particle_steps - p0) / (ms * 1e-3), "ms_per_step": ms / k,
+           "particles": int(sol.Info().num_particles), "cells": cells, "grid": list(dim), "steps": k}
+    sol.close()
+    return res
 
 
 def run_e2e(args, wl, rank, world, dev, variant):

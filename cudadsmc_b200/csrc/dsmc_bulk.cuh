@@ -61,14 +61,6 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
-// Closes this thread's current group of asynchronous copies.
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-// Waits until at most one group of this thread's copies is in flight.
-__device__ __forceinline__ void cp_async_wait_group1() {
-  asm volatile("cp.async.wait_group 1;" ::: "memory");
-}
 
 // Waits for an mbarrier phase for at most about a second.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* m, uint32_t parity) {

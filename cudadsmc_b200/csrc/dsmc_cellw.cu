@@ -217,12 +217,7 @@ __device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint
 
 // ---------------------------------------------------- order + pair counts ----
 
-// PIPE: a chunk's sorted state is written out one chunk later, after the
-// next chunk's gathers are issued, so that the gathers' memory latency
-// overlaps the other work of the warp (the state buffers are double
-// buffered; cp.async groups track the chunks).  Otherwise each chunk waits
-// for its own gathers before it is written.
-template <int CAPW, int WARPS, int MINB, bool PIPE>
+template <int CAPW, int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -256,9 +251,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
   uint32_t lcnt = 0;   // entries in S.lbuf
   WChunk C;
   C.valid = 0;
-  // PIPE: the chunk whose gathers are in flight and whose write is pending
-  uint32_t q_base = 0, q_n = 0, q_buf = 0;
-  bool q_valid = false;
   // writes chunk (base, n) from state buffer b to the mid arrays
   auto write_chunk = [&](uint32_t b, uint32_t base, uint32_t n) {
     const uint32_t o = base & 3u;
@@ -272,16 +264,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       const uint32_t g = base + q;
       p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
       p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
-    }
-  };
-  // the pending chunk once all of this lane's gathers have landed
-  auto flush_pending = [&]() {
-    if (PIPE && q_valid) {
-      cp_async_wait_all();
-      __syncwarp();
-      write_chunk(q_buf, q_base, q_n);
-      __syncwarp();
-      q_valid = false;
     }
   };
   // (sigma g)max and remainder of a chunk's cells, loaded one chunk ahead
@@ -325,7 +307,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       phase ^= 1u << C.buf;
       if (!__all_sync(kFull, ok)) {
         if (lane == 0 && p.meta) atomicOr(&p.meta->error, kErrTimeout);
-        flush_pending();
         // this chunk's and the next chunk's copies may still be in flight:
         // let them land (again bounded) before the shared memory goes away
         mbar_wait_bounded(&S.mbar[C.buf], par);
@@ -336,8 +317,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     __syncwarp();
 
     if (C.giant) {
-      // the buffer after this chunk's is the pending chunk's: write it first
-      flush_pending();
       giant_order_warp(p, C.base, C.base + C.n);
       if (do_collide) {
         // the giant cell's pair count, from lane C.cur's (sigma g)max
@@ -353,9 +332,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
                      make_uint4(gc, C.base, C.n, M));
       }
     } else if (C.n > 0) {
-      // the pending chunk sits in this chunk's buffer when an empty chunk
-      // came between them: write it before the gathers land there
-      if (PIPE && q_valid && q_buf == (uint32_t)C.buf) flush_pending();
       const uint32_t off = C.base & 3u;
       float* X = S.part[C.buf][0] + off;
       float* Y = S.part[C.buf][1] + off;
@@ -450,26 +426,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      if (PIPE) {
-        // C of the previous chunk, whose gathers were issued one chunk ago
-        // (at most this chunk's group still in flight); this chunk's write
-        // is pending until the next chunk's gathers are issued
-        cp_async_commit();
-        if (q_valid) {
-          cp_async_wait_group1();
-          __syncwarp();
-          write_chunk(q_buf, q_base, q_n);
-        }
-        q_valid = true;
-        q_base = base;
-        q_n = n;
-        q_buf = C.buf;
-      } else {
-        cp_async_wait_all();
-        __syncwarp();
-        // C: the chunk, now in sorted order, to the mid arrays
-        write_chunk(C.buf, base, n);
-      }
+      cp_async_wait_all();
+      __syncwarp();
+      // C: the chunk, now in sorted order, to the mid arrays
+      write_chunk(C.buf, base, n);
     }
     __syncwarp();
     if (n_in_b) {
@@ -481,7 +441,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     C = N;
     mr_c = mr_n;
   }
-  flush_pending();
   if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
   __shared__ unsigned long long s_red[WARPS];
   if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
@@ -838,7 +797,7 @@ struct LaunchShapeW {
   int per_sm = 0;
 };
 
-template <int CAPW, int WARPS, int MINB, bool PIPE = false>
+template <int CAPW, int WARPS, int MINB>
 cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
@@ -847,11 +806,11 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   LaunchShapeW& ls = cache[dev & 7];
   const size_t smem = collide_smem_bytes<CAPW, WARPS>();
   if (ls.device != dev) {
-    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB, PIPE>,
+    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB, PIPE>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB>,
                                                       WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
@@ -862,7 +821,7 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  k_order_w<CAPW, WARPS, MINB, PIPE><<<grid, WARPS * 32, smem, stream>>>(p);
+  k_order_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -961,15 +920,12 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 // CTA-wide ones): (particles per warp chunk, warps per CTA, CTAs per SM the
 // registers are capped for) of the order kernel and the flight kernel's form
 // (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 4;
-// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs); 4-7 the order kernel's
-// pipelined form (a chunk written out after the next chunk's gathers are
-// issued), one particle per lane in the flight
-// kernel: 4 (128, 4, 4), 5 (128, 4, 6), 6 (128, 8, 3), 7 (256, 4, 4).
-int cell_kernel_w_variants() { return 8; }
+// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs).
+int cell_kernel_w_variants() { return 4; }
 
 int cell_kernel_w_capacity(int v) {
-  static const int caps[8] = {256, 128, 128, 128, 128, 128, 128, 256};
-  return caps[v < 0 || v > 7 ? 1 : v];
+  static const int caps[4] = {256, 128, 128, 128};
+  return caps[v < 0 || v > 3 ? 1 : v];
 }
 
 uint32_t cell_kernel_w_tile() { return kWarpTile; }
@@ -981,10 +937,6 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         case 0: return launch_order_w<256, 4, 4>(p, stream);
         case 2: return launch_order_w<128, 8, 3>(p, stream);
         case 3: return launch_order_w<128, 4, 6>(p, stream);
-        case 4: return launch_order_w<128, 4, 4, true>(p, stream);
-        case 5: return launch_order_w<128, 4, 6, true>(p, stream);
-        case 6: return launch_order_w<128, 8, 3, true>(p, stream);
-        case 7: return launch_order_w<256, 4, 4, true>(p, stream);
         default: return launch_order_w<128, 4, 4>(p, stream);
       }
     case 1:

@@ -272,98 +272,78 @@ __device__ __forceinline__ bool intersect_triangle_rel(float3 o, float3 d, float
 
 // Nearest triangle crossed by the segment o + s d, s in [0, dist] (d unit),
 // among the triangles of every geometry cell the segment passes through
-// (Amanatides-Woo traversal of the uniform grid).
+// (Amanatides-Woo traversal of the uniform grid).  The walk keeps its state
+// per axis in scalars (no arrays indexed at run time, which would live in
+// local memory), and the next cell's triangle range is loaded while the
+// current cell's triangles are tested, so each cell costs one round trip to
+// memory for its planes (and one more for the vertices of the few triangles
+// whose plane the segment crosses).
+struct DdaAxis {
+  int i, step, dim;
+  float tmax, tdel;
+};
+
+__device__ __forceinline__ bool dda_axis_init(float o, float d, float lo, float hi, float cs, int dim,
+                                              float& t0, float& t1, DdaAxis& a) {
+  a.dim = dim;
+  if (fabsf(d) < 1e-30f) {
+    if (o < lo || o > hi) return false;
+    a.step = 0;
+    a.tmax = 3.0e38f;
+    a.tdel = 3.0e38f;
+    return true;
+  }
+  const float id = 1.f / d;
+  float ta = (lo - o) * id, tb = (hi - o) * id;
+  if (ta > tb) { const float s = ta; ta = tb; tb = s; }
+  t0 = fmaxf(t0, ta);
+  t1 = fminf(t1, tb);
+  a.step = d > 0.f ? 1 : -1;
+  a.tdel = fabsf(cs * id);
+  return true;
+}
+
+__device__ __forceinline__ void dda_axis_start(float o, float d, float lo, float cs, float tstart, DdaAxis& a) {
+  const float pp = o + d * tstart;
+  const int i = (int)floorf((pp - lo) / cs);
+  a.i = min(max(i, 0), a.dim - 1);
+  if (a.step > 0) a.tmax = (lo + (a.i + 1) * cs - o) / d;
+  else if (a.step < 0) a.tmax = (lo + a.i * cs - o) / d;
+}
+
+// The axis whose boundary the walk crosses next (0, 1, 2).
+__device__ __forceinline__ int dda_next_axis(const DdaAxis& x, const DdaAxis& y, const DdaAxis& z) {
+  return (x.tmax <= y.tmax && x.tmax <= z.tmax) ? 0 : (y.tmax <= z.tmax ? 1 : 2);
+}
+
 __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, float3 d, float dist,
                                                  float* t_out, uint32_t* entry_out) {
   const GridGeom& g = G.grid;
   float t0 = 0.f, t1 = dist;
-  float oa[3] = {o.x, o.y, o.z}, da[3] = {d.x, d.y, d.z};
-  float lo[3] = {g.gmin.x, g.gmin.y, g.gmin.z}, hi[3] = {g.gmax.x, g.gmax.y, g.gmax.z};
-  float cs[3] = {g.cell.x, g.cell.y, g.cell.z};
-  int dm[3] = {(int)g.dim.x, (int)g.dim.y, (int)g.dim.z};
-  // slab and cell-crossing parameters by reciprocal multiplies (the start
-  // cell below keeps the division)
-  float ida[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) ida[a] = fabsf(da[a]) < 1e-30f ? 0.f : 1.f / da[a];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    if (fabsf(da[a]) < 1e-30f) {
-      if (oa[a] < lo[a] || oa[a] > hi[a]) return false;
-    } else {
-      float ta = (lo[a] - oa[a]) * ida[a], tb = (hi[a] - oa[a]) * ida[a];
-      if (ta > tb) { float s = ta; ta = tb; tb = s; }
-      t0 = fmaxf(t0, ta);
-      t1 = fminf(t1, tb);
-    }
-  }
+  DdaAxis X, Y, Z;
+  if (!dda_axis_init(o.x, d.x, g.gmin.x, g.gmax.x, g.cell.x, (int)g.dim.x, t0, t1, X)) return false;
+  if (!dda_axis_init(o.y, d.y, g.gmin.y, g.gmax.y, g.cell.y, (int)g.dim.y, t0, t1, Y)) return false;
+  if (!dda_axis_init(o.z, d.z, g.gmin.z, g.gmax.z, g.cell.z, (int)g.dim.z, t0, t1, Z)) return false;
   if (t0 > t1) return false;
-  int idx[3], stp[3];
-  float tmax[3], tdel[3];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    float p = oa[a] + da[a] * t0;
-    int i = (int)floorf((p - lo[a]) / cs[a]);
-    idx[a] = min(max(i, 0), dm[a] - 1);
-    if (da[a] > 0.f) {
-      stp[a] = 1;
-      tmax[a] = (lo[a] + (idx[a] + 1) * cs[a] - oa[a]) * ida[a];
-      tdel[a] = cs[a] * ida[a];
-    } else if (da[a] < 0.f) {
-      stp[a] = -1;
-      tmax[a] = (lo[a] + idx[a] * cs[a] - oa[a]) * ida[a];
-      tdel[a] = -cs[a] * ida[a];
-    } else {
-      stp[a] = 0;
-      tmax[a] = 3.0e38f;
-      tdel[a] = 3.0e38f;
-    }
-  }
-  // The cells the segment crosses are known before any triangle is tested:
-  // load the triangle ranges of the first few together and prefetch their
-  // planes and vertices into L2, so that the walk below pays one round trip to
-  // memory instead of three per cell (its loads then hit the caches).
-  {
-    constexpr int kAhead = 6;
-    int pidx[3] = {idx[0], idx[1], idx[2]};
-    float ptmax[3] = {tmax[0], tmax[1], tmax[2]};
-    uint2 pse[kAhead];
-    int np = 0;
-    bool more = true;
-#pragma unroll
-    for (int k = 0; k < kAhead; k++) {
-      if (more) {
-        // the walk's own stepping rule
-        const uint32_t c = ((uint32_t)pidx[2] * g.dim.y + (uint32_t)pidx[1]) * g.dim.x + (uint32_t)pidx[0];
-        pse[k] = geo_ld(&G.start_end[c]);
-        np = k + 1;
-        const float texit = fminf(ptmax[0], fminf(ptmax[1], ptmax[2]));
-        if (texit > t1) {
-          more = false;
-        } else {
-          const int a = (ptmax[0] <= ptmax[1] && ptmax[0] <= ptmax[2]) ? 0 : (ptmax[1] <= ptmax[2] ? 1 : 2);
-          pidx[a] += stp[a];
-          if (pidx[a] < 0 || pidx[a] >= dm[a]) more = false;
-          else ptmax[a] += tdel[a];
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < kAhead; k++) {
-      if (k < np && pse[k].x < pse[k].y) {
-        geo_prefetch(G.plane + pse[k].x);
-        geo_prefetch(G.tri + kTriStride * (size_t)pse[k].x);
-        if (kTriStride * (pse[k].y - pse[k].x) > 8u)  // stays inside the cell's entries
-          geo_prefetch(G.tri + kTriStride * (size_t)pse[k].x + 8);
-      }
-    }
-  }
+  dda_axis_start(o.x, d.x, g.gmin.x, g.cell.x, t0, X);
+  dda_axis_start(o.y, d.y, g.gmin.y, g.cell.y, t0, Y);
+  dda_axis_start(o.z, d.z, g.gmin.z, g.cell.z, t0, Z);
+  auto cell_of = [&](int ix, int iy, int iz) {
+    return ((uint32_t)iz * g.dim.y + (uint32_t)iy) * g.dim.x + (uint32_t)ix;
+  };
   float best = 3.0e38f;
   uint32_t best_i = kNone;
-  const int max_iter = dm[0] + dm[1] + dm[2] + 3;
+  uint2 se = geo_ld(&G.start_end[cell_of(X.i, Y.i, Z.i)]);
+  const int max_iter = (int)(g.dim.x + g.dim.y + g.dim.z) + 3;
   for (int it = 0; it < max_iter; it++) {
-    uint32_t c = ((uint32_t)idx[2] * g.dim.y + (uint32_t)idx[1]) * g.dim.x + (uint32_t)idx[0];
-    const uint2 se = geo_ld(&G.start_end[c]);
+    // the walk's next cell, and its triangle range on the way
+    const float texit = fminf(X.tmax, fminf(Y.tmax, Z.tmax));
+    const int ax = dda_next_axis(X, Y, Z);
+    int nx = X.i, ny = Y.i, nz = Z.i;
+    if (ax == 0) nx += X.step; else if (ax == 1) ny += Y.step; else nz += Z.step;
+    const bool more = texit <= t1 && nx >= 0 && nx < X.dim && ny >= 0 && ny < Y.dim && nz >= 0 && nz < Z.dim;
+    uint2 se_next = make_uint2(0u, 0u);
+    if (more) se_next = geo_ld(&G.start_end[cell_of(nx, ny, nz)]);
     for (uint32_t i0 = se.x; i0 < se.y; i0 += 8) {
       // the planes of up to 8 of the cell's triangles in one round of loads
       float4 P[8];
@@ -380,9 +360,9 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
         const float s1 = fmaf(dist, dot_x(pn, d), s0);
         const float tol = __fmul_rn(1e-7f, fabsf(P[k].w) + 1.f);
         if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
-        float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
-        float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
-        float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
+        const float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
+        const float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
+        const float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
         float t;
         if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
                                    make_float3(C.x, C.y, C.z), &t) &&
@@ -392,12 +372,11 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
         }
       }
     }
-    float texit = fminf(tmax[0], fminf(tmax[1], tmax[2]));
-    if (best <= texit || texit > t1) break;
-    int a = (tmax[0] <= tmax[1] && tmax[0] <= tmax[2]) ? 0 : (tmax[1] <= tmax[2] ? 1 : 2);
-    idx[a] += stp[a];
-    if (idx[a] < 0 || idx[a] >= dm[a]) break;
-    tmax[a] += tdel[a];
+    if (best <= texit || !more) break;
+    if (ax == 0) { X.i = nx; X.tmax += X.tdel; }
+    else if (ax == 1) { Y.i = ny; Y.tmax += Y.tdel; }
+    else { Z.i = nz; Z.tmax += Z.tdel; }
+    se = se_next;
   }
   if (best_i == kNone) return false;
   *t_out = best;

@@ -277,11 +277,10 @@ int dsmc_step_graph(dsmc_handle* h, float dt, int nsteps);
 /* Launch shape of the step's cell kernel (no counterpart in the reference,
  * whose kernels use fixed block sizes).  Variants 0-3 are a CTA-wide kernel:
  * 0 = 512 threads per CTA and up to 2048 particles per shared-memory chunk,
- * 1 = 256/1024, 2 = 128/512, 3 = 64/256.  Variants 4-11 are split kernels
+ * 1 = 256/1024, 2 = 128/512, 3 = 64/256.  Variants 4-7 are split kernels
  * whose warps each work through their own tiles of 32 cells, with chunks of
- * up to 256 (4, 11) or 128 (5-10) particles per warp; 8-11 load each
- * particle's state into registers and store it to its sorted slot, 4-7
- * stage it in shared memory; 5 is the default.  Results do not
+ * up to 256 (4) or 128 (5-7) particles per warp; 5 is the default.  Results
+ * do not
  * depend on the variant, except in the Philox mode for a cell holding more
  * particles than the chunk (it is then collided by one thread instead of one
  * warp, a different but equivalent stream of draws).  Changing it drops the
