@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "dsmc_b200.h"
+#include "dsmc_geomgrid.hpp"
 #include "dsmc_host.hpp"
 #include "dsmc_kernels.cuh"
 
@@ -55,6 +56,7 @@ struct dsmc_handle {
   uint2* gse = nullptr;
   float4* gtri = nullptr;
   float4* gplane = nullptr;
+  float4* gbound = nullptr;
   GridGeom gcgrid{};  // grid of the clearance table gclear
 
   bool has_state = false;
@@ -176,7 +178,7 @@ void free_all(dsmc_handle* h) {
   }
   void* ps[] = {h->orig, h->ntc_list, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
                 h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse,
-                h->gtri, h->gplane, h->mt_state, h->mt_cfg};
+                h->gtri, h->gplane, h->gbound, h->mt_state, h->mt_cfg};
   for (void* p : ps) cudaFree(p);
   h->mt_state = nullptr;
   h->mt_cfg = nullptr;
@@ -241,6 +243,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.start_end = h->gse;
     p.geom.tri = h->gtri;
     p.geom.plane = h->gplane;
+    p.geom.bound = h->gbound;
     p.geom.clear = h->gclear;
     p.geom.cgrid = h->gcgrid;
     p.geom.diffuse = h->cfg.wall_diffuse;
@@ -726,48 +729,30 @@ int dsmc_build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t
   return DSMC_OK;
 }
 
-static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
-                           const uint32_t* tris, uint32_t ntris, const float* normals) {
+// The face normals of the mesh when the caller gives none.
+static const float* normals_or_faces(const float* verts, uint32_t nverts, const uint32_t* tris,
+                                     uint32_t ntris, const float* normals, std::vector<float>& nrm) {
+  if (normals) return normals;
+  std::vector<float> v(verts, verts + 3 * (size_t)nverts);
+  std::vector<uint32_t> t(tris, tris + 3 * (size_t)ntris);
+  dsmcb::face_normals(v, t, nrm);
+  return nrm.data();
+}
+
+static void free_geometry(dsmcb::GeomDevice& gd) {
+  cudaFree(gd.flags);
+  cudaFree(gd.se);
+  cudaFree(gd.tri);
+  cudaFree(gd.plane);
+  cudaFree(gd.bound);
+  gd = dsmcb::GeomDevice{};
+}
+
+// Takes over the device arrays of a built grid (h->ggrid holds its host copy)
+// and fills the clearance table.
+static int install_geometry(dsmc_handle* h, dsmcb::GeomDevice& gd) {
   const auto& g = h->ggrid;
-  std::vector<float> nrm;
-  if (!normals) {
-    std::vector<float> v(verts, verts + 3 * (size_t)nverts);
-    std::vector<uint32_t> t(tris, tris + 3 * (size_t)ntris);
-    dsmcb::face_normals(v, t, nrm);
-    normals = nrm.data();
-  }
   const uint32_t gc = g.dim[0] * g.dim[1] * g.dim[2];
-  std::vector<uint32_t> flags(gc);
-  std::vector<uint2> se(gc);
-  const size_t stride = dsmcb::kTriStride;
-  std::vector<float4> tri(stride * (g.tri_ids.size() + 1));
-  std::vector<float4> plane(g.tri_ids.size() + 1);
-  size_t off = 0;
-  for (uint32_t c = 0; c < gc; c++) {
-    flags[c] = g.flags[c];
-    if (g.count[c]) se[c] = make_uint2((uint32_t)off, (uint32_t)(off + g.count[c]));
-    else se[c] = make_uint2(0xffffffffu, 0xffffffffu);
-    for (uint32_t k = 0; k < g.count[c]; k++) {
-      uint32_t t = g.tri_ids[off + k];
-      const float* a = verts + 3 * (size_t)tris[3 * t];
-      const float* b = verts + 3 * (size_t)tris[3 * t + 1];
-      const float* cc = verts + 3 * (size_t)tris[3 * t + 2];
-      const float* n = normals + 3 * (size_t)t;
-      tri[stride * (off + k)] = make_float4(a[0], a[1], a[2], n[0]);
-      tri[stride * (off + k) + 1] = make_float4(b[0], b[1], b[2], n[1]);
-      tri[stride * (off + k) + 2] = make_float4(cc[0], cc[1], cc[2], n[2]);
-      // plane of the triangle from its vertices (unit normal, offset)
-      double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
-      double e2[3] = {(double)cc[0] - a[0], (double)cc[1] - a[1], (double)cc[2] - a[2]};
-      double pn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
-                      e1[0] * e2[1] - e1[1] * e2[0]};
-      double l = std::sqrt(pn[0] * pn[0] + pn[1] * pn[1] + pn[2] * pn[2]);
-      if (l > 0) { pn[0] /= l; pn[1] /= l; pn[2] /= l; }
-      plane[off + k] = make_float4((float)pn[0], (float)pn[1], (float)pn[2],
-                                   (float)(pn[0] * a[0] + pn[1] * a[1] + pn[2] * a[2]));
-    }
-    off += g.count[c];
-  }
   // Chebyshev cell distance of every cell to the nearest cell holding
   // triangles (multi-source BFS over the 26-neighbourhood): (distance - 1) x
   // the smallest cell size bounds the distance from any point of the cell to
@@ -801,20 +786,16 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
   cudaFree(h->gse);
   cudaFree(h->gtri);
   cudaFree(h->gplane);
-  h->gflags = nullptr; h->gclear = nullptr; h->gse = nullptr; h->gtri = nullptr;
-  h->gplane = nullptr;
-  CK(h, dalloc(&h->gflags, gc), "geometry alloc");
+  cudaFree(h->gbound);
+  h->gflags = gd.flags;
+  h->gse = gd.se;
+  h->gtri = gd.tri;
+  h->gplane = gd.plane;
+  h->gbound = gd.bound;
+  h->gclear = nullptr;
+  gd = dsmcb::GeomDevice{};
+  h->has_geom = false;
   CK(h, dalloc(&h->gclear, fc), "geometry alloc");
-  CK(h, dalloc(&h->gse, gc), "geometry alloc");
-  CK(h, dalloc(&h->gtri, tri.size()), "geometry alloc");
-  CK(h, dalloc(&h->gplane, plane.size()), "geometry alloc");
-  CK(h, cudaMemcpy(h->gflags, flags.data(), gc * 4, cudaMemcpyHostToDevice), "geometry upload");
-
-  CK(h, cudaMemcpy(h->gse, se.data(), gc * sizeof(uint2), cudaMemcpyHostToDevice), "geometry upload");
-  CK(h, cudaMemcpy(h->gtri, tri.data(), tri.size() * sizeof(float4), cudaMemcpyHostToDevice),
-     "geometry upload");
-  CK(h, cudaMemcpy(h->gplane, plane.data(), plane.size() * sizeof(float4), cudaMemcpyHostToDevice),
-     "geometry upload");
   {
     h->gcgrid.gmin = make_float3(g.bbox[0], g.bbox[1], g.bbox[2]);
     h->gcgrid.gmax = make_float3(g.bbox[3], g.bbox[4], g.bbox[5]);
@@ -841,6 +822,7 @@ static int upload_geometry(dsmc_handle* h, const float* verts, uint32_t nverts,
   return DSMC_OK;
 }
 
+// The grid of a mesh, binned on the device (dsmc_geomgrid.cu).
 int dsmc_set_mesh(dsmc_handle* h, const float* verts, uint32_t nverts, const uint32_t* tris,
                   uint32_t ntris, const float* normals, const int grid_dim[3]) {
   if (!h || !verts || !tris || !grid_dim || ntris == 0) return fail(h, DSMC_ERR_ARG, "bad mesh");
@@ -848,8 +830,16 @@ int dsmc_set_mesh(dsmc_handle* h, const float* verts, uint32_t nverts, const uin
     if (grid_dim[k] <= 0) return fail(h, DSMC_ERR_ARG, "geometry grid dims must be > 0");
   for (uint32_t i = 0; i < 3 * ntris; i++)
     if (tris[i] >= nverts) return fail(h, DSMC_ERR_ARG, "triangle index out of range");
-  dsmcb::build_geometry_grid(verts, nverts, tris, ntris, grid_dim, h->ggrid);
-  return upload_geometry(h, verts, nverts, tris, ntris, normals);
+  std::vector<float> nrm;
+  normals = normals_or_faces(verts, nverts, tris, ntris, normals, nrm);
+  dsmcb::geometry_grid_frame(verts, nverts, grid_dim, h->ggrid);
+  dsmcb::GeomDevice gd;
+  const cudaError_t e = dsmcb::build_geometry_device(h->ggrid, verts, nverts, tris, ntris, normals, gd);
+  if (e) {
+    free_geometry(gd);
+    return fail(h, DSMC_ERR_CUDA, std::string("geometry grid build: ") + cudaGetErrorString(e));
+  }
+  return install_geometry(h, gd);
 }
 
 int dsmc_set_geometry_grid(dsmc_handle* h, const float bbox[6], const float cell[3],
@@ -875,7 +865,60 @@ int dsmc_set_geometry_grid(dsmc_handle* h, const float bbox[6], const float cell
     if (t >= ntris) return fail(h, DSMC_ERR_ARG, "triangle id out of range");
   for (uint32_t i = 0; i < 3 * ntris; i++)
     if (tris[i] >= nverts) return fail(h, DSMC_ERR_ARG, "triangle index out of range");
-  return upload_geometry(h, verts, nverts, tris, ntris, normals);
+  std::vector<float> nrm;
+  normals = normals_or_faces(verts, nverts, tris, ntris, normals, nrm);
+  // the given binning to the device, then the same entry records
+  std::vector<uint32_t> start((size_t)gc + 1, 0u), fl(gc);
+  for (uint32_t c = 0; c < gc; c++) {
+    start[c + 1] = start[c] + g.count[c];
+    fl[c] = g.flags[c] ? 1u : 0u;
+  }
+  dsmcb::GeomDevice gd;
+  uint32_t *d_start = nullptr, *d_ids = nullptr, *d_tris = nullptr;
+  float *d_verts = nullptr, *d_normals = nullptr;
+  auto up = [](auto** p, const auto* src, size_t n) {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), (n ? n : 1) * sizeof(**p));
+    if (!e && n) e = cudaMemcpy(*p, src, n * sizeof(**p), cudaMemcpyHostToDevice);
+    return e;
+  };
+  cudaError_t e = up(&d_start, start.data(), start.size());
+  if (!e) e = up(&d_ids, g.tri_ids.data(), total);
+  if (!e) e = up(&d_tris, tris, 3 * (size_t)ntris);
+  if (!e) e = up(&d_verts, verts, 3 * (size_t)nverts);
+  if (!e) e = up(&d_normals, normals, 3 * (size_t)ntris);
+  if (!e) e = up(&gd.flags, fl.data(), fl.size());
+  if (!e) e = dsmcb::geometry_entries_device(d_start, d_ids, gc, (uint32_t)total, d_verts, d_tris,
+                                             d_normals, gd);
+  if (!e) e = cudaDeviceSynchronize();
+  cudaFree(d_start);
+  cudaFree(d_ids);
+  cudaFree(d_tris);
+  cudaFree(d_verts);
+  cudaFree(d_normals);
+  if (e) {
+    free_geometry(gd);
+    return fail(h, DSMC_ERR_CUDA, std::string("geometry upload: ") + cudaGetErrorString(e));
+  }
+  return install_geometry(h, gd);
+}
+
+int dsmc_get_geometry_grid(dsmc_handle* h, float bbox[6], float cell[3], int dim[3],
+                           uint32_t* cell_count, uint32_t* tri_ids, float* planes, uint64_t cap,
+                           uint8_t* flags, uint64_t* n_entries) {
+  if (!h) return DSMC_ERR_ARG;
+  if (!h->has_geom) return fail(h, DSMC_ERR_STATE, "no geometry grid (dsmc_set_mesh)");
+  const auto& g = h->ggrid;
+  if (bbox) std::memcpy(bbox, g.bbox, sizeof(g.bbox));
+  if (cell) std::memcpy(cell, g.cell, sizeof(g.cell));
+  if (dim)
+    for (int k = 0; k < 3; k++) dim[k] = (int)g.dim[k];
+  if (cell_count) std::memcpy(cell_count, g.count.data(), g.count.size() * 4);
+  if (flags) std::memcpy(flags, g.flags.data(), g.flags.size());
+  const size_t n = std::min<size_t>(cap, g.tri_ids.size());
+  if (tri_ids) std::memcpy(tri_ids, g.tri_ids.data(), n * 4);
+  if (planes && n) CK(h, cudaMemcpy(planes, h->gplane, n * sizeof(float4), cudaMemcpyDeviceToHost), "read planes");
+  if (n_entries) *n_entries = g.tri_ids.size();
+  return DSMC_OK;
 }
 
 int dsmc_read_raw_mesh(const char* path, float* verts, uint32_t* nverts, uint32_t* tris,

@@ -14,6 +14,11 @@
 //      stable order of the reference's sort) are computed
 //   B  NTC pair counts (and remainders); cells with pairs are listed
 //   C  the chunk goes to the mid arrays in sorted order
+// The two-pass form of the same step splits this in two: k_rank_w runs the
+// chunk loop with orig alone (A restores the stable order by rewriting, in
+// place, the orig of the slots whose position changes; B as above), and
+// k_gather_w then moves the state, mid[s] = in[orig[s]], one slot per thread
+// at full occupancy (no per-chunk waits between a warp's gathers).
 // k_ntc_w: the listed cells' NTC selections in place on the mid arrays, a
 // lane per light cell, a warp per dense cell (Philox mode).
 // k_flight_w (flight + keys): streams the sorted particles, 32 at a time per
@@ -28,8 +33,9 @@
 // every cell that fits a chunk.  Gathering through orig lets the scatter write
 // orig alone (one scattered 4-byte store per particle instead of seven).
 //
-// Traffic per particle: k_order_w orig 4 + state 24 read, 24 written;
-// k_flight_w 24 read, 24 + key 4 written.  Per cell: 8 B of starts, 16 B of
+// Traffic per particle: k_order_w orig 4 + state 24 read, 24 written (the
+// two-pass form reads orig twice and writes it again where a cell's order
+// changes); k_flight_w 24 read, 24 + key 4 written.  Per cell: 8 B of starts, 16 B of
 // (sigma g)max read + written, 32 B more in the reference RNG mode, 80 B of
 // sampling sums on sampling steps.
 #include "dsmc_bulk.cuh"
@@ -43,18 +49,20 @@ using namespace dev;
 constexpr uint32_t kWarpTile = 32;  // cells per warp tile, one per lane
 constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach the body
 
-template <int CAPW>
+// ROWS = 7 (order kernel): x y z u v w orig of a chunk; ROWS = 1 (rank
+// pass): orig alone.
+template <int CAPW, int ROWS>
 struct __align__(16) WarpSmem {
-  static constexpr int kOrig = 6;  // orig's row in part
-  float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
-  uint4 lbuf[2 * kWarpTile];   // light-cell list entries not yet in the global list
-  uint32_t cr[kWarpTile];      // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
+  static constexpr int kOrig = ROWS - 1;  // orig's row in part
+  float part[2][ROWS][CAPW + 8];  // a chunk, double buffered
+  uint4 lbuf[2 * kWarpTile];      // light-cell list entries not yet in the global list
+  uint32_t cr[kWarpTile];         // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
   unsigned long long mbar[2];
 };
 
-template <int CAPW, int WARPS>
+template <int CAPW, int WARPS, int ROWS>
 constexpr size_t collide_smem_bytes() {
-  return WARPS * sizeof(WarpSmem<CAPW>);
+  return WARPS * sizeof(WarpSmem<CAPW, ROWS>);
 }
 
 // A tile of 32 cells as the lanes see it: lane L holds the start and end of
@@ -121,8 +129,8 @@ __device__ __forceinline__ WChunk make_wchunk(const WTile& T, uint32_t cur, int 
 // into buffer c.buf.  The library's buffers carry 16 bytes of slack, so the
 // whole 16-byte aligned cover of [base, base + n) is copied (at most CAPW + 6
 // elements).
-template <int CAPW>
-__device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>& S, const WChunk& c) {
+template <class Smem>
+__device__ __forceinline__ void issue_wchunk(const StepParams& p, Smem& S, const WChunk& c) {
   const uint32_t ia = c.base & ~3u, ib = (c.base + c.n + 3u) & ~3u;
   const uint32_t bytes = (ib - ia) * 4u;
   const uint32_t lane = lane_id();
@@ -130,7 +138,7 @@ __device__ __forceinline__ void issue_wchunk(const StepParams& p, WarpSmem<CAPW>
   __syncwarp();
   if (lane == 0) {
     fence_proxy_async();
-    bulk_g2s(S.part[c.buf][WarpSmem<CAPW>::kOrig], p.in_orig + ia, bytes, &S.mbar[c.buf]);
+    bulk_g2s(S.part[c.buf][Smem::kOrig], p.in_orig + ia, bytes, &S.mbar[c.buf]);
   }
 }
 
@@ -149,6 +157,88 @@ static __device__ __noinline__ void giant_order_warp(const StepParams& p, uint32
     p.mid.x[d] = p.in.x[my]; p.mid.y[d] = p.in.y[my]; p.mid.z[d] = p.in.z[my];
     p.mid.u[d] = p.in.u[my]; p.mid.v[d] = p.in.v[my]; p.mid.w[d] = p.in.w[my];
   }
+}
+
+// The same cell in the rank pass: its orig in stable order, in place.  The
+// sorted origs go through the cell's slots of p.mid.x first (the gather pass
+// writes every slot of mid afterwards), so that no lane overwrites an orig
+// another lane still counts against.
+static __device__ __noinline__ void giant_rank_warp(const StepParams& p, uint32_t s, uint32_t e) {
+  const uint32_t n = e - s;
+  const uint32_t lane = lane_id();
+  uint32_t* tmp = reinterpret_cast<uint32_t*>(p.mid.x);
+  if (lane == 0 && p.meta) atomicAdd(&p.meta->giant_cells, 1u);
+  for (uint32_t i = lane; i < n; i += 32) {
+    const uint32_t my = p.in_orig[s + i];
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < n; j++) rank += (uint32_t)(p.in_orig[s + j] < my);
+    tmp[s + rank] = my;
+  }
+  __syncwarp();
+  for (uint32_t i = lane; i < n; i += 32) p.in_orig[s + i] = tmp[s + i];
+}
+
+// Descents of orig inside a chunk (OR: its n origs).  A cell without one is
+// in stable order already (its particles took their tickets in one or a few
+// increasing runs, the common case) and a slot's rank there is its position;
+// only cells with a descent count smaller origs.  True for the lanes whose
+// nonempty cell (chunk-relative start s0, nc particles) has one.  All lanes
+// call it.
+template <int CAPW>
+__device__ __forceinline__ bool cell_has_descent(const uint32_t* OR, uint32_t n, bool ne, uint32_t s0,
+                                                 uint32_t nc) {
+  const uint32_t lane = lane_id();
+  uint32_t dw[CAPW / 32];
+#pragma unroll
+  for (int k = 0; k < CAPW / 32; k++) {
+    const uint32_t t = 32u * k + lane;
+    dw[k] = __ballot_sync(kFull, t > 0 && t < n && OR[t - 1] > OR[t]);
+  }
+  bool unsorted = false;
+  if (ne && nc > 1) {
+    const uint32_t lo_b = s0 + 1u, hi_b = s0 + nc;
+#pragma unroll
+    for (int k = 0; k < CAPW / 32; k++) {
+      const uint32_t w0 = 32u * k;
+      const uint32_t l = max(lo_b, w0), h = min(hi_b, w0 + 32u);
+      if (l < h) {
+        const uint32_t m = (uint32_t)(((1ull << (h - w0)) - 1ull) & ~((1ull << (l - w0)) - 1ull));
+        unsorted |= (dw[k] & m) != 0u;
+      }
+    }
+  }
+  return unsorted;
+}
+
+// Position in stable (cell, orig) order of chunk slot t = b0 + lane (orig
+// `my`; t itself for t >= n).  Its cell is the last nonempty cell starting at
+// or before t, found by its ordinal among them: the lanes stand for the
+// tile's cells (chunk-relative start s0, nonempty `ne`), giving the starts in
+// [b0, b0 + 32) as a bit mask and the count before.  In a cell flagged with a
+// descent (bit 31 of its `cr` entry: start | end << 16) the rank is the
+// number of smaller origs there; ORA holds the chunk's origs from offset
+// `off`.  All lanes call it.
+__device__ __forceinline__ uint32_t stable_slot(const uint32_t* ORA, const uint32_t* cr, uint32_t off,
+                                                uint32_t b0, uint32_t n, uint32_t my, bool ne,
+                                                uint32_t s0) {
+  const uint32_t lane = lane_id(), t = b0 + lane;
+  const unsigned starts =
+      __reduce_or_sync(kFull, (ne && s0 >= b0 && s0 < b0 + 32u) ? 1u << (s0 - b0) : 0u);
+  const uint32_t before = __popc(__ballot_sync(kFull, ne && s0 < b0));
+  uint32_t pos = t;
+  if (t < n) {
+    const uint32_t ab = cr[before + __popc(starts & (0xffffffffu >> (31u - lane))) - 1u];
+    if (ab >> 31) {
+      const uint32_t a = ab & 0xffffu, b = (ab >> 16) & 0x7fffu;
+      uint32_t rank = 0;
+      // one element per step: the lanes of a cell read the same word (a
+      // broadcast), and lanes of different cells only differ in the trip
+      // count (a 16-byte form with edge cases diverged in both)
+      for (uint32_t j = a + off; j < b + off; j++) rank += (uint32_t)(ORA[j] < my);
+      pos = a + rank;
+    }
+  }
+  return pos;
 }
 
 // Appends e for every lane with `put` to list (one atomic per warp; all lanes
@@ -217,11 +307,14 @@ __device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint
 
 // ---------------------------------------------------- order + pair counts ----
 
-template <int CAPW, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
+// The chunk loop of the order kernel (RANK false) and of the rank pass (RANK
+// true: orig put in stable order in place, no state moved; the gather pass
+// moves it afterwards).
+template <int CAPW, int WARPS, bool RANK>
+__device__ __forceinline__ void order_chunks(const StepParams& p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  using Smem = WarpSmem<CAPW>;
+  using Smem = WarpSmem<CAPW, RANK ? 1 : 7>;
   Smem& S = reinterpret_cast<Smem*>(smem_raw)[warp];
   const bool do_fixup = (p.flags & kDoFixup) != 0;
   const bool do_collide = (p.flags & kDoCollide) != 0;
@@ -317,7 +410,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
     __syncwarp();
 
     if (C.giant) {
-      giant_order_warp(p, C.base, C.base + C.n);
+      if constexpr (RANK) {
+        if (do_fixup) giant_rank_warp(p, C.base, C.base + C.n);
+      } else {
+        giant_order_warp(p, C.base, C.base + C.n);
+      }
       if (do_collide) {
         // the giant cell's pair count, from lane C.cur's (sigma g)max
         const uint32_t gc = c0 + C.cur;
@@ -333,82 +430,57 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       }
     } else if (C.n > 0) {
       const uint32_t off = C.base & 3u;
-      float* X = S.part[C.buf][0] + off;
-      float* Y = S.part[C.buf][1] + off;
-      float* Z = S.part[C.buf][2] + off;
-      float* U = S.part[C.buf][3] + off;
-      float* V = S.part[C.buf][4] + off;
-      float* W = S.part[C.buf][5] + off;
       const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig] + off);
-      const uint32_t base = C.base, n = C.n;
-      // A: each particle's sorted position, sorted = (cell, orig), then the
-      // gather of its state through orig straight to that position
-      // (asynchronous 4-byte copies, in flight while the pair counts run).
-      // The origs are distinct, so a particle's rank in its cell is the
-      // number of smaller origs there (element j of the chunk sits at
-      // ORA[j + off]).
+      // element j of the chunk sits at ORA[j + off]
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig]);
-      if (do_fixup) {
-        // Descents of orig inside the chunk.  A cell without one is in stable
-        // order already (its particles took their tickets in one or a few
-        // increasing runs, the common case) and a slot's rank there is its
-        // position; only cells with a descent count smaller origs.  The flag
-        // goes to bit 31 of the cell's range entry.
-        uint32_t dw[CAPW / 32];
-#pragma unroll
-        for (int k = 0; k < CAPW / 32; k++) {
-          const uint32_t t = 32u * k + lane;
-          dw[k] = __ballot_sync(kFull, t > 0 && t < n && OR[t - 1] > OR[t]);
-        }
-        if (ne && nc > 1) {
-          bool unsorted = false;
-          const uint32_t lo_b = s0 + 1u, hi_b = s0 + nc;
-#pragma unroll
-          for (int k = 0; k < CAPW / 32; k++) {
-            const uint32_t w0 = 32u * k;
-            const uint32_t l = max(lo_b, w0), h = min(hi_b, w0 + 32u);
-            if (l < h) {
-              const uint32_t m = (uint32_t)(((1ull << (h - w0)) - 1ull) & ~((1ull << (l - w0)) - 1ull));
-              unsorted |= (dw[k] & m) != 0u;
-            }
-          }
-          if (unsorted) S.cr[ne_idx] |= 0x80000000u;
-        }
-        __syncwarp();
-      }
-      for (uint32_t b0 = 0; b0 < n; b0 += 32) {
-        const uint32_t t = b0 + lane;
-        const uint32_t my = t < n ? OR[t] : 0u;
-        uint32_t pos = t;
+      const uint32_t base = C.base, n = C.n;
+      if constexpr (RANK) {
+        // A: the slots of cells with a descent get their orig in stable
+        // order (only those whose position changes are written)
         if (do_fixup) {
-          // the slot's cell: the last nonempty cell starting at or before t,
-          // by its ordinal among them (lanes here stand for the tile's cells:
-          // the starts in [b0, b0 + 32) as a bit mask, and the count before)
-          const unsigned starts =
-              __reduce_or_sync(kFull, (ne && s0 >= b0 && s0 < b0 + 32u) ? 1u << (s0 - b0) : 0u);
-          const uint32_t before = __popc(__ballot_sync(kFull, ne && s0 < b0));
-          if (t < n) {
-            const uint32_t ab = S.cr[before + __popc(starts & (0xffffffffu >> (31u - lane))) - 1u];
-            if (ab >> 31) {
-              const uint32_t a = ab & 0xffffu, b = (ab >> 16) & 0x7fffu;
-              const uint32_t lo = a + off, hi = b + off;
-              uint32_t rank = 0;
-              // one element per step: the lanes of a cell read the same word
-              // (a broadcast), and lanes of different cells only differ in
-              // the trip count (a 16-byte form with edge cases diverged in
-              // both)
-              for (uint32_t j = lo; j < hi; j++) rank += (uint32_t)(ORA[j] < my);
-              pos = a + rank;
+          const bool desc = cell_has_descent<CAPW>(OR, n, ne, s0, nc);
+          if (desc) S.cr[ne_idx] |= 0x80000000u;
+          const bool any = __any_sync(kFull, desc);
+          __syncwarp();
+          if (any) {
+            for (uint32_t b0 = 0; b0 < n; b0 += 32) {
+              // a strip without a flagged cell keeps its order
+              if (!__any_sync(kFull, desc && s0 < b0 + 32u && s0 + nc > b0)) continue;
+              const uint32_t t = b0 + lane;
+              const uint32_t my = t < n ? OR[t] : 0u;
+              const uint32_t pos = stable_slot(ORA, S.cr, off, b0, n, my, ne, s0);
+              if (t < n && pos != t) p.in_orig[base + pos] = my;
             }
           }
         }
-        if (t < n) {
-          cp_async4(X + pos, p.in.x + my);
-          cp_async4(Y + pos, p.in.y + my);
-          cp_async4(Z + pos, p.in.z + my);
-          cp_async4(U + pos, p.in.u + my);
-          cp_async4(V + pos, p.in.v + my);
-          cp_async4(W + pos, p.in.w + my);
+      } else {
+        float* X = S.part[C.buf][0] + off;
+        float* Y = S.part[C.buf][1] + off;
+        float* Z = S.part[C.buf][2] + off;
+        float* U = S.part[C.buf][3] + off;
+        float* V = S.part[C.buf][4] + off;
+        float* W = S.part[C.buf][5] + off;
+        // A: each particle's sorted position, sorted = (cell, orig), then the
+        // gather of its state through orig straight to that position
+        // (asynchronous 4-byte copies, in flight while the pair counts run).
+        // The origs are distinct, so a particle's rank in its cell is the
+        // number of smaller origs there.
+        if (do_fixup) {
+          if (cell_has_descent<CAPW>(OR, n, ne, s0, nc)) S.cr[ne_idx] |= 0x80000000u;
+          __syncwarp();
+        }
+        for (uint32_t b0 = 0; b0 < n; b0 += 32) {
+          const uint32_t t = b0 + lane;
+          const uint32_t my = t < n ? OR[t] : 0u;
+          const uint32_t pos = do_fixup ? stable_slot(ORA, S.cr, off, b0, n, my, ne, s0) : t;
+          if (t < n) {
+            cp_async4(X + pos, p.in.x + my);
+            cp_async4(Y + pos, p.in.y + my);
+            cp_async4(Z + pos, p.in.z + my);
+            cp_async4(U + pos, p.in.u + my);
+            cp_async4(V + pos, p.in.v + my);
+            cp_async4(W + pos, p.in.w + my);
+          }
         }
       }
       // B: pair counts (the new remainder is stored now); cells with pairs
@@ -426,10 +498,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      cp_async_wait_all();
-      __syncwarp();
-      // C: the chunk, now in sorted order, to the mid arrays
-      write_chunk(C.buf, base, n);
+      if constexpr (!RANK) {
+        cp_async_wait_all();
+        __syncwarp();
+        // C: the chunk, now in sorted order, to the mid arrays
+        write_chunk(C.buf, base, n);
+      }
     }
     __syncwarp();
     if (n_in_b) {
@@ -444,6 +518,53 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
   if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
   __shared__ unsigned long long s_red[WARPS];
   if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
+}
+
+template <int CAPW, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
+  order_chunks<CAPW, WARPS, false>(p);
+}
+
+// Rank pass of the two-pass order (orig in stable order in place, pair counts
+// and cell lists); k_gather_w then moves the state.
+template <int CAPW, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_rank_w(const __grid_constant__ StepParams p) {
+  order_chunks<CAPW, WARPS, true>(p);
+}
+
+// Gather pass of the two-pass order: mid[s] = in[orig[s]] for every slot of
+// the step (start[cells] of them), orig in stable order already.  UNROLL
+// slots per thread, blockDim.x apart, keep their loads in flight together;
+// neighbouring slots mostly have neighbouring origs, so a warp's gathered
+// loads touch few sectors.
+template <int UNROLL>
+__global__ void __launch_bounds__(256) k_gather_w(const __grid_constant__ StepParams p) {
+  const uint32_t n = __ldg(&p.start[p.cells]);
+  const uint32_t span = blockDim.x * UNROLL;
+  for (uint32_t s0 = blockIdx.x * span + threadIdx.x; s0 < n; s0 += gridDim.x * span) {
+    uint32_t o[UNROLL];
+#pragma unroll
+    for (int k = 0; k < UNROLL; k++) {
+      const uint32_t s = s0 + k * blockDim.x;
+      o[k] = s < n ? __ldg(&p.in_orig[s]) : 0u;
+    }
+    float v[6][UNROLL];
+#pragma unroll
+    for (int k = 0; k < UNROLL; k++) {
+      if (s0 + k * blockDim.x < n) {
+        v[0][k] = __ldg(&p.in.x[o[k]]); v[1][k] = __ldg(&p.in.y[o[k]]); v[2][k] = __ldg(&p.in.z[o[k]]);
+        v[3][k] = __ldg(&p.in.u[o[k]]); v[4][k] = __ldg(&p.in.v[o[k]]); v[5][k] = __ldg(&p.in.w[o[k]]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < UNROLL; k++) {
+      const uint32_t s = s0 + k * blockDim.x;
+      if (s < n) {
+        p.mid.x[s] = v[0][k]; p.mid.y[s] = v[1][k]; p.mid.z[s] = v[2][k];
+        p.mid.u[s] = v[3][k]; p.mid.v[s] = v[4][k]; p.mid.w[s] = v[5][k];
+      }
+    }
+  }
 }
 
 // ------------------------------------------------------- NTC selections ----
@@ -795,25 +916,36 @@ struct LaunchShapeW {
   int device = -1;
   uint32_t n_scan_tiles = 0;
   int per_sm = 0;
+  int gather_per_sm = 0;
 };
 
-template <int CAPW, int WARPS, int MINB>
+constexpr int kGatherUnroll = 4;
+
+// The order kernel, or with RANK the rank pass followed by the gather pass.
+template <int CAPW, int WARPS, int MINB, bool RANK = false>
 cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   LaunchShapeW& ls = cache[dev & 7];
-  const size_t smem = collide_smem_bytes<CAPW, WARPS>();
+  void (*kern)(const StepParams);
+  if constexpr (RANK) kern = k_rank_w<CAPW, WARPS, MINB>;
+  else kern = k_order_w<CAPW, WARPS, MINB>;
+  const size_t smem = collide_smem_bytes<CAPW, WARPS, RANK ? 1 : 7>();
   if (ls.device != dev) {
-    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB>,
-                                                      WARPS * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    if (RANK) {
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ls.gather_per_sm, k_gather_w<kGatherUnroll>,
+                                                        256, 0);
+      if (e != cudaSuccess) return e;
+      if (ls.gather_per_sm < 1) return cudaErrorInvalidConfiguration;
+    }
     ls.device = dev;
     ls.per_sm = per_sm;
   }
@@ -821,7 +953,12 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  k_order_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
+  kern<<<grid, WARPS * 32, smem, stream>>>(p);
+  if (!RANK) return cudaGetLastError();
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // a full wave: the particle count is known only on the device
+  k_gather_w<kGatherUnroll><<<(uint32_t)(num_sms() * ls.gather_per_sm), 256, 0, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -920,12 +1057,13 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 // CTA-wide ones): (particles per warp chunk, warps per CTA, CTAs per SM the
 // registers are capped for) of the order kernel and the flight kernel's form
 // (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 4;
-// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs).
-int cell_kernel_w_variants() { return 4; }
+// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs); 4 the two-pass order
+// (rank pass (256, 4, 8), then the gather pass) and single flights.
+int cell_kernel_w_variants() { return 5; }
 
 int cell_kernel_w_capacity(int v) {
-  static const int caps[4] = {256, 128, 128, 128};
-  return caps[v < 0 || v > 3 ? 1 : v];
+  static const int caps[5] = {256, 128, 128, 128, 256};
+  return caps[v < 0 || v > 4 ? 1 : v];
 }
 
 uint32_t cell_kernel_w_tile() { return kWarpTile; }
@@ -937,6 +1075,7 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         case 0: return launch_order_w<256, 4, 4>(p, stream);
         case 2: return launch_order_w<128, 8, 3>(p, stream);
         case 3: return launch_order_w<128, 4, 6>(p, stream);
+        case 4: return launch_order_w<256, 4, 8, true>(p, stream);
         default: return launch_order_w<128, 4, 4>(p, stream);
       }
     case 1:

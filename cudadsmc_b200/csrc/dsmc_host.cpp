@@ -603,12 +603,11 @@ bool tri_box_overlap(const float center[3], const float half[3], const float tri
 // src/reggrid.cpp:27-93).  Each triangle is tested against the cells its
 // bounding box touches (plus one cell of margin); entries stay in triangle
 // order within a cell, the order the reference's cell-major loop produces.
-void build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris,
-                         const int dim[3], GeomGrid& out) {
+void geometry_grid_frame(const float* verts, uint32_t nverts, const int dim[3], GeomGrid& out) {
   float mn[3] = {100000, 100000, 100000}, mx[3] = {-100000, -100000, -100000};
   for (uint32_t i = 0; i < nverts; i++)
     for (int k = 0; k < 3; k++) {
-      float x = verts[3 * i + k];
+      float x = verts[3 * (size_t)i + k];
       if (x < mn[k]) mn[k] = x;
       if (x > mx[k]) mx[k] = x;
     }
@@ -618,6 +617,12 @@ void build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tr
     out.bbox[k] = mn[k];
     out.bbox[3 + k] = mx[k];
   }
+}
+
+void build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris,
+                         const int dim[3], GeomGrid& out) {
+  geometry_grid_frame(verts, nverts, dim, out);
+  const float mn[3] = {out.bbox[0], out.bbox[1], out.bbox[2]};
   const uint32_t dx = out.dim[0], dy = out.dim[1], dz = out.dim[2];
   const uint32_t ncell = dx * dy * dz;
   std::vector<std::vector<uint32_t>> bins(ncell);

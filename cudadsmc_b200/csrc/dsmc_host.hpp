@@ -33,6 +33,8 @@ void mesh_icosphere(int level, float radius, const float* center, std::vector<fl
 void mesh_capsule(float rn, float theta_deg, float length, const float* c, uint32_t ntarget,
                   uint64_t seed, std::vector<float>& verts, std::vector<uint32_t>& tris);
 bool tri_box_overlap(const float center[3], const float half[3], const float tri[9]);
+// The grid's frame: dim, the mesh's bounding box and the cell size.
+void geometry_grid_frame(const float* verts, uint32_t nverts, const int dim[3], GeomGrid& out);
 void build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tris, uint32_t ntris,
                          const int dim[3], GeomGrid& out);
 

@@ -104,8 +104,8 @@ struct StepParams {
 
   // buffers
   SoA in;             // state the cell kernel reads (sorted by scatter)
-  const uint32_t* in_orig;
-  SoA out;            // state the cell kernel writes (sorted order)
+  uint32_t* in_orig;  // written only by the rank pass of the split variants
+  SoA out;          // state the cell kernel writes (sorted order)
   SoA mid;            // split variants: the sorted post-collision state between
                       // the collide kernel (which gathers it from `in` through
                       // in_orig) and the flight kernel (which writes `out`)

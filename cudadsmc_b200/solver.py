@@ -273,6 +273,27 @@ class DSMCSolver:
                     "DownloadState")
         return p, v
 
+    def GeometryGrid(self):
+        """The handle's geometry grid (built on the device by SetModel): bbox,
+        cell size, dims, per-cell triangle counts, triangle ids in bin order,
+        flags, and each entry's plane (unit normal, offset) as the device
+        holds it."""
+        dim = np.zeros(3, np.int32)
+        ne = ctypes.c_uint64()
+        self._check(lib().dsmc_get_geometry_grid(self.h, None, None, _ptr(dim), None, None, None, 0,
+                                                 None, ctypes.byref(ne)), "get_geometry_grid")
+        ncell = int(dim[0]) * int(dim[1]) * int(dim[2])
+        bbox = np.zeros(6, np.float32)
+        cell = np.zeros(3, np.float32)
+        count = np.zeros(ncell, np.uint32)
+        flags = np.zeros(ncell, np.uint8)
+        ids = np.zeros(max(ne.value, 1), np.uint32)
+        planes = np.zeros((max(ne.value, 1), 4), np.float32)
+        self._check(lib().dsmc_get_geometry_grid(self.h, _ptr(bbox), _ptr(cell), _ptr(dim), _ptr(count),
+                                                 _ptr(ids), _ptr(planes), ne.value, _ptr(flags),
+                                                 ctypes.byref(ne)), "get_geometry_grid")
+        return bbox, cell, dim, count, ids[: ne.value], flags, planes[: ne.value]
+
     def ReadKeys(self):
         """Next-step cell key of every particle slot (0xffffffff: left the
         domain), in the order of DownloadState."""

@@ -188,13 +188,24 @@ int dsmc_set_geometry_grid(dsmc_handle* h, const float bbox[6], const float cell
                            const uint8_t* flags, const float* verts, uint32_t nverts,
                            const uint32_t* tris, uint32_t ntris, const float* normals);
 
-/* The geometry-grid builder on its own (host; same binning as dsmc_set_mesh).
+/* The geometry-grid builder on the host (the same binning as dsmc_set_mesh
+ * computes on the device).
  * Returns the number of bin entries through *n_entries (tri_ids holds at most
  * cap of them). */
 int dsmc_build_geometry_grid(const float* verts, uint32_t nverts, const uint32_t* tris,
                              uint32_t ntris, const int grid_dim[3], float bbox[6], float cell[3],
                              uint32_t* cell_count, uint32_t* tri_ids, uint64_t cap,
                              uint8_t* flags, uint64_t* n_entries);
+
+/* The handle's geometry grid as dsmc_set_mesh built it on the device (or as
+ * dsmc_set_geometry_grid received it): bbox, cell size, dims, per-cell
+ * triangle count, triangle ids in bin order, per-cell flag, and with planes
+ * != NULL each entry's plane (unit normal x, y, z and offset; 4 floats per
+ * entry) read from the device.  Any output may be NULL; tri_ids and planes
+ * hold at most cap entries; *n_entries gets the entry count. */
+int dsmc_get_geometry_grid(dsmc_handle* h, float bbox[6], float cell[3], int dim[3],
+                           uint32_t* cell_count, uint32_t* tri_ids, float* planes, uint64_t cap,
+                           uint8_t* flags, uint64_t* n_entries);
 
 /* Model::LoadRaw (src/model.cpp:348-401): reads the reference's .raw mesh
  * (vertices, indices, face normals).  With verts == NULL only the counts are

@@ -148,6 +148,14 @@ def test_collide_taus(cuda, omega, ppc):
     torch.cuda.synchronize()
     sd_g = np_u32(sd_t).reshape(-1, 4)
     same = np.all(sd_g == sd_or, axis=1)
+    # The oracle runs on the host: its cosf/sinf (libm) and the GPU's
+    # __cosf/__sinf differ in the last bits, so post-collision velocities can
+    # differ by an ulp, and a later acceptance test in the same cell (random
+    # number against sigma g / (sigma g)max) that close to its threshold can
+    # go the other way; that cell's stream then consumes a different number
+    # of draws.  Such cells (at most 0.1 %) are left out of the exact
+    # comparison; against the reference's own GPU kernels every cell is
+    # bit-identical (test_gpu_step.py, test_steps_vs_reference_kernels).
     assert same.mean() >= 0.999, f"RNG streams diverged in {np.sum(~same)} cells"
     st_g = st_t.cpu().numpy()
     assert np.array_equal(st_g[same, 0], st_or[same, 0])  # selections

@@ -57,6 +57,14 @@ def test_one_step_vs_oracle(cuda, periodic):
     mr_g, sd_g = solver.GetCellState()
     assert pg.shape == po.shape
     same = np.all(sd_g == sd_o, axis=1)
+    # The oracle runs on the host: its cosf/sinf (libm) and the GPU's
+    # __cosf/__sinf differ in the last bits, so post-collision velocities can
+    # differ by an ulp, and a later acceptance test in the same cell (random
+    # number against sigma g / (sigma g)max) that close to its threshold can
+    # go the other way; that cell's stream then consumes a different number
+    # of draws.  Such cells (at most 0.1 %) are left out of the exact
+    # comparison; against the reference's own GPU kernels every cell is
+    # bit-identical (test_steps_vs_reference_kernels).
     assert same.mean() >= 0.999
     counts = (cse[:, 1] - cse[:, 0]).astype(np.int64)
     mask = np.repeat(same, counts)
@@ -150,19 +158,16 @@ def test_steps_vs_reference_kernels(cuda, periodic, steps):
     exact_part = np.all(pg[:, :3] == pr[:, :3], axis=1).mean()
     print(f"steps={steps}: cells with identical RNG state {exact_cells:.6f}, "
           f"particles with identical position {exact_part:.6f}")
-    assert exact_cells >= 0.999
-    if steps == 1:
-        same = np.all(sd_g == sd_r, axis=1)
-        tmp = np.zeros(n, np.uint32)
-        mask = np.ones(n, bool)
-        scale = 3 * 400.0
-        assert np.max(np.abs(vg[mask, :3] - vr[mask, :3])) / scale <= 1e-6
-        assert exact_part > 0.999
-        del tmp, same
-    else:
-        # a single accept decision decided differently by rounding changes
-        # its cell's later history; the bulk stays identical
-        assert exact_part > 0.99
+    # Both sides run on the same GPU with the same intrinsics (__cosf,
+    # __sinf, sqrtf), the same HybridTaus draws and the same rounding steps
+    # (the library writes out as fmaf each multiply-add that the reference's
+    # nvcc build contracts), so every step is bit-identical: RNG states,
+    # positions, velocities and the (sigma g)max / remainder pairs.
+    assert exact_cells == 1.0
+    assert exact_part == 1.0
+    assert np.array_equal(pg[:, :3], pr[:, :3])
+    assert np.array_equal(vg[:, :3], vr[:, :3])
+    assert np.array_equal(mr_g, mr_r)
 
 
 @pytest.mark.parametrize("rng,density", [("taus", 1e20), ("philox", 1e20), ("philox", 6e20)])
@@ -174,7 +179,7 @@ def test_kernel_variants_give_identical_steps(cuda, rng, density):
     collide such cells with one thread (a different Philox stream, by
     design) and are only required to report them as giant cells."""
     nv = KernelVariantCount()
-    assert nv == 8
+    assert nv == 9
     out = []
     for v in range(nv):
         s = make_settings(density=density, rng=rng, init_kind="maxwell", seed=5).set(sample_every=3)
@@ -206,6 +211,34 @@ def test_kernel_variants_give_identical_steps(cuda, rng, density):
         assert np.array_equal(out[0][1][1], out[v][1][1])
         assert np.array_equal(out[0][2], out[v][2], equal_nan=True)
     assert compared >= (nv - 1 if density <= 1e20 else 4)
+
+
+@pytest.mark.parametrize("rng,density", [("taus", 1e20), ("philox", 6e20), ("taus", 1.5e21),
+                                         ("philox", 1.5e21)])
+def test_two_pass_order_matches_the_order_kernel(cuda, rng, density):
+    """The two-pass order (variant 8: a rank pass that puts orig in stable
+    order in place, then a gather of the state) and the one-pass order kernel
+    with the same 256-particle chunks (variant 4) compute identical steps.
+    At 1.5e21 about 365 particles sit in a cell, more than a chunk holds, so
+    every cell takes the giant-cell path of both."""
+    out = []
+    for v in (4, 8):
+        s = make_settings(density=density, rng=rng, init_kind="maxwell", seed=9).set(sample_every=2)
+        solver = DSMCSolver().Init(s)
+        solver.SetKernelVariant(v)
+        solver.InitSystemState()
+        solver.RunSimulationStep(1e-5, 3)
+        solver.StepGraph(1e-5, 3)
+        solver.Sync()
+        out.append((solver.DownloadState(), solver.GetCellState(), solver.Fields(),
+                    solver.Info().giant_cells))
+        solver.close()
+    assert out[0][3] == out[1][3]
+    assert (out[0][3] > 0) == (density > 1e21)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1][0], out[1][1][0])
+    assert np.array_equal(out[0][1][1], out[1][1][1])
+    assert np.array_equal(out[0][2], out[1][2], equal_nan=True)
 
 
 def test_graph_replay_profiles_kernels_without_changing_results(cuda):
