@@ -56,7 +56,6 @@ struct dsmc_handle {
   uint2* gse = nullptr;
   float4* gtri = nullptr;
   float4* gplane = nullptr;
-  float4* gbound = nullptr;
   GridGeom gcgrid{};  // grid of the clearance table gclear
 
   bool has_state = false;
@@ -178,7 +177,7 @@ void free_all(dsmc_handle* h) {
   }
   void* ps[] = {h->orig, h->ntc_list, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
                 h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse,
-                h->gtri, h->gplane, h->gbound, h->mt_state, h->mt_cfg};
+                h->gtri, h->gplane, h->mt_state, h->mt_cfg};
   for (void* p : ps) cudaFree(p);
   h->mt_state = nullptr;
   h->mt_cfg = nullptr;
@@ -243,7 +242,6 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.start_end = h->gse;
     p.geom.tri = h->gtri;
     p.geom.plane = h->gplane;
-    p.geom.bound = h->gbound;
     p.geom.clear = h->gclear;
     p.geom.cgrid = h->gcgrid;
     p.geom.diffuse = h->cfg.wall_diffuse;
@@ -744,7 +742,6 @@ static void free_geometry(dsmcb::GeomDevice& gd) {
   cudaFree(gd.se);
   cudaFree(gd.tri);
   cudaFree(gd.plane);
-  cudaFree(gd.bound);
   gd = dsmcb::GeomDevice{};
 }
 
@@ -786,12 +783,10 @@ static int install_geometry(dsmc_handle* h, dsmcb::GeomDevice& gd) {
   cudaFree(h->gse);
   cudaFree(h->gtri);
   cudaFree(h->gplane);
-  cudaFree(h->gbound);
   h->gflags = gd.flags;
   h->gse = gd.se;
   h->gtri = gd.tri;
   h->gplane = gd.plane;
-  h->gbound = gd.bound;
   h->gclear = nullptr;
   gd = dsmcb::GeomDevice{};
   h->has_geom = false;

@@ -14,11 +14,6 @@
 //      stable order of the reference's sort) are computed
 //   B  NTC pair counts (and remainders); cells with pairs are listed
 //   C  the chunk goes to the mid arrays in sorted order
-// The two-pass form of the same step splits this in two: k_rank_w runs the
-// chunk loop with orig alone (A restores the stable order by rewriting, in
-// place, the orig of the slots whose position changes; B as above), and
-// k_gather_w then moves the state, mid[s] = in[orig[s]], one slot per thread
-// at full occupancy (no per-chunk waits between a warp's gathers).
 // k_ntc_w: the listed cells' NTC selections in place on the mid arrays, a
 // lane per light cell, a warp per dense cell (Philox mode).
 // k_flight_w (flight + keys): streams the sorted particles, 32 at a time per
@@ -33,9 +28,8 @@
 // every cell that fits a chunk.  Gathering through orig lets the scatter write
 // orig alone (one scattered 4-byte store per particle instead of seven).
 //
-// Traffic per particle: k_order_w orig 4 + state 24 read, 24 written (the
-// two-pass form reads orig twice and writes it again where a cell's order
-// changes); k_flight_w 24 read, 24 + key 4 written.  Per cell: 8 B of starts, 16 B of
+// Traffic per particle: k_order_w orig 4 + state 24 read, 24 written;
+// k_flight_w 24 read, 24 + key 4 written.  Per cell: 8 B of starts, 16 B of
 // (sigma g)max read + written, 32 B more in the reference RNG mode, 80 B of
 // sampling sums on sampling steps.
 #include "dsmc_bulk.cuh"
@@ -49,20 +43,18 @@ using namespace dev;
 constexpr uint32_t kWarpTile = 32;  // cells per warp tile, one per lane
 constexpr uint32_t kFlightQ = 64;   // per-warp queue of flights that may reach the body
 
-// ROWS = 7 (order kernel): x y z u v w orig of a chunk; ROWS = 1 (rank
-// pass): orig alone.
-template <int CAPW, int ROWS>
+template <int CAPW>
 struct __align__(16) WarpSmem {
-  static constexpr int kOrig = ROWS - 1;  // orig's row in part
-  float part[2][ROWS][CAPW + 8];  // a chunk, double buffered
-  uint4 lbuf[2 * kWarpTile];      // light-cell list entries not yet in the global list
-  uint32_t cr[kWarpTile];         // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
+  static constexpr int kOrig = 6;  // orig's row in part
+  float part[2][7][CAPW + 8];  // x y z u v w orig of a chunk, double buffered
+  uint4 lbuf[2 * kWarpTile];   // light-cell list entries not yet in the global list
+  uint32_t cr[kWarpTile];      // the chunk's nonempty cells in order: start | end << 16 (chunk-relative)
   unsigned long long mbar[2];
 };
 
-template <int CAPW, int WARPS, int ROWS>
+template <int CAPW, int WARPS>
 constexpr size_t collide_smem_bytes() {
-  return WARPS * sizeof(WarpSmem<CAPW, ROWS>);
+  return WARPS * sizeof(WarpSmem<CAPW>);
 }
 
 // A tile of 32 cells as the lanes see it: lane L holds the start and end of
@@ -157,25 +149,6 @@ static __device__ __noinline__ void giant_order_warp(const StepParams& p, uint32
     p.mid.x[d] = p.in.x[my]; p.mid.y[d] = p.in.y[my]; p.mid.z[d] = p.in.z[my];
     p.mid.u[d] = p.in.u[my]; p.mid.v[d] = p.in.v[my]; p.mid.w[d] = p.in.w[my];
   }
-}
-
-// The same cell in the rank pass: its orig in stable order, in place.  The
-// sorted origs go through the cell's slots of p.mid.x first (the gather pass
-// writes every slot of mid afterwards), so that no lane overwrites an orig
-// another lane still counts against.
-static __device__ __noinline__ void giant_rank_warp(const StepParams& p, uint32_t s, uint32_t e) {
-  const uint32_t n = e - s;
-  const uint32_t lane = lane_id();
-  uint32_t* tmp = reinterpret_cast<uint32_t*>(p.mid.x);
-  if (lane == 0 && p.meta) atomicAdd(&p.meta->giant_cells, 1u);
-  for (uint32_t i = lane; i < n; i += 32) {
-    const uint32_t my = p.in_orig[s + i];
-    uint32_t rank = 0;
-    for (uint32_t j = 0; j < n; j++) rank += (uint32_t)(p.in_orig[s + j] < my);
-    tmp[s + rank] = my;
-  }
-  __syncwarp();
-  for (uint32_t i = lane; i < n; i += 32) p.in_orig[s + i] = tmp[s + i];
 }
 
 // Descents of orig inside a chunk (OR: its n origs).  A cell without one is
@@ -307,14 +280,11 @@ __device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint
 
 // ---------------------------------------------------- order + pair counts ----
 
-// The chunk loop of the order kernel (RANK false) and of the rank pass (RANK
-// true: orig put in stable order in place, no state moved; the gather pass
-// moves it afterwards).
-template <int CAPW, int WARPS, bool RANK>
-__device__ __forceinline__ void order_chunks(const StepParams& p) {
+template <int CAPW, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  using Smem = WarpSmem<CAPW, RANK ? 1 : 7>;
+  using Smem = WarpSmem<CAPW>;
   Smem& S = reinterpret_cast<Smem*>(smem_raw)[warp];
   const bool do_fixup = (p.flags & kDoFixup) != 0;
   const bool do_collide = (p.flags & kDoCollide) != 0;
@@ -410,11 +380,7 @@ __device__ __forceinline__ void order_chunks(const StepParams& p) {
     __syncwarp();
 
     if (C.giant) {
-      if constexpr (RANK) {
-        if (do_fixup) giant_rank_warp(p, C.base, C.base + C.n);
-      } else {
-        giant_order_warp(p, C.base, C.base + C.n);
-      }
+      giant_order_warp(p, C.base, C.base + C.n);
       if (do_collide) {
         // the giant cell's pair count, from lane C.cur's (sigma g)max
         const uint32_t gc = c0 + C.cur;
@@ -434,53 +400,32 @@ __device__ __forceinline__ void order_chunks(const StepParams& p) {
       // element j of the chunk sits at ORA[j + off]
       const uint32_t* ORA = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig]);
       const uint32_t base = C.base, n = C.n;
-      if constexpr (RANK) {
-        // A: the slots of cells with a descent get their orig in stable
-        // order (only those whose position changes are written)
-        if (do_fixup) {
-          const bool desc = cell_has_descent<CAPW>(OR, n, ne, s0, nc);
-          if (desc) S.cr[ne_idx] |= 0x80000000u;
-          const bool any = __any_sync(kFull, desc);
-          __syncwarp();
-          if (any) {
-            for (uint32_t b0 = 0; b0 < n; b0 += 32) {
-              // a strip without a flagged cell keeps its order
-              if (!__any_sync(kFull, desc && s0 < b0 + 32u && s0 + nc > b0)) continue;
-              const uint32_t t = b0 + lane;
-              const uint32_t my = t < n ? OR[t] : 0u;
-              const uint32_t pos = stable_slot(ORA, S.cr, off, b0, n, my, ne, s0);
-              if (t < n && pos != t) p.in_orig[base + pos] = my;
-            }
-          }
-        }
-      } else {
-        float* X = S.part[C.buf][0] + off;
-        float* Y = S.part[C.buf][1] + off;
-        float* Z = S.part[C.buf][2] + off;
-        float* U = S.part[C.buf][3] + off;
-        float* V = S.part[C.buf][4] + off;
-        float* W = S.part[C.buf][5] + off;
-        // A: each particle's sorted position, sorted = (cell, orig), then the
-        // gather of its state through orig straight to that position
-        // (asynchronous 4-byte copies, in flight while the pair counts run).
-        // The origs are distinct, so a particle's rank in its cell is the
-        // number of smaller origs there.
-        if (do_fixup) {
-          if (cell_has_descent<CAPW>(OR, n, ne, s0, nc)) S.cr[ne_idx] |= 0x80000000u;
-          __syncwarp();
-        }
-        for (uint32_t b0 = 0; b0 < n; b0 += 32) {
-          const uint32_t t = b0 + lane;
-          const uint32_t my = t < n ? OR[t] : 0u;
-          const uint32_t pos = do_fixup ? stable_slot(ORA, S.cr, off, b0, n, my, ne, s0) : t;
-          if (t < n) {
-            cp_async4(X + pos, p.in.x + my);
-            cp_async4(Y + pos, p.in.y + my);
-            cp_async4(Z + pos, p.in.z + my);
-            cp_async4(U + pos, p.in.u + my);
-            cp_async4(V + pos, p.in.v + my);
-            cp_async4(W + pos, p.in.w + my);
-          }
+      float* X = S.part[C.buf][0] + off;
+      float* Y = S.part[C.buf][1] + off;
+      float* Z = S.part[C.buf][2] + off;
+      float* U = S.part[C.buf][3] + off;
+      float* V = S.part[C.buf][4] + off;
+      float* W = S.part[C.buf][5] + off;
+      // A: each particle's sorted position, sorted = (cell, orig), then the
+      // gather of its state through orig straight to that position
+      // (asynchronous 4-byte copies, in flight while the pair counts run).
+      // The origs are distinct, so a particle's rank in its cell is the
+      // number of smaller origs there.
+      if (do_fixup) {
+        if (cell_has_descent<CAPW>(OR, n, ne, s0, nc)) S.cr[ne_idx] |= 0x80000000u;
+        __syncwarp();
+      }
+      for (uint32_t b0 = 0; b0 < n; b0 += 32) {
+        const uint32_t t = b0 + lane;
+        const uint32_t my = t < n ? OR[t] : 0u;
+        const uint32_t pos = do_fixup ? stable_slot(ORA, S.cr, off, b0, n, my, ne, s0) : t;
+        if (t < n) {
+          cp_async4(X + pos, p.in.x + my);
+          cp_async4(Y + pos, p.in.y + my);
+          cp_async4(Z + pos, p.in.z + my);
+          cp_async4(U + pos, p.in.u + my);
+          cp_async4(V + pos, p.in.v + my);
+          cp_async4(W + pos, p.in.w + my);
         }
       }
       // B: pair counts (the new remainder is stored now); cells with pairs
@@ -498,12 +443,10 @@ __device__ __forceinline__ void order_chunks(const StepParams& p) {
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      if constexpr (!RANK) {
-        cp_async_wait_all();
-        __syncwarp();
-        // C: the chunk, now in sorted order, to the mid arrays
-        write_chunk(C.buf, base, n);
-      }
+      cp_async_wait_all();
+      __syncwarp();
+      // C: the chunk, now in sorted order, to the mid arrays
+      write_chunk(C.buf, base, n);
     }
     __syncwarp();
     if (n_in_b) {
@@ -518,53 +461,6 @@ __device__ __forceinline__ void order_chunks(const StepParams& p) {
   if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
   __shared__ unsigned long long s_red[WARPS];
   if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
-}
-
-template <int CAPW, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
-  order_chunks<CAPW, WARPS, false>(p);
-}
-
-// Rank pass of the two-pass order (orig in stable order in place, pair counts
-// and cell lists); k_gather_w then moves the state.
-template <int CAPW, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_rank_w(const __grid_constant__ StepParams p) {
-  order_chunks<CAPW, WARPS, true>(p);
-}
-
-// Gather pass of the two-pass order: mid[s] = in[orig[s]] for every slot of
-// the step (start[cells] of them), orig in stable order already.  UNROLL
-// slots per thread, blockDim.x apart, keep their loads in flight together;
-// neighbouring slots mostly have neighbouring origs, so a warp's gathered
-// loads touch few sectors.
-template <int UNROLL>
-__global__ void __launch_bounds__(256) k_gather_w(const __grid_constant__ StepParams p) {
-  const uint32_t n = __ldg(&p.start[p.cells]);
-  const uint32_t span = blockDim.x * UNROLL;
-  for (uint32_t s0 = blockIdx.x * span + threadIdx.x; s0 < n; s0 += gridDim.x * span) {
-    uint32_t o[UNROLL];
-#pragma unroll
-    for (int k = 0; k < UNROLL; k++) {
-      const uint32_t s = s0 + k * blockDim.x;
-      o[k] = s < n ? __ldg(&p.in_orig[s]) : 0u;
-    }
-    float v[6][UNROLL];
-#pragma unroll
-    for (int k = 0; k < UNROLL; k++) {
-      if (s0 + k * blockDim.x < n) {
-        v[0][k] = __ldg(&p.in.x[o[k]]); v[1][k] = __ldg(&p.in.y[o[k]]); v[2][k] = __ldg(&p.in.z[o[k]]);
-        v[3][k] = __ldg(&p.in.u[o[k]]); v[4][k] = __ldg(&p.in.v[o[k]]); v[5][k] = __ldg(&p.in.w[o[k]]);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < UNROLL; k++) {
-      const uint32_t s = s0 + k * blockDim.x;
-      if (s < n) {
-        p.mid.x[s] = v[0][k]; p.mid.y[s] = v[1][k]; p.mid.z[s] = v[2][k];
-        p.mid.u[s] = v[3][k]; p.mid.v[s] = v[4][k]; p.mid.w[s] = v[5][k];
-      }
-    }
-  }
 }
 
 // ------------------------------------------------------- NTC selections ----
@@ -916,36 +812,25 @@ struct LaunchShapeW {
   int device = -1;
   uint32_t n_scan_tiles = 0;
   int per_sm = 0;
-  int gather_per_sm = 0;
 };
 
-constexpr int kGatherUnroll = 4;
-
-// The order kernel, or with RANK the rank pass followed by the gather pass.
-template <int CAPW, int WARPS, int MINB, bool RANK = false>
+template <int CAPW, int WARPS, int MINB>
 cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   LaunchShapeW& ls = cache[dev & 7];
-  void (*kern)(const StepParams);
-  if constexpr (RANK) kern = k_rank_w<CAPW, WARPS, MINB>;
-  else kern = k_order_w<CAPW, WARPS, MINB>;
-  const size_t smem = collide_smem_bytes<CAPW, WARPS, RANK ? 1 : 7>();
+  const size_t smem = collide_smem_bytes<CAPW, WARPS>();
   if (ls.device != dev) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(k_order_w<CAPW, WARPS, MINB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, WARPS * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_order_w<CAPW, WARPS, MINB>,
+                                                      WARPS * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    if (RANK) {
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ls.gather_per_sm, k_gather_w<kGatherUnroll>,
-                                                        256, 0);
-      if (e != cudaSuccess) return e;
-      if (ls.gather_per_sm < 1) return cudaErrorInvalidConfiguration;
-    }
     ls.device = dev;
     ls.per_sm = per_sm;
   }
@@ -953,12 +838,7 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  kern<<<grid, WARPS * 32, smem, stream>>>(p);
-  if (!RANK) return cudaGetLastError();
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  // a full wave: the particle count is known only on the device
-  k_gather_w<kGatherUnroll><<<(uint32_t)(num_sms() * ls.gather_per_sm), 256, 0, stream>>>(p);
+  k_order_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -1057,13 +937,12 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 // CTA-wide ones): (particles per warp chunk, warps per CTA, CTAs per SM the
 // registers are capped for) of the order kernel and the flight kernel's form
 // (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 4;
-// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs); 4 the two-pass order
-// (rank pass (256, 4, 8), then the gather pass) and single flights.
-int cell_kernel_w_variants() { return 5; }
+// one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs).
+int cell_kernel_w_variants() { return 4; }
 
 int cell_kernel_w_capacity(int v) {
-  static const int caps[5] = {256, 128, 128, 128, 256};
-  return caps[v < 0 || v > 4 ? 1 : v];
+  static const int caps[4] = {256, 128, 128, 128};
+  return caps[v < 0 || v > 3 ? 1 : v];
 }
 
 uint32_t cell_kernel_w_tile() { return kWarpTile; }
@@ -1075,7 +954,6 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         case 0: return launch_order_w<256, 4, 4>(p, stream);
         case 2: return launch_order_w<128, 8, 3>(p, stream);
         case 3: return launch_order_w<128, 4, 6>(p, stream);
-        case 4: return launch_order_w<256, 4, 8, true>(p, stream);
         default: return launch_order_w<128, 4, 4>(p, stream);
       }
     case 1:

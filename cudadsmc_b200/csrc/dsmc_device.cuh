@@ -228,10 +228,6 @@ struct GeomView {
   // per bin entry, the triangle's plane (unit normal, offset), packed apart
   // from the vertices so that a cell's planes share cache lines
   const float4* plane;
-  // per bin entry, a sphere holding the triangle (centroid, radius), read
-  // with the planes: a segment that crosses the plane far from the sphere
-  // cannot hit the triangle, whose vertices then stay unread
-  const float4* bound;
   // clearance table: per cell of cgrid (the triangle grid refined by a small
   // factor, same bounds), a lower bound of the distance from any point of the
   // cell to the surface
@@ -272,30 +268,6 @@ __device__ __forceinline__ bool intersect_triangle_rel(float3 o, float3 d, float
   if (v < 0.f || u + v > 1.f) return false;
   *t = __fmul_rn(dot_x(e2, qv), inv);
   return true;
-}
-
-// Whether the segment o + s d (s in [0, dist], d unit) may hit a triangle
-// whose plane P it crosses (signed end distances s0, s1 to the plane), judged
-// by the crossing point against the triangle's bounding sphere S.  The test
-// only ever keeps more than it must: the crossing parameter s0 / (s0 - s1) is
-// taken with a bound E on the rounding of s0 and s1 (the stored plane and
-// the dot products, well above the plane test's tolerance), which moves the
-// crossing point by at most dist * 1.5 E / |s0 - s1| along the segment; the
-// sphere is widened by twice that and by a relative slack for the ray/
-// triangle test's own rounding.  Near-parallel crossings (|s0 - s1| <= 4 E)
-// are always kept.
-__device__ __forceinline__ bool crossing_near(float3 o, float3 d, float dist, float s0, float s1, float4 P,
-                                              float4 S) {
-  const float ds = s0 - s1;
-  const float E = 1e-6f * (fabsf(P.w) + fabsf(o.x) + fabsf(o.y) + fabsf(o.z) + dist + 1.f);
-  if (!(fabsf(ds) > 4.f * E)) return true;
-  const float tau = fminf(fmaxf(s0 / ds, 0.f), 1.f);
-  const float s = tau * dist;
-  const float3 X = make_float3(o.x + d.x * s, o.y + d.y * s, o.z + d.z * s);
-  const float dx = X.x - S.x, dy = X.y - S.y, dz = X.z - S.z;
-  const float r = S.w * (1.f + 1e-5f) + dist * (4.f * E / fabsf(ds)) +
-                  1e-6f * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z) + 1.f);
-  return dx * dx + dy * dy + dz * dz <= r * r;
 }
 
 // Nearest triangle crossed by the segment o + s d, s in [0, dist] (d unit),
@@ -373,14 +345,11 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
     uint2 se_next = make_uint2(0u, 0u);
     if (more) se_next = geo_ld(&G.start_end[cell_of(nx, ny, nz)]);
     for (uint32_t i0 = se.x; i0 < se.y; i0 += 8) {
-      // the planes and bounding spheres of up to 8 of the cell's triangles
-      // in one round of loads
-      float4 P[8], S[8];
+      // the planes of up to 8 of the cell's triangles in one round of loads
+      float4 P[8];
 #pragma unroll
-      for (int k = 0; k < 8; k++) {
+      for (int k = 0; k < 8; k++)
         P[k] = i0 + k < se.y ? geo_ld(&G.plane[i0 + k]) : make_float4(0.f, 0.f, 0.f, 1.f);
-        S[k] = i0 + k < se.y ? geo_ld(&G.bound[i0 + k]) : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         const uint32_t i = i0 + k;
@@ -391,7 +360,6 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
         const float s1 = fmaf(dist, dot_x(pn, d), s0);
         const float tol = __fmul_rn(1e-7f, fabsf(P[k].w) + 1.f);
         if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
-        if (!crossing_near(o, d, dist, s0, s1, P[k], S[k])) continue;
         const float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
         const float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
         const float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);

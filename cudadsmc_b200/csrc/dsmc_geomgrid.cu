@@ -12,8 +12,7 @@
 // order the reference's cell-major loop produces, and k_enclose flags the
 // cells between flagged cells along z (src/reggrid.cpp:49-79).  k_entries
 // writes per entry the triangle's vertices with its face normal packed into
-// .w, its plane (unit normal and offset, evaluated in FP64) and a sphere that
-// holds it (the traversal's crossing-point test).
+// .w, and its plane (unit normal and offset, evaluated in FP64).
 //
 // The arithmetic is that of the host build (dsmc_host.cpp:
 // build_geometry_grid, tri_box_overlap, compiled without contraction) with
@@ -192,13 +191,12 @@ __global__ void __launch_bounds__(256) k_cell_ranges(const uint32_t* start, uint
   }
 }
 
-// Per entry: the triangle's vertices with its face normal in .w, its plane
-// from the vertices in FP64 (unit normal n, offset n . a) rounded to FP32 at
-// the end, and a sphere holding it (centroid, largest vertex distance
-// rounded up).
+// Per entry: the triangle's vertices with its face normal in .w, and its
+// plane from the vertices in FP64 (unit normal n, offset n . a), rounded to
+// FP32 at the end.
 __global__ void __launch_bounds__(256) k_entries(const uint32_t* ids, uint32_t n, const float* verts,
                                                  const uint32_t* tris, const float* normals, float4* tri,
-                                                 float4* plane, float4* bound) {
+                                                 float4* plane) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint32_t t = ids[i];
     const float* a = verts + 3 * (size_t)tris[3 * (size_t)t];
@@ -224,17 +222,6 @@ __global__ void __launch_bounds__(256) k_entries(const uint32_t* ids, uint32_t n
         __dadd_rn(__dadd_rn(__dmul_rn(pn[0], a[0]), __dmul_rn(pn[1], a[1])), __dmul_rn(pn[2], a[2]));
     plane[i] = make_float4(__double2float_rn(pn[0]), __double2float_rn(pn[1]), __double2float_rn(pn[2]),
                            __double2float_rn(w));
-    double cen[3], r2 = 0.0;
-    for (int k = 0; k < 3; k++) cen[k] = ((double)a[k] + (double)b[k] + (double)c[k]) / 3.0;
-    const float* vs[3] = {a, b, c};
-    for (int q = 0; q < 3; q++) {
-      double d2 = 0.0;
-      for (int k = 0; k < 3; k++) d2 += ((double)vs[q][k] - cen[k]) * ((double)vs[q][k] - cen[k]);
-      r2 = fmax(r2, d2);
-    }
-    bound[i] = make_float4((float)cen[0], (float)cen[1], (float)cen[2],
-                           __double2float_ru(sqrt(r2) * (1.0 + 1e-6) + 1e-7 * (fabs(cen[0]) + fabs(cen[1]) +
-                                                                             fabs(cen[2]) + 1.0)));
   }
 }
 
@@ -277,11 +264,9 @@ cudaError_t geometry_entries_device(const uint32_t* start, const uint32_t* ids, 
   cudaError_t e = alloc_n(&out.se, cells);
   if (!e) e = alloc_n(&out.tri, kTriStride * ((size_t)entries + 1));
   if (!e) e = alloc_n(&out.plane, (size_t)entries + 1);
-  if (!e) e = alloc_n(&out.bound, (size_t)entries + 1);
   if (e) return e;
   k_cell_ranges<<<blocks_for(cells), 256>>>(start, out.se, cells);
-  if (entries)
-    k_entries<<<blocks_for(entries), 256>>>(ids, entries, verts, tris, normals, out.tri, out.plane, out.bound);
+  if (entries) k_entries<<<blocks_for(entries), 256>>>(ids, entries, verts, tris, normals, out.tri, out.plane);
   return cudaGetLastError();
 }
 

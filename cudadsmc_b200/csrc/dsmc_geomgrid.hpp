@@ -11,13 +11,12 @@ namespace dsmcb {
 
 // The device arrays the traversal kernels read (cudaMalloc'd; the caller
 // frees them): per cell the has-geometry flag and the entry range, per entry
-// the triangle record (3 float4), the plane and the bounding sphere.
+// the triangle record (3 float4) and the plane.
 struct GeomDevice {
   uint32_t* flags = nullptr;
   uint2* se = nullptr;
   float4* tri = nullptr;
   float4* plane = nullptr;
-  float4* bound = nullptr;
 };
 
 // Bins the mesh (host arrays) into g's frame (bbox, cell and dim set, e.g. by
@@ -28,8 +27,8 @@ cudaError_t build_geometry_device(GeomGrid& g, const float* verts, uint32_t nver
 
 // The entry ranges, triangle records and planes of a given binning (device
 // arrays: start has cells + 1 exclusive offsets, ids the triangle of each
-// entry; verts, tris and normals on the device); allocates out.se, out.tri,
-// out.plane and out.bound.
+// entry; verts, tris and normals on the device); allocates out.se, out.tri
+// and out.plane.
 cudaError_t geometry_entries_device(const uint32_t* start, const uint32_t* ids, uint32_t cells,
                                     uint32_t entries, const float* verts, const uint32_t* tris,
                                     const float* normals, GeomDevice& out);

@@ -104,8 +104,8 @@ struct StepParams {
 
   // buffers
   SoA in;             // state the cell kernel reads (sorted by scatter)
-  uint32_t* in_orig;  // written only by the rank pass of the split variants
-  SoA out;          // state the cell kernel writes (sorted order)
+  const uint32_t* in_orig;
+  SoA out;            // state the cell kernel writes (sorted order)
   SoA mid;            // split variants: the sorted post-collision state between
                       // the collide kernel (which gathers it from `in` through
                       // in_orig) and the flight kernel (which writes `out`)
@@ -150,8 +150,8 @@ cudaError_t launch_scatter(bool with_state, const SoA& src, SoA dst, const uint3
 cudaError_t launch_cell(const StepParams& p, cudaStream_t stream);
 // Variants of the cell kernel.  CTA-wide: 0 (512 threads, 2048 particles per
 // chunk, 1 CTA/SM), 1 (256, 1024, 2), 2 (128, 512, 4), 3 (64, 256, up to 8).
-// Warp-autonomous (particles per warp chunk, warps per CTA): 4 (256, 4),
-// 5 (128, 4), 6 (128, 8), 7 (64, 8).
+// Warp-autonomous (particles per warp chunk, warps per CTA, CTAs per SM):
+// 4 (256, 4, 4), 5 (128, 4, 4), 6 (128, 8, 3), 7 (128, 4, 6).
 int cell_kernel_variants();
 int cell_kernel_chunk_capacity(int variant);
 // Variants at or above 4 use the warp-autonomous kernel, whose tiles are

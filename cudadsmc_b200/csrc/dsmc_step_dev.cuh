@@ -570,6 +570,78 @@ __device__ __forceinline__ bool defer_decide(const StepParams& p, float3 pos, fl
   return path_box_meets_grid(p.geom.grid, pos, e);
 }
 
+// One leg of a nearest-mode flight, from old_pos to pos: its length, its
+// direction and its nearest wall crossing (t along d, bin entry e, the
+// crossed triangle's plane P).
+struct NearestLeg {
+  float3 d;
+  float dist, t;
+  uint32_t e;
+  float4 P;
+};
+enum : int {
+  kLegFree = 0,    // no wall crossed: the leg ends at pos
+  kLegWall = 1,    // a wall crossed from the front
+  kLegInside = 2,  // a face crossed from its back side: the particle is inside the body
+};
+
+// The leg's length and unit direction; false for a leg of (nearly) zero length.
+__device__ __forceinline__ bool leg_path(float3 old_pos, float3 pos, NearestLeg& L) {
+  const float3 seg = make_float3(pos.x - old_pos.x, pos.y - old_pos.y, pos.z - old_pos.z);
+  L.dist = sqrtf(fmaf(seg.z, seg.z, fmaf(seg.x, seg.x, __fmul_rn(seg.y, seg.y))));
+  if (!(L.dist > 1e-12f)) return false;
+  const float idist = 1.f / L.dist;
+  L.d = make_float3(__fmul_rn(seg.x, idist), __fmul_rn(seg.y, idist), __fmul_rn(seg.z, idist));
+  return true;
+}
+
+// The leg's nearest wall crossing.  pretested: the clearance test of this
+// leg is already done (its answer was that the leg may reach the body).  The
+// mesh is closed with outward normals: a face reached from its back side
+// holds a particle inside the body (left over from a fill of a cell the body
+// covers in part), which is removed.
+__device__ __forceinline__ int nearest_leg(const GeomView& G, float3 old_pos, float3 pos, bool pretested,
+                                           NearestLeg& L) {
+  if (!leg_path(old_pos, pos, L)) return kLegFree;
+  if (!pretested) {
+    // a path shorter than the start cell's clearance cannot reach the body
+    const uint32_t cc = coll_cell_id(G.cgrid, old_pos);
+    if (cc != kNone && L.dist < geo_ld(&G.clear[cc])) return kLegFree;
+    // a path outside the geometry grid whose box misses the grid's box
+    if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) return kLegFree;
+  }
+  if (!nearest_wall_hit(G, old_pos, L.d, L.dist, &L.t, &L.e)) return kLegFree;
+  L.P = geo_ld(&G.plane[L.e]);
+  if (fmaf(L.d.z, L.P.z, fmaf(L.d.x, L.P.x, __fmul_rn(L.d.y, L.P.y))) > 0.f) return kLegInside;
+  return kLegWall;
+}
+
+// The wall's answer to a front crossing: from the hit point, set off the
+// wall by 1e-6 m along the outward normal, the particle flies the rest of the
+// leg's length re-emitted (diffuse, at its incoming speed's time) or
+// reflected (specular); old_pos becomes the hit point.
+__device__ __forceinline__ void wall_response(const GeomView& G, const NearestLeg& L, float3& old_pos,
+                                              float3& pos, float3& vel, PhiloxStream& rng) {
+  const float3 n = make_float3(L.P.x, L.P.y, L.P.z);
+  const float3 hp = make_float3(fmaf(n.x, 1e-6f, fmaf(L.d.x, L.t, old_pos.x)),
+                                fmaf(n.y, 1e-6f, fmaf(L.d.y, L.t, old_pos.y)),
+                                fmaf(n.z, 1e-6f, fmaf(L.d.z, L.t, old_pos.z)));
+  const float rest = L.dist - L.t;
+  if (G.diffuse) {
+    const float speed = sqrtf(fmaf(vel.z, vel.z, fmaf(vel.x, vel.x, __fmul_rn(vel.y, vel.y))));
+    vel = diffuse_emit(n, G.wall_vstd, rng);
+    const float tau = speed > 0.f ? rest / speed : 0.f;
+    pos = make_float3(fmaf(vel.x, tau, hp.x), fmaf(vel.y, tau, hp.y), fmaf(vel.z, tau, hp.z));
+  } else {
+    const float vn2 = 2.f * fmaf(vel.z, n.z, fmaf(vel.x, n.x, __fmul_rn(vel.y, n.y)));
+    vel = make_float3(fmaf(-vn2, n.x, vel.x), fmaf(-vn2, n.y, vel.y), fmaf(-vn2, n.z, vel.z));
+    const float sp = sqrtf(fmaf(vel.z, vel.z, fmaf(vel.x, vel.x, __fmul_rn(vel.y, vel.y))));
+    const float3 r = sp > 0.f ? make_float3(vel.x / sp, vel.y / sp, vel.z / sp) : vel;
+    pos = make_float3(fmaf(r.x, rest, hp.x), fmaf(r.y, rest, hp.y), fmaf(r.z, rest, hp.z));
+  }
+  old_pos = hp;
+}
+
 // One particle's flight with the body: IntegrateDev / ProcessCollisionsDev,
 // kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.
 // pretested: the caller already found that the path from pos may reach the
@@ -590,45 +662,11 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
     // flight after each re-emission (extension for bodies with diffuse walls)
     const GeomView& G = p.geom;
     for (uint32_t b = 0; b < kCollisionLimit; b++) {
-      const float3 seg = make_float3(pos.x - old_pos.x, pos.y - old_pos.y, pos.z - old_pos.z);
-      const float dist = sqrtf(fmaf(seg.z, seg.z, fmaf(seg.x, seg.x, __fmul_rn(seg.y, seg.y))));
-      if (!(dist > 1e-12f)) break;
-      // a path shorter than the start cell's clearance cannot reach the body
-      if (!(pretested && b == 0)) {
-        const uint32_t cc = coll_cell_id(G.cgrid, old_pos);
-        if (cc != kNone && dist < geo_ld(&G.clear[cc])) break;
-        // a path outside the geometry grid whose box misses the grid's box
-        if (cc == kNone && !path_box_meets_grid(G.grid, old_pos, pos)) break;
-      }
-      const float idist = 1.f / dist;
-      const float3 d = make_float3(__fmul_rn(seg.x, idist), __fmul_rn(seg.y, idist), __fmul_rn(seg.z, idist));
-      float t;
-      uint32_t e;
-      if (!nearest_wall_hit(G, old_pos, d, dist, &t, &e)) break;
-      const float4 P = geo_ld(&G.plane[e]);
-      const float3 n = make_float3(P.x, P.y, P.z);
-      // the mesh is closed with outward normals: a face reached from its
-      // back side holds a particle inside the body (left over from a fill of
-      // a cell the body covers in part), which is removed
-      if (fmaf(d.z, n.z, fmaf(d.x, n.x, __fmul_rn(d.y, n.y))) > 0.f) return false;
-      // the hit point, set off the wall by 1e-6 m along the outward normal
-      const float3 hp = make_float3(fmaf(n.x, 1e-6f, fmaf(d.x, t, old_pos.x)),
-                                    fmaf(n.y, 1e-6f, fmaf(d.y, t, old_pos.y)),
-                                    fmaf(n.z, 1e-6f, fmaf(d.z, t, old_pos.z)));
-      const float rest = dist - t;
-      if (G.diffuse) {
-        const float speed = sqrtf(fmaf(vel.z, vel.z, fmaf(vel.x, vel.x, __fmul_rn(vel.y, vel.y))));
-        vel = diffuse_emit(n, G.wall_vstd, rng);
-        const float tau = speed > 0.f ? rest / speed : 0.f;
-        pos = make_float3(fmaf(vel.x, tau, hp.x), fmaf(vel.y, tau, hp.y), fmaf(vel.z, tau, hp.z));
-      } else {
-        const float vn2 = 2.f * fmaf(vel.z, n.z, fmaf(vel.x, n.x, __fmul_rn(vel.y, n.y)));
-        vel = make_float3(fmaf(-vn2, n.x, vel.x), fmaf(-vn2, n.y, vel.y), fmaf(-vn2, n.z, vel.z));
-        const float sp = sqrtf(fmaf(vel.z, vel.z, fmaf(vel.x, vel.x, __fmul_rn(vel.y, vel.y))));
-        const float3 r = sp > 0.f ? make_float3(vel.x / sp, vel.y / sp, vel.z / sp) : vel;
-        pos = make_float3(fmaf(r.x, rest, hp.x), fmaf(r.y, rest, hp.y), fmaf(r.z, rest, hp.z));
-      }
-      old_pos = hp;
+      NearestLeg L;
+      const int r = nearest_leg(G, old_pos, pos, pretested && b == 0, L);
+      if (r == kLegFree) break;
+      if (r == kLegInside) return false;
+      wall_response(G, L, old_pos, pos, vel, rng);
     }
   } else if (p.has_geom) {
     const GeomView& G = p.geom;

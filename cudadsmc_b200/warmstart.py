@@ -215,11 +215,15 @@ def generate(conds, seed, settle, sample, group=64, log=print):
     return out
 
 
-def convergence(conds, seeds, refs, ref_noise, window, max_steps, threshold, warm=None):
-    """Steps until the systematic block-state error of a window (sampled in
-    two halves, noise subtracted) against the reference falls to `threshold`
-    (None if not within max_steps), the error curves and the wall time."""
+def convergence(conds, seeds, refs, ref_noise, window, max_steps, threshold, warm=None, stride=None):
+    """Steps until the systematic block-state error of the trailing window of
+    `window` steps (its two halves give the noise, which is subtracted)
+    against the reference falls to `threshold`, checked every `stride` steps
+    once a whole window has run (None if not within max_steps); the error
+    curves (one value per check) and the wall time."""
     import cudadsmc_b200 as cb
+    stride = stride or window
+    assert window % stride == 0 and (window // stride) % 2 == 0 or stride == window
     t0 = time.time()
     sols = [make_solver(c, s) for c, s in zip(conds, seeds)]
     for i, sol in enumerate(sols):
@@ -230,18 +234,29 @@ def convergence(conds, seeds, refs, ref_noise, window, max_steps, threshold, war
     batch = cb.DSMCBatch(sols)
     done = [None] * len(sols)
     curves = [[] for _ in sols]
+    segs = []  # per segment of `stride` steps: each member's (sums, samples)
+    per = window // stride
+    seg_len = [stride] if stride != window else [window // 2, window - window // 2]
     steps = 0
     while steps < max_steps and any(d is None for d in done):
-        halves = []
-        for w in (window // 2, window - window // 2):
+        for w in seg_len:
             for sol in sols:
                 sol.ResetSamples()
             batch.Step(w)
             batch.Sync()
-            halves.append([sol.SampleStatistics()[::2] for sol in sols])
-        steps += window
+            segs.append([sol.SampleStatistics()[::2] for sol in sols])
+            steps += w
+        need = per if stride != window else 2
+        if len(segs) < need:
+            continue
+        last = segs[-need:]
+        segs = last
+        h = need // 2
         for i, c in enumerate(conds):
-            (s1, n1), (s2, n2) = halves[0][i], halves[1][i]
+            s1 = sum(seg[i][0] for seg in last[:h])
+            n1 = sum(seg[i][1] for seg in last[:h])
+            s2 = sum(seg[i][0] for seg in last[h:])
+            n2 = sum(seg[i][1] for seg in last[h:])
             b1 = block_state_from_sums(s1, n1, c)
             b2 = block_state_from_sums(s2, n2, c)
             mid = block_state_from_sums(s1 + s2, n1 + n2, c)
@@ -264,6 +279,8 @@ def main():
     ap.add_argument("--sample", type=int, default=1500)
     ap.add_argument("--ref-sample", type=int, default=3000)
     ap.add_argument("--window", type=int, default=200)
+    ap.add_argument("--stride", type=int, default=None,
+                    help="check the trailing window every STRIDE steps (default: the window)")
     ap.add_argument("--max-steps", type=int, default=4000)
     ap.add_argument("--threshold", type=float, default=0.02)
     ap.add_argument("--epochs", type=int, default=300)
@@ -329,12 +346,12 @@ def main():
     for i in range(0, args.test, args.group):
         sl = slice(i, min(args.test, i + args.group))
         d, cc, w = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
-                               args.max_steps, args.threshold)
+                               args.max_steps, args.threshold, stride=args.stride)
         cold_steps += d
         cold_curves += cc
         cold_wall += w
         d, cc, w = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
-                               args.max_steps, args.threshold, warm=pred[sl])
+                               args.max_steps, args.threshold, warm=pred[sl], stride=args.stride)
         warm_steps += d
         warm_curves += cc
         warm_wall += w
@@ -344,7 +361,7 @@ def main():
         for i in range(0, args.test, args.group):
             sl = slice(i, min(args.test, i + args.group))
             d, cc, _ = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
-                                   args.max_steps, args.threshold, warm=ref_cells[sl])
+                                   args.max_steps, args.threshold, warm=ref_cells[sl], stride=args.stride)
             ideal_steps += d
             ideal_curves += cc
     cs = np.array([s if s is not None else np.nan for s in cold_steps], np.float64)
@@ -355,7 +372,8 @@ def main():
     res = {
         "train_conditions": args.train, "test_conditions": args.test,
         "settle_steps": args.settle, "sample_steps": args.sample, "ref_sample_steps": args.ref_sample,
-        "window": args.window, "threshold": args.threshold, "error_blocks": f"{BLOCK}^3 cells",
+        "window": args.window, "stride": args.stride or args.window, "threshold": args.threshold,
+        "error_blocks": f"{BLOCK}^3 cells",
         "generation_s": t_gen, "training_s": t_train, "prediction_s": t_pred,
         "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1],
         "error_definition": "relative L2 over blocks of 4^3 cells of (n/n_inf, u/U, v/U, w/U, T/T_inf) "

@@ -319,7 +319,7 @@ def test_inflow_injection_matches_oracle(cuda):
     sol.close()
 
 
-@pytest.mark.parametrize("variant", [5, 7, 0, 8])
+@pytest.mark.parametrize("variant", [5, 7, 0])
 def test_step_matches_oracle(cuda, variant):
     """Whole timesteps of a sphere flow in the capsule workload's mode: the
     GPU steps 12 times to develop the flow, then each of three more steps is

@@ -86,7 +86,7 @@ def test_clearance_never_exceeds_distance(cuda, grid):
     solver.close()
 
 
-@pytest.mark.parametrize("variant", [0, 4, 5, 7, 8])
+@pytest.mark.parametrize("variant", [0, 4, 5, 7])
 def test_full_steps_keep_particles_outside(cuda, variant):
     solver, _, _ = make_solver()
     solver.SetKernelVariant(variant)
