@@ -1145,7 +1145,6 @@ int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out)
   ip.kind = DSMC_INIT_MAXWELL;
   ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
   ip.cell_state = fill_state(h);
-  ip.exact_moments = 1;
   ip.reject_inside = geo;
   if (geo) {
     ip.geom = base_params(h, c.dt).geom;

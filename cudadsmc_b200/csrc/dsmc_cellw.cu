@@ -411,14 +411,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
       // (asynchronous 4-byte copies, in flight while the pair counts run).
       // The origs are distinct, so a particle's rank in its cell is the
       // number of smaller origs there.
+      // (strips of 32 slots without a cell that has a descent keep their
+      // order)
+      bool desc = false;
       if (do_fixup) {
-        if (cell_has_descent<CAPW>(OR, n, ne, s0, nc)) S.cr[ne_idx] |= 0x80000000u;
+        desc = cell_has_descent<CAPW>(OR, n, ne, s0, nc);
+        if (desc) S.cr[ne_idx] |= 0x80000000u;
         __syncwarp();
       }
+      const bool any_desc = __any_sync(kFull, desc);
       for (uint32_t b0 = 0; b0 < n; b0 += 32) {
         const uint32_t t = b0 + lane;
         const uint32_t my = t < n ? OR[t] : 0u;
-        const uint32_t pos = do_fixup ? stable_slot(ORA, S.cr, off, b0, n, my, ne, s0) : t;
+        const bool rank = any_desc && __any_sync(kFull, desc && s0 < b0 + 32u && s0 + nc > b0);
+        const uint32_t pos = rank ? stable_slot(ORA, S.cr, off, b0, n, my, ne, s0) : t;
         if (t < n) {
           cp_async4(X + pos, p.in.x + my);
           cp_async4(Y + pos, p.in.y + my);

@@ -483,41 +483,6 @@ __global__ void k_init_fill(const __grid_constant__ InitParams p) {
   }
 }
 
-// A fill's sampling noise in the cell moments, taken out: each cell's
-// velocities are shifted to the cell state's mean and their deviations
-// scaled so that the cell's temperature (the mean square deviation per
-// component, as the sampling measures it) is the state's exactly.  Without
-// this the seeded moments carry a noise of about 1/sqrt(particles) per cell,
-// which stays in the flow until the particles leave the domain.  Cells of
-// fewer than two particles keep their draws.  One thread per cell.
-__global__ void k_fill_moments(const __grid_constant__ InitParams p) {
-  for (uint32_t cell = blockIdx.x * blockDim.x + threadIdx.x; cell < p.cells; cell += gridDim.x * blockDim.x) {
-    const uint32_t s = p.cell_slot[cell], n = p.cell_count[cell];
-    if (s == kNone || n < 2) continue;
-    double mu = 0.0, mv = 0.0, mw = 0.0;
-    for (uint32_t i = s; i < s + n; i++) {
-      mu += p.out.u[i];
-      mv += p.out.v[i];
-      mw += p.out.w[i];
-    }
-    mu /= n;
-    mv /= n;
-    mw /= n;
-    double ss = 0.0;
-    for (uint32_t i = s; i < s + n; i++) {
-      const double a = p.out.u[i] - mu, b = p.out.v[i] - mv, c = p.out.w[i] - mw;
-      ss += a * a + b * b + c * c;
-    }
-    const float4 st = p.cell_state[cell];
-    const double var = ss / (3.0 * n);
-    const double scale = var > 0.0 ? (double)st.w / sqrt(var) : 0.0;
-    for (uint32_t i = s; i < s + n; i++) {
-      p.out.u[i] = (float)(st.x + (p.out.u[i] - mu) * scale);
-      p.out.v[i] = (float)(st.y + (p.out.v[i] - mv) * scale);
-      p.out.w[i] = (float)(st.z + (p.out.w[i] - mw) * scale);
-    }
-  }
-}
 
 // --------------------------------------------------------------- inflow ----
 
@@ -899,7 +864,6 @@ cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream) {
   const uint64_t total = (uint64_t)p.cells * p.ppc;
   const uint32_t grid = grid_for(total, 256, 8);
   k_init_fill<<<grid, 256, 0, stream>>>(p);
-  if (p.exact_moments && p.cell_state) k_fill_moments<<<grid_for(p.cells, 256, 8), 256, 0, stream>>>(p);
   return cudaGetLastError();
 }
 

@@ -221,8 +221,6 @@ struct InitParams {
   GeomView geom;
   const float4* cell_point;   // optional per cell: a point outside the mesh (w = 1) or none (w = 0)
   SoA out;
-  int exact_moments;          // with cell_state: each cell's velocities shifted and scaled to its
-                              // mean and temperature exactly (cells of 2 or more particles)
 };
 cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream);
 // Fraction of every cell outside the mesh (64 stratified points per cell)

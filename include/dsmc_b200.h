@@ -233,10 +233,7 @@ int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out);
  * kernels/dsmc_kernel.cu:394-427): fields5 holds per cell (x fastest) the
  * number density n [m^-3], the mean velocity (u, v, w) [m/s] and the
  * temperature T [K].  Each cell receives n V_c / F_N particles (rounded
- * stochastically from the seed) drawn from the Maxwellian at (u, v, w, T),
- * then shifted and scaled so that every cell of two or more particles holds
- * the mean velocity and temperature exactly (a quiet start: no sampling
- * noise in the seeded moments);
+ * stochastically from the seed) drawn from the Maxwellian at (u, v, w, T);
  * cells covered by the mesh stay empty, as in dsmc_init_state; non-finite or
  * non-positive n gives an empty cell, a non-finite or non-positive T the
  * configured temperature.  Resets the sampling accumulators. */
