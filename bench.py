@@ -42,7 +42,9 @@ ARGON = dict(gas_mass=6.63e-26, gas_diam=4.17e-10, gas_tref=273.0, gas_omega=0.8
 
 
 def wl_capsule_4m():
-    """Hypersonic argon over a blunt capsule, 4M particles, 128x64x64 cells."""
+    """Hypersonic argon over a blunt capsule, 128x64x64 cells: 4.26M particles
+    at the free-stream fill, about 3.3M once the flow around the body has
+    developed (the timed steps)."""
     dom = (1.2, 0.6, 0.6)
     dim = (128, 64, 64)
     cell_v = (dom[0] / dim[0]) * (dom[1] / dim[1]) * (dom[2] / dim[2])
@@ -61,7 +63,8 @@ def wl_capsule_4m():
     return dict(name="capsule_mach7_argon_4M_128x64x64", settings=s, mesh=mesh,
                 desc=f"argon VHS w=0.81, Mach {mach:.0f} (U={U:.0f} m/s), T=200 K, n=1e20, "
                      "diffuse capsule wall 500 K (nose r=0.15 m, 20 deg cone, ~20k tris), "
-                     "inflow -x, outflow elsewhere, 1.2x0.6x0.6 m, 128x64x64 cells, ~4.2M particles")
+                     "inflow -x, outflow elsewhere, 1.2x0.6x0.6 m, 128x64x64 cells, 4.26M particles at the fill, "
+                     "about 3.3M in the developed flow")
 
 
 def wl_sphere_500k():
