@@ -570,9 +570,7 @@ def run_batch(args, rank, world):
     batch = cb.DSMCBatch(sols)
     stream = torch.cuda.Stream()  # a real stream: the batch's branches fork from it
     batch.SetStream(stream.cuda_stream)
-    batch.Step(args.warmup)
-    variants = batch.Autotune(steps=2) if args.tune_steps > 0 else None
-    batch.Step(2)
+    batch.Step(args.warmup + 2)
     batch.Sync()
 
     def particle_steps():
@@ -617,14 +615,16 @@ def run_batch(args, rank, world):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded members, generated mesh)",
         "config": {"workload": wl["name"], "description": wl["desc"], "members": len(sols),
                    "particles_now_total": int(sum(n_now)), "particles_now_min": int(min(n_now)),
-                   "particles_now_max": int(max(n_now)), "cell_kernel_variants": variants,
+                   "particles_now_max": int(max(n_now)),
+                   "batched_launches": "each stage once per step for all members (order kernel in "
+                                       "the (128 particles, 4 warps) shape)",
                    "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
                    "l2_policy": "working set of all members (several GB) > 126 MB L2"},
         "sequential": {"value": seq_value, "ms_per_step": seq_ms / k2,
                        "note": "same members, one graph launch per member per step, one stream"},
-        "gpu_launches": args.steps * sum(kernels_per_step(m["settings"], v, True)
-                                         for m, v in zip(wl["members"],
-                                                         variants or [5] * len(wl["members"]))),
+        # the batch launches each stage once for all members: scan, scatter,
+        # order, inflow plan and fill, NTC, flight, mesh, sampling
+        "gpu_launches": args.steps * 9,
         "clocks": clk.summary(),
     }
     batch.close()
@@ -639,10 +639,11 @@ def run_batch(args, rank, world):
 def single_same_size(args, particles, members, stream):
     """One sphere flow as large as the whole ensemble (the members' cells
     together, 256 x 128 x 128 for 64 members of 64 x 32 x 32, and their
-    particles together), stepped with the same kernels: the throughput a
-    batch could reach if its members' per-step launches cost nothing beyond
-    their particles' work, the bound a persistent batched kernel would aim
-    at."""
+    particles together), stepped with the same kernels.  Not the same physics:
+    its particles are spread evenly (7.5 per cell, where the members hold
+    0.8-30) and one body covers a far smaller share of its cells than each
+    member's does, so its kernels' work per particle is lower than the
+    ensemble's."""
     import torch
     import cudadsmc_b200 as cb
     f = max(1, round(members ** (1.0 / 3.0)))

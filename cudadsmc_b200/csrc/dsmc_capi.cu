@@ -318,29 +318,53 @@ cudaError_t ensure_side(dsmc_handle* h) {
 
 // Inflow injection of every inflow face on `stream` (timed when on the
 // handle's stream).
+dsmcb::InjectParams inject_params(dsmc_handle* h, const dsmcb::Inflow& in, float dt, uint2 seed) {
+  dsmcb::InjectParams ip{};
+  ip.grid = h->grid;
+  ip.cells = h->cells;
+  ip.inflow = in;
+  ip.dt = dt;
+  ip.seed = seed;
+  ip.capacity = h->capacity;
+  ip.remainder = h->inj_rem + in.face;
+  ip.st = soa_of(h->A);
+  ip.keys = h->keys;
+  ip.count = h->count;
+  ip.tile_sum = h->tile_sum;
+  ip.n_scan_tiles = h->n_scan_tiles;
+  ip.plan = h->inj_plan + 2 * in.face;
+  ip.meta = h->meta;
+  return ip;
+}
+
 cudaError_t enqueue_inflow(dsmc_handle* h, float dt, uint2 seed, cudaStream_t stream) {
   for (const auto& in : h->inflows) {
-    dsmcb::InjectParams ip{};
-    ip.grid = h->grid;
-    ip.cells = h->cells;
-    ip.inflow = in;
-    ip.dt = dt;
-    ip.seed = seed;
-    ip.capacity = h->capacity;
-    ip.remainder = h->inj_rem + in.face;
-    ip.st = soa_of(h->A);
-    ip.keys = h->keys;
-    ip.count = h->count;
-    ip.tile_sum = h->tile_sum;
-    ip.n_scan_tiles = h->n_scan_tiles;
-    ip.plan = h->inj_plan + 2 * in.face;
-    ip.meta = h->meta;
+    const dsmcb::InjectParams ip = inject_params(h, in, dt, seed);
     const cudaError_t e = stream == h->stream
                               ? timed(h, 3, [&] { return dsmcb::launch_inject(ip, stream); })
                               : dsmcb::launch_inject(ip, stream);
     if (e) return e;
   }
   return cudaSuccess;
+}
+
+// The cell kernels' parameters of one timestep (split: the split kernels,
+// which gather the state from A through orig; else the fused kernel, which
+// reads it scattered into B).
+dsmcb::StepParams step_params(dsmc_handle* h, float dt, bool split) {
+  dsmcb::StepParams p = base_params(h, dt);
+  p.in = split ? soa_of(h->A) : soa_of(h->B);
+  p.mid = soa_of(h->B);
+  p.in_orig = h->orig;
+  p.out = soa_of(h->A);
+  p.out_key = h->keys;
+  p.flags = dsmcb::kDoFixup | dsmcb::kDoCollide | dsmcb::kDoMove | dsmcb::kDoKeys | dsmcb::kPadded;
+  if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
+  p.cell_variant = h->variant;
+  p.defer_list = h->orig;
+  p.ntc_light = h->ntc_list;
+  p.ntc_heavy = h->ntc_list + h->cells;
+  return p;
 }
 
 // One timestep: scan -> scatter -> cell (-> inflow injection).  With the split
@@ -364,18 +388,7 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
                                  h->capacity, h->stream);
   });
   if (e) return e;
-  dsmcb::StepParams p = base_params(h, dt);
-  p.in = split ? soa_of(h->A) : soa_of(h->B);
-  p.mid = soa_of(h->B);
-  p.in_orig = h->orig;
-  p.out = soa_of(h->A);
-  p.out_key = h->keys;
-  p.flags = dsmcb::kDoFixup | dsmcb::kDoCollide | dsmcb::kDoMove | dsmcb::kDoKeys | dsmcb::kPadded;
-  if (h->cfg.sample_every > 0) p.flags |= dsmcb::kDoSample;
-  p.cell_variant = h->variant;
-  p.defer_list = h->orig;
-  p.ntc_light = h->ntc_list;
-  p.ntc_heavy = h->ntc_list + h->cells;
+  const dsmcb::StepParams p = step_params(h, dt, split);
   // the inflow branch (not while the injection itself is being timed: its
   // events are on the handle's stream)
   const bool fork = split && !h->inflows.empty() && h->side &&
@@ -1814,12 +1827,18 @@ struct dsmc_batch {
   std::vector<dsmc_handle*> members;
   std::vector<float> dt;
   std::vector<uint64_t> gen;
-  std::vector<cudaStream_t> branch;
-  std::vector<cudaEvent_t> ev;  // fork + one join per member
   cudaStream_t stream = nullptr;
   bool own_stream = true;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // the batched launches' device tables (written before each capture): the
+  // members' parameters, their sort arrays, the inflow faces, and per stage
+  // the members' first blocks
+  dsmcb::StepParams* d_params = nullptr;
+  dsmcb::SortArgs* d_sort = nullptr;
+  dsmcb::InjectParams* d_inj = nullptr;
+  uint32_t* d_block0 = nullptr;
+  size_t cap_members = 0, cap_inj = 0;
   std::string err;
 };
 
@@ -1839,8 +1858,10 @@ void batch_drop_graph(dsmc_batch* b) {
 
 void batch_free(dsmc_batch* b) {
   batch_drop_graph(b);
-  for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
-  for (cudaStream_t s : b->branch) cudaStreamDestroy(s);
+  cudaFree(b->d_params);
+  cudaFree(b->d_sort);
+  cudaFree(b->d_inj);
+  cudaFree(b->d_block0);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -1852,30 +1873,130 @@ bool batch_graph_current(const dsmc_batch* b, const std::vector<float>& dt) {
   return true;
 }
 
+// Block offsets of a stage: member i gets blocks[i] (at least 1) blocks.
+void offsets(const std::vector<uint32_t>& blocks, std::vector<uint32_t>& out) {
+  out.push_back(0);
+  for (uint32_t k : blocks) out.push_back(out.back() + std::max(k, 1u));
+}
+
+// Shares of `wave` blocks by weight, at least one block each.
+std::vector<uint32_t> shares(const std::vector<double>& w, uint32_t wave) {
+  double total = 0.0;
+  for (double x : w) total += x;
+  std::vector<uint32_t> out(w.size(), 1u);
+  for (size_t i = 0; i < w.size(); i++)
+    if (total > 0.0) out[i] = std::max(1u, (uint32_t)std::lround((double)wave * w[i] / total));
+  return out;
+}
+
+// The batch's step: each stage of the split step launched once for all
+// members, member i running its own parameters in a share of the grid
+// (dsmcb::BatchOf), in the stage order of a member stepped alone (scan,
+// scatter, order, inflow injection, NTC, flight, mesh, sampling).  Shares
+// follow the members' particle counts at capture time (cells for the scan and
+// the sampling), so that every stage fills the GPU once with the whole
+// ensemble's work instead of once per member.
 int batch_capture(dsmc_batch* b, const std::vector<float>& dt) {
   batch_drop_graph(b);
   const size_t n = b->members.size();
-  std::vector<cudaStream_t> saved(n);
-  std::vector<bool> prof(n);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e) return batch_fail(b, DSMC_ERR_CUDA, std::string("batch sync: ") + cudaGetErrorString(e));
+  std::vector<dsmcb::StepParams> P(n);
+  std::vector<dsmcb::SortArgs> A(n);
+  std::vector<dsmcb::InjectParams> I;
+  std::vector<double> np(n), nc(n);
+  uint32_t max_tiles = 0;
   for (size_t i = 0; i < n; i++) {
-    const cudaError_t es = ensure_side(b->members[i]);
-    if (es) return batch_fail(b, DSMC_ERR_CUDA, std::string("side stream: ") + cudaGetErrorString(es));
-  }
-  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-  if (!e) e = cudaEventRecord(b->ev[0], b->stream);
-  for (size_t i = 0; i < n && !e; i++) {
     dsmc_handle* h = b->members[i];
-    saved[i] = h->stream;
-    prof[i] = h->profiling;
-    h->profiling = false;
-    h->stream = b->branch[i];
-    e = cudaStreamWaitEvent(b->branch[i], b->ev[0], 0);
-    if (!e) e = enqueue_step(h, dt[i]);
-    if (!e) e = cudaEventRecord(b->ev[i + 1], b->branch[i]);
-    if (!e) e = cudaStreamWaitEvent(b->stream, b->ev[i + 1], 0);
-    h->stream = saved[i];
-    h->profiling = prof[i];
+    if (h->mt_on) return batch_fail(b, DSMC_ERR_STATE, "the -mt collisions cannot run in a batch");
+    Meta m{};
+    const int st = read_meta(h, m);
+    if (st) return batch_fail(b, st, h->err);
+    np[i] = (double)m.n_alive + (double)m.n_pending + 1.0;
+    nc[i] = (double)h->cells;
+    // every member runs the split kernels with the order kernel's
+    // (128 particles, 4 warps, 4 CTAs) shape and tiles of 32 cells, whatever
+    // shape it uses stepped alone
+    P[i] = step_params(h, dt[i], true);
+    P[i].cell_variant = 5;
+    P[i].cells_per_tile = (int)dsmcb::cell_kernel_w_tile();
+    P[i].n_tiles = (h->cells + dsmcb::cell_kernel_w_tile() - 1) / dsmcb::cell_kernel_w_tile();
+    A[i] = dsmcb::SortArgs{h->count, h->cursor, h->start, h->tile_sum, h->orig, h->keys,
+                           h->meta, h->cells, h->n_scan_tiles, h->capacity};
+    for (const auto& in : h->inflows) I.push_back(inject_params(h, in, dt[i], P[i].seed));
+    max_tiles = std::max(max_tiles, h->n_scan_tiles);
   }
+  const size_t flight_smem = (size_t)max_tiles * 4u;
+  uint32_t wave[5];
+  e = dsmcb::cell_batch_waves(wave, flight_smem);
+  if (e) return batch_fail(b, DSMC_ERR_CUDA, std::string("batch shapes: ") + cudaGetErrorString(e));
+  // per stage: scan, scatter, order, NTC, flight, mesh, sampling; then the
+  // inflow plan (one block per face) and fill
+  std::vector<std::vector<uint32_t>> blocks(9);
+  for (size_t i = 0; i < n; i++) blocks[0].push_back(b->members[i]->n_scan_tiles);
+  // the order kernel's and the NTC kernel's work per tile of 32 cells has a
+  // floor (a tile's chunk costs about as much with few particles as with
+  // eight per cell): weigh their shares by cells as well as particles
+  std::vector<double> wcell(n);
+  for (size_t i = 0; i < n; i++) wcell[i] = np[i] + 8.0 * nc[i];
+  blocks[1] = shares(np, (uint32_t)dsmcb::num_sms() * 4u);
+  blocks[2] = shares(wcell, wave[0]);
+  for (size_t i = 0; i < n; i++)  // the order kernel needs no more warps than tiles
+    blocks[2][i] = std::min(blocks[2][i], std::max(1u, (P[i].n_tiles + 3u) / 4u));
+  blocks[3] = shares(wcell, wave[1]);
+  blocks[4] = shares(np, wave[2]);
+  blocks[5] = shares(np, wave[3]);
+  blocks[6] = shares(nc, wave[4]);
+  blocks[7].assign(I.size(), 1u);
+  blocks[8].assign(I.size(), 4u);
+  std::vector<uint32_t> off;
+  std::vector<size_t> at(9);
+  std::vector<uint32_t> total(9);
+  for (int k = 0; k < 9; k++) {
+    at[k] = off.size();
+    offsets(blocks[k], off);
+    total[k] = off.back();
+  }
+  // device tables (grown as needed)
+  if (n > b->cap_members) {
+    cudaFree(b->d_params);
+    cudaFree(b->d_sort);
+    b->d_params = nullptr;
+    b->d_sort = nullptr;
+    b->cap_members = 0;
+    e = cudaMalloc(&b->d_params, n * sizeof(dsmcb::StepParams));
+    if (!e) e = cudaMalloc(&b->d_sort, n * sizeof(dsmcb::SortArgs));
+    if (e) return batch_fail(b, DSMC_ERR_OOM, "batch tables");
+    b->cap_members = n;
+  }
+  if (I.size() > b->cap_inj) {
+    cudaFree(b->d_inj);
+    b->d_inj = nullptr;
+    b->cap_inj = 0;
+    e = cudaMalloc(&b->d_inj, I.size() * sizeof(dsmcb::InjectParams));
+    if (e) return batch_fail(b, DSMC_ERR_OOM, "batch tables");
+    b->cap_inj = I.size();
+  }
+  cudaFree(b->d_block0);
+  b->d_block0 = nullptr;
+  e = cudaMalloc(&b->d_block0, off.size() * sizeof(uint32_t));
+  if (!e) e = cudaMemcpy(b->d_params, P.data(), n * sizeof(dsmcb::StepParams), cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy(b->d_sort, A.data(), n * sizeof(dsmcb::SortArgs), cudaMemcpyHostToDevice);
+  if (!e && !I.empty())
+    e = cudaMemcpy(b->d_inj, I.data(), I.size() * sizeof(dsmcb::InjectParams), cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy(b->d_block0, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e) return batch_fail(b, DSMC_ERR_CUDA, std::string("batch tables: ") + cudaGetErrorString(e));
+  const uint32_t nm = (uint32_t)n, ni = (uint32_t)I.size();
+  auto sv = [&](int k) { return dsmcb::BatchOf<dsmcb::SortArgs>{b->d_sort, b->d_block0 + at[k], nm}; };
+  auto pv = [&](int k) { return dsmcb::BatchOf<dsmcb::StepParams>{b->d_params, b->d_block0 + at[k], nm}; };
+  auto iv = [&](int k) { return dsmcb::BatchOf<dsmcb::InjectParams>{b->d_inj, b->d_block0 + at[k], ni}; };
+  e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (!e) e = dsmcb::launch_scan_b(sv(0), total[0], b->stream);
+  if (!e) e = dsmcb::launch_scatter_b(sv(1), total[1], b->stream);
+  if (!e) e = dsmcb::launch_cell_stage_b(0, pv(2), total[2], flight_smem, b->stream);
+  if (!e && ni) e = dsmcb::launch_inject_b(iv(7), total[7], iv(8), total[8], flight_smem, b->stream);
+  for (int st = 1; st < 5 && !e; st++)
+    e = dsmcb::launch_cell_stage_b(st, pv(2 + st), total[2 + st], flight_smem, b->stream);
   cudaError_t e2 = cudaStreamEndCapture(b->stream, &b->graph);
   if (e || e2) {
     batch_drop_graph(b);
@@ -1914,17 +2035,7 @@ int dsmc_batch_create(dsmc_handle* const* members, uint32_t n, dsmc_batch** out)
     b->members.push_back(members[i]);
   }
   b->gen.assign(n, 0);
-  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-  for (uint32_t i = 0; i < n && !e; i++) {
-    cudaStream_t s = nullptr;
-    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (!e) b->branch.push_back(s);
-  }
-  for (uint32_t i = 0; i <= n && !e; i++) {
-    cudaEvent_t ev = nullptr;
-    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
-    if (!e) b->ev.push_back(ev);
-  }
+  const cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e) {
     g_create_error = std::string("batch streams: ") + cudaGetErrorString(e);
     batch_free(b);

@@ -280,8 +280,10 @@ __device__ __forceinline__ void flush_cells(const uint4* buf, uint32_t cnt, uint
 
 // ---------------------------------------------------- order + pair counts ----
 
-template <int CAPW, int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
+// The order kernel's body for block vb of vg (the launch's grid, or a
+// member's share of a batched launch).
+template <int CAPW, int WARPS>
+__device__ __forceinline__ void order_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   using Smem = WarpSmem<CAPW>;
@@ -297,8 +299,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
   }
   __syncwarp();
 
-  const uint32_t nwarps = gridDim.x * WARPS;
-  const uint32_t gw = blockIdx.x * WARPS + warp;
+  const uint32_t nwarps = vg * WARPS;
+  const uint32_t gw = vb * WARPS + warp;
   TileQueue tq{nwarps, gw + nwarps, p.meta ? &p.meta->tile_next : nullptr};
   WTile A = load_tile(p, gw);
   uint32_t pend = 0, tb = 0;
@@ -469,6 +471,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_const
   if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
 }
 
+template <int CAPW, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
+  order_body<CAPW, WARPS>(p, blockIdx.x, gridDim.x);
+}
+template <int CAPW, int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_order_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  uint32_t vb, vg;
+  const StepParams& p = bv.locate(vb, vg);
+  order_body<CAPW, WARPS>(p, vb, vg);
+}
+
 // ------------------------------------------------------- NTC selections ----
 
 constexpr uint32_t kNtcClaim = 256;  // claim slots per warp: the largest chunk
@@ -484,7 +497,7 @@ constexpr uint32_t kNtcClaim = 256;  // claim slots per warp: the largest chunk
 // more (with a static split the blocks holding both a second round of light
 // cells and a dense cell set the kernel's length).
 template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ StepParams p) {
+__device__ __forceinline__ void ntc_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
   __shared__ uint32_t s_claim[WARPS][kNtcClaim];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
@@ -494,7 +507,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ St
   uint32_t col = 0;
   double sum_g = 0.0;
   const uint32_t nl = p.meta->n_light, nh = p.meta->n_heavy;
-  const uint32_t gw = blockIdx.x * WARPS + warp, nw = gridDim.x * WARPS;
+  const uint32_t gw = vb * WARPS + warp, nw = vg * WARPS;
   for (uint32_t h = gw; h < nh; h += nw) {
     const uint4 e = p.ntc_heavy[h];
     GlobalVel acc{p.mid.u, p.mid.v, p.mid.w, e.y};
@@ -533,6 +546,17 @@ __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ St
     block_add(&p.meta->collisions, (unsigned long long)col, s_col);
     block_add(&p.meta->sum_g, sum_g, s_g);
   }
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ StepParams p) {
+  ntc_body<WARPS>(p, blockIdx.x, gridDim.x);
+}
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_ntc_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  uint32_t vb, vg;
+  const StepParams& p = bv.locate(vb, vg);
+  ntc_body<WARPS>(p, vb, vg);
 }
 
 // ------------------------------------------------ flight + keys + sample ----
@@ -589,8 +613,8 @@ __device__ __forceinline__ void list_deferred(const StepParams& p, const uint32_
 // state of a group is loaded two iterations ahead, and in nearest mode the
 // clearance lookup of its deferral test one iteration ahead, so that both
 // latencies are covered.
-template <int WARPS, int MINB>
-__global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
+template <int WARPS>
+__device__ __forceinline__ void flight_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
   __shared__ uint32_t s_q[WARPS][kFlightQ];
   extern __shared__ uint32_t s_tile[];  // this block's next-step counts per scan tile
   for (uint32_t t = threadIdx.x; t < p.n_scan_tiles; t += blockDim.x) s_tile[t] = 0;
@@ -603,9 +627,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
   const bool piped = split && p.geom.nearest;
   uint32_t* q = s_q[warp];
   // this warp's groups: per of the ceil(n / 32) groups from gb, particles [gb * 32, end)
-  const uint32_t ngroups = (n + 31u) / 32u, nwarps = gridDim.x * WARPS;
+  const uint32_t ngroups = (n + 31u) / 32u, nwarps = vg * WARPS;
   const uint32_t per = (ngroups + nwarps - 1u) / nwarps;
-  const uint32_t gb = min((blockIdx.x * WARPS + warp) * per, ngroups);
+  const uint32_t gb = min((vb * WARPS + warp) * per, ngroups);
   const uint32_t end = min(min(gb + per, ngroups) * 32u, n);
   const uint32_t stride = 32u;
   const uint32_t g0 = gb * 32u + lane;
@@ -658,6 +682,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_cons
   if (p.meta) block_add(&p.meta->removed, removed, s_rm);
   __syncthreads();
   flush_tile_hist(s_tile, p.tile_sum, p.n_scan_tiles);
+}
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
+  flight_body<WARPS>(p, blockIdx.x, gridDim.x);
+}
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  uint32_t vb, vg;
+  const StepParams& p = bv.locate(vb, vg);
+  flight_body<WARPS>(p, vb, vg);
 }
 
 // Paired form of k_flight_w: lane L flies particles 2L and 2L+1 of each group
@@ -770,12 +805,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_con
 // The flight with the body is inlined, at 2 CTAs per SM for its registers:
 // the list is a partial wave whose time is one traversal's chain of loads,
 // and a call's spills lengthened it (47 -> 35 us for 61k flights).
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
+__device__ __forceinline__ void mesh_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const uint32_t n = p.meta->n_defer;
   uint32_t removed = 0;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+  for (uint32_t base = vb * blockDim.x; base < n; base += vg * blockDim.x) {
     const uint32_t i = base + threadIdx.x;
     const bool go = i < n;
     uint32_t g = 0;
@@ -795,21 +829,41 @@ __global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ St
   if (p.meta) block_add(&p.meta->removed, removed, s_rm);
 }
 
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
+  mesh_body(p, blockIdx.x, gridDim.x);
+}
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_mesh_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  uint32_t vb, vg;
+  const StepParams& p = bv.locate(vb, vg);
+  mesh_body(p, vb, vg);
+}
+
 // FP64 sampling after the flights, one cell per thread (the reference's
 // SampleCellStatisticsDev order: each cell's particles in sorted order, with
 // their velocities after the move); returns at once on other steps.
-__global__ void __launch_bounds__(256) k_sample_w(const __grid_constant__ StepParams p) {
+__device__ __forceinline__ void sample_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const bool do_sample =
       (p.flags & kDoSample) &&
       ((p.flags & kSampleForce) || (p.sample_every > 0 && step % (uint32_t)p.sample_every == 0));
   if (!do_sample) return;
-  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < p.cells; c += gridDim.x * blockDim.x) {
+  for (uint32_t c = vb * blockDim.x + threadIdx.x; c < p.cells; c += vg * blockDim.x) {
     const uint32_t s = __ldg(&p.start[c]), e = __ldg(&p.start[c + 1]);
     GlobalVel a{p.out.u, p.out.v, p.out.w, s};
     sample_cell(p.acc, p.cells, c, (int)(e - s), a);
   }
-  if (p.meta && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&p.meta->samples, 1u);
+  if (p.meta && vb == 0 && threadIdx.x == 0) atomicAdd(&p.meta->samples, 1u);
+}
+
+__global__ void __launch_bounds__(256) k_sample_w(const __grid_constant__ StepParams p) {
+  sample_body(p, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_sample_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  uint32_t vb, vg;
+  const StepParams& p = bv.locate(vb, vg);
+  sample_body(p, vb, vg);
 }
 
 // ------------------------------------------------------------- launches ----
@@ -980,6 +1034,52 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
       if (p.flags & kDoSample) return launch_sample_w(p, stream);
       return cudaSuccess;
   }
+}
+
+// Batched forms of the split kernels for ensembles: the order kernel in the
+// (128 particles, 4 warps, 4 CTAs per SM) shape, single-particle flights.
+cudaError_t cell_batch_waves(uint32_t wave[5], size_t flight_smem) {
+  const size_t osmem = collide_smem_bytes<128, 4>();
+  cudaError_t e = cudaFuncSetAttribute(k_order_wb<128, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)osmem);
+  if (e != cudaSuccess) return e;
+  int per[5] = {0, 0, 0, 0, 0};
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_order_wb<128, 4, 4>, 128, osmem);
+  if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_ntc_wb<kNtcWarps>, kNtcWarps * 32, 0);
+  if (!e)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_flight_wb<kFlightWarps, 4>, kFlightWarps * 32,
+                                                      flight_smem);
+  if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[3], k_mesh_wb<2>, 256, 0);
+  per[4] = 8;
+  if (e != cudaSuccess) return e;
+  for (int k = 0; k < 5; k++) {
+    if (per[k] < 1) return cudaErrorInvalidConfiguration;
+    wave[k] = (uint32_t)(num_sms() * per[k]);
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32_t blocks, size_t flight_smem,
+                                cudaStream_t stream) {
+  if (blocks == 0) return cudaSuccess;
+  switch (stage) {
+    case 0:
+      k_order_wb<128, 4, 4><<<blocks, 128, collide_smem_bytes<128, 4>(), stream>>>(bv);
+      break;
+    case 1:
+      k_ntc_wb<kNtcWarps><<<blocks, kNtcWarps * 32, 0, stream>>>(bv);
+      break;
+    case 2:
+      k_flight_wb<kFlightWarps, 4><<<blocks, kFlightWarps * 32, flight_smem, stream>>>(bv);
+      break;
+    case 3:
+      k_mesh_wb<2><<<blocks, 256, 0, stream>>>(bv);
+      break;
+    default:
+      k_sample_wb<<<blocks, 256, 0, stream>>>(bv);
+      break;
+  }
+  return cudaGetLastError();
 }
 
 cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream) {

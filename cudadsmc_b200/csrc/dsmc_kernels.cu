@@ -72,11 +72,11 @@ __global__ void k_index(GridGeom g, const float* __restrict__ x, const float* __
 // its offset is the sum of the per-tile totals before it, which the producer
 // kernels accumulated alongside the counts.  Resets the counts and the
 // scatter's cursors.
-__global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor, uint32_t* start,
-                                              uint32_t cells, const uint32_t* tile_sum, Meta* meta,
-                                              int bump) {
+__device__ __forceinline__ void scan_body(uint32_t* count, uint32_t* cursor, uint32_t* start,
+                                          uint32_t cells, const uint32_t* tile_sum, Meta* meta, int bump,
+                                          const uint32_t vb, const uint32_t vg) {
   __shared__ uint32_t s_warp[8], s_part[8];
-  const uint32_t b = blockIdx.x;
+  const uint32_t b = vb;
   // the block's counts and the totals of the tiles before it, loaded together
   const uint32_t c0 = b * kScanTile + threadIdx.x * 8;
   // 8 whole counts, read and written 16 bytes at a time where the arrays
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
       }
     }
   }
-  if (b == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) {
+  if (b == vg - 1 && threadIdx.x == blockDim.x - 1) {
     start[cells] = run;
     meta->n_scatter = meta->n_alive + meta->n_pending;
     meta->n_pending = 0;
@@ -157,6 +157,17 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
   }
 }
 
+__global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor, uint32_t* start,
+                                              uint32_t cells, const uint32_t* tile_sum, Meta* meta,
+                                              int bump) {
+  scan_body(count, cursor, start, cells, tile_sum, meta, bump, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_scan_b(const __grid_constant__ BatchOf<SortArgs> bv) {
+  uint32_t vb, vg;
+  const SortArgs& a = bv.locate(vb, vg);
+  scan_body(a.count, a.cursor, a.start, a.cells, a.tile_sum, a.meta, 1, vb, vg);
+}
+
 // Scatter into sorted order: dst[start[key] + ticket] = src[i], orig = i.  The
 // tickets come from per-cell cursors (one atomic per distinct key per group of
 // 32).  Each warp takes kScatterU groups of 32 consecutive particles at once,
@@ -167,18 +178,17 @@ __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor,
 constexpr int kScatterU = 4;
 
 template <bool STATE>
-__global__ void __launch_bounds__(256, 4) k_scatter(SoA src, SoA dst, const uint32_t* __restrict__ keys,
-                                                    const uint32_t* __restrict__ start,
-                                                    uint32_t* cursor, uint32_t* __restrict__ orig,
-                                                    uint32_t cells, uint32_t* tile_sum,
-                                                    uint32_t n_scan_tiles, Meta* meta,
-                                                    uint32_t capacity) {
-  if (blockIdx.x == 0)
+__device__ __forceinline__ void scatter_body(SoA src, SoA dst, const uint32_t* __restrict__ keys,
+                                             const uint32_t* __restrict__ start, uint32_t* cursor,
+                                             uint32_t* __restrict__ orig, uint32_t cells,
+                                             uint32_t* tile_sum, uint32_t n_scan_tiles, Meta* meta,
+                                             uint32_t capacity, const uint32_t vb, const uint32_t vg) {
+  if (vb == 0)
     for (uint32_t t = threadIdx.x; t < n_scan_tiles; t += blockDim.x) tile_sum[t] = 0;
   const uint32_t n = meta->n_scatter;
   const uint32_t lane = lane_id();
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t gw = (vb * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (vg * blockDim.x) >> 5;
   constexpr int U = kScatterU;
   const uint32_t stride = nw * 32u * U;
   // keys of the next iteration load while this one's tickets are in flight
@@ -242,6 +252,25 @@ __global__ void __launch_bounds__(256, 4) k_scatter(SoA src, SoA dst, const uint
       orig[d] = i;
     }
   }
+}
+
+template <bool STATE>
+__global__ void __launch_bounds__(256, 4) k_scatter(SoA src, SoA dst, const uint32_t* __restrict__ keys,
+                                                    const uint32_t* __restrict__ start,
+                                                    uint32_t* cursor, uint32_t* __restrict__ orig,
+                                                    uint32_t cells, uint32_t* tile_sum,
+                                                    uint32_t n_scan_tiles, Meta* meta,
+                                                    uint32_t capacity) {
+  scatter_body<STATE>(src, dst, keys, start, cursor, orig, cells, tile_sum, n_scan_tiles, meta, capacity,
+                      blockIdx.x, gridDim.x);
+}
+// orig only (the split kernels)
+__global__ void __launch_bounds__(256, 4) k_scatter_b(const __grid_constant__ BatchOf<SortArgs> bv) {
+  uint32_t vb, vg;
+  const SortArgs& a = bv.locate(vb, vg);
+  const SoA none{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  scatter_body<false>(none, none, a.keys, a.start, a.cursor, a.orig, a.cells, a.tile_sum, a.n_scan_tiles,
+                      a.meta, a.capacity, vb, vg);
 }
 
 // ------------------------------------------------------------ sort stage ----
@@ -488,8 +517,8 @@ __global__ void k_init_fill(const __grid_constant__ InitParams p) {
 
 // Plan: number of particles the face injects this step (carrying the
 // fractional remainder), reserved after the particles already in the array.
-__global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* plan) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void inject_plan_body(const InjectParams& p, uint32_t* plan, const uint32_t vb) {
+  if (threadIdx.x != 0 || vb != 0) return;
   const float want = fmaf(__fmul_rn(p.inflow.number_flux, p.inflow.area), p.dt, *p.remainder);
   uint32_t k = want > 0.f ? (uint32_t)want : 0u;
   const uint32_t have = p.meta->n_alive + p.meta->n_pending;
@@ -502,6 +531,15 @@ __global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* 
   plan[1] = k;
   p.meta->n_pending += k;
   p.meta->injected += k;
+}
+
+__global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* plan) {
+  inject_plan_body(p, plan, blockIdx.x);
+}
+__global__ void k_inject_plan_b(const __grid_constant__ BatchOf<InjectParams> bv) {
+  uint32_t vb, vg;
+  const InjectParams& p = bv.locate(vb, vg);
+  inject_plan_body(p, p.plan, vb);
 }
 
 // Inward normal speed of the drifting Maxwellian weighted by flux,
@@ -530,7 +568,8 @@ __device__ __forceinline__ float sample_flux_normal(float s, PhiloxStream& r) {
 __device__ __forceinline__ float& comp(float3& a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 __device__ __forceinline__ float compc(const float3& a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 
-__global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint32_t* plan) {
+__device__ __forceinline__ void inject_fill_body(const InjectParams& p, const uint32_t* plan,
+                                                 const uint32_t vb, const uint32_t vg) {
   extern __shared__ uint32_t s_tile[];
   const uint32_t step = p.meta->step;
   for (uint32_t t = threadIdx.x; t < p.n_scan_tiles; t += blockDim.x) s_tile[t] = 0;
@@ -542,7 +581,7 @@ __global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint
   const GridGeom& g = p.grid;
   const float cmp = p.inflow.vstd * 1.41421356f;
   const float s = sign * compc(p.inflow.stream, ax) / cmp;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < k; base += gridDim.x * blockDim.x) {
+  for (uint32_t base = vb * blockDim.x; base < k; base += vg * blockDim.x) {
     const uint32_t i = base + threadIdx.x;
     const bool active = i < k;
     bool live = false;
@@ -578,6 +617,15 @@ __global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint
   }
   __syncthreads();
   flush_tile_hist(s_tile, p.tile_sum, p.n_scan_tiles);
+}
+
+__global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint32_t* plan) {
+  inject_fill_body(p, plan, blockIdx.x, gridDim.x);
+}
+__global__ void k_inject_fill_b(const __grid_constant__ BatchOf<InjectParams> bv) {
+  uint32_t vb, vg;
+  const InjectParams& p = bv.locate(vb, vg);
+  inject_fill_body(p, p.plan, vb, vg);
 }
 
 }  // namespace
@@ -864,6 +912,24 @@ cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream) {
   const uint64_t total = (uint64_t)p.cells * p.ppc;
   const uint32_t grid = grid_for(total, 256, 8);
   k_init_fill<<<grid, 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream) {
+  if (blocks) k_scan_b<<<blocks, 256, 0, stream>>>(bv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream) {
+  if (blocks) k_scatter_b<<<blocks, 256, 0, stream>>>(bv);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_inject_b(const BatchOf<InjectParams>& plan, uint32_t plan_blocks,
+                            const BatchOf<InjectParams>& fill, uint32_t fill_blocks, size_t fill_smem,
+                            cudaStream_t stream) {
+  if (plan_blocks) k_inject_plan_b<<<plan_blocks, 32, 0, stream>>>(plan);
+  if (fill_blocks) k_inject_fill_b<<<fill_blocks, 256, fill_smem, stream>>>(fill);
   return cudaGetLastError();
 }
 

@@ -132,6 +132,40 @@ struct StepParams {
                            // collide kernel has read it)
 };
 
+// A batched launch: one grid for several members (instances of the step),
+// member m owning blocks [block0[m], block0[m + 1]) of it; each block runs the
+// member's kernel body with its index and count inside that share, as if the
+// member's kernel had been launched alone with that grid.
+template <class T>
+struct BatchOf {
+  const T* items;          // per member, in device memory
+  const uint32_t* block0;  // members + 1 block offsets
+  uint32_t members;
+  __device__ __forceinline__ const T& locate(uint32_t& vb, uint32_t& vg) const {
+    uint32_t lo = 0, hi = members;  // the last member whose first block is at or before this one
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (block0[mid] <= blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    vb = blockIdx.x - block0[lo];
+    vg = block0[lo + 1] - block0[lo];
+    return items[lo];
+  }
+};
+
+// Per member, the arrays of the scan and the scatter (batched launches).
+struct SortArgs {
+  uint32_t* count;
+  uint32_t* cursor;
+  uint32_t* start;
+  uint32_t* tile_sum;
+  uint32_t* orig;
+  const uint32_t* keys;
+  Meta* meta;
+  uint32_t cells, n_scan_tiles, capacity;
+};
+
 // Launchers (all asynchronous on `stream`).
 cudaError_t launch_index(const GridGeom& g, uint32_t cells, const float* x, const float* y,
                          const float* z, uint32_t n, uint32_t* keys, uint32_t* count,
@@ -259,5 +293,21 @@ cudaError_t launch_inject(const InjectParams& p, cudaStream_t stream);
 
 int num_sms();
 uint32_t grid_for(uint64_t work, int threads, int per_sm);
+
+// Batched launches of the step's kernels over the members of an ensemble
+// (BatchOf; every member's blocks run its own parameters).
+cudaError_t launch_scan_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream);
+cudaError_t launch_scatter_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream);
+// One block of 32 threads per entry for the plan; the fill's blocks shared
+// among the entries.
+cudaError_t launch_inject_b(const BatchOf<InjectParams>& plan, uint32_t plan_blocks,
+                            const BatchOf<InjectParams>& fill, uint32_t fill_blocks, size_t fill_smem,
+                            cudaStream_t stream);
+// Full-wave block counts of the batched cell stages: order, NTC, flight, mesh,
+// sampling.
+cudaError_t cell_batch_waves(uint32_t wave[5], size_t flight_smem);
+// Stage 0 order, 1 NTC, 2 flight, 3 mesh, 4 sampling.
+cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32_t blocks, size_t flight_smem,
+                                cudaStream_t stream);
 
 }  // namespace dsmcb

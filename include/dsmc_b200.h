@@ -310,13 +310,17 @@ int dsmc_autotune(dsmc_handle* h, float dt, int steps, int* best, float* ms_per_
 
 /* Batches (no counterpart in the reference, which runs one solver per
  * process): independent handles of uneven size advanced together, one CUDA
- * graph launch per timestep with one branch per member, so small instances
- * run concurrently.  Members must live on the current device and appear once;
- * the batch does not own them (destroy the batch first).  Batch work is
- * ordered on the batch stream, not on the members' streams: call
- * dsmc_batch_sync before using a member on its own.  The graph is captured on
- * the first step and again whenever a dt or a member's launch set changes
- * (kernel variant, mesh, stream).  Results equal stepping each member alone. */
+ * graph launch per timestep in which each kernel of the step runs once for
+ * all members (each member in a share of the grid that follows its particle
+ * count), so that the ensemble fills the GPU like one large instance.
+ * Members run the split kernels with the order kernel's (128 particles,
+ * 4 warps) shape whatever shape they use alone; the -mt collisions are
+ * refused.  Members must live on the current device and appear once; the
+ * batch does not own them (destroy the batch first).  Batch work is ordered
+ * on the batch stream, not on the members' streams: call dsmc_batch_sync
+ * before using a member on its own.  The graph is captured on the first step
+ * and again whenever a dt or a member's launch set changes (mesh, stream).
+ * Results equal stepping each member alone with that shape. */
 typedef struct dsmc_batch dsmc_batch;
 int dsmc_batch_create(dsmc_handle* const* members, uint32_t n, dsmc_batch** out);
 int dsmc_batch_destroy(dsmc_batch* b);
@@ -328,8 +332,9 @@ int dsmc_batch_set_stream(dsmc_batch* b, void* stream);
 int dsmc_batch_step(dsmc_batch* b, const float* dt, int nsteps);
 /* Synchronises the batch stream and reports the members' device error flags. */
 int dsmc_batch_sync(dsmc_batch* b);
-/* dsmc_autotune for every member (each advances by (count - 4) * (steps + 2) steps);
- * variants (optional) receives the chosen variant per member. */
+/* dsmc_autotune for every member, for the shape it uses when stepped alone
+ * (each advances by (count - 4) * (steps + 2) steps); variants (optional)
+ * receives the chosen variant per member. */
 int dsmc_batch_autotune(dsmc_batch* b, const float* dt, int steps, int* variants);
 
 /* SampleCellStatistics (kernels/dsmc_kernel.cu:892-910): adds the current
