@@ -690,7 +690,8 @@ def run_e2e(args, wl, rank, world, dev, variant):
     step is one replay of the step's graph (dsmc_step_graph) followed by an
     asynchronous copy of that step's collision totals into pinned host memory
     (dsmc_totals_async), which the host reads while the next step runs (after
-    enqueueing step i it waits for step i-1's copy); the sampled fields are
+    enqueueing step i it waits for step i-4's copy, so that a pause of the
+    host shorter than four steps leaves the GPU busy); the sampled fields are
     read back at the end (d2h)."""
     import torch
     sol = build_solver(wl, seed_offset=rank)
@@ -699,12 +700,15 @@ def run_e2e(args, wl, rank, world, dev, variant):
     sol.InitSystemState()
     state = sol.DownloadState()  # the initial state, as a host would provide it
     host = torch.from_numpy(state).pin_memory()
-    tot = torch.zeros((2, 24), dtype=torch.uint8).pin_memory()
+    lag, ring = 4, 8  # totals read 4 steps behind, from a ring of 8 pinned slots
+    tot = torch.zeros((ring, 24), dtype=torch.uint8).pin_memory()
     fields_host = torch.zeros((sol.Info().cells, 5), dtype=torch.float64).pin_memory()
-    ev = [torch.cuda.Event(), torch.cuda.Event()]
+    ev = [torch.cuda.Event() for _ in range(ring)]
     dt = wl["settings"]["dt"]
-    # as many steps as the device-timed region: a run uploads its state once
-    k = max(3, args.steps if args.e2e_steps is None else min(args.steps, args.e2e_steps))
+    # a run of at least 1000 steps (as many as the device-timed region when
+    # that is longer): a DSMC run uploads its state once and steps thousands
+    # of times, so a short timed region would measure the upload instead
+    k = max(3, max(args.steps, 1000) if args.e2e_steps is None else args.e2e_steps)
     sol.UploadState(host.numpy(), soa=True)  # warm the path once (captures the step graph)
     sol.StepGraph(dt, 3)
     sol.Sync()
@@ -717,13 +721,14 @@ def run_e2e(args, wl, rank, world, dev, variant):
     totals = None
     for i in range(k):
         sol.StepGraph(dt, 1)
-        sol.TotalsAsync(tot[i % 2].data_ptr())
-        ev[i % 2].record()
-        if i:
-            ev[(i - 1) % 2].synchronize()
-            totals = sol.TotalsFromBytes(tot[(i - 1) % 2].numpy())
-    ev[(k - 1) % 2].synchronize()
-    totals = sol.TotalsFromBytes(tot[(k - 1) % 2].numpy())
+        sol.TotalsAsync(tot[i % ring].data_ptr())
+        ev[i % ring].record()
+        if i >= lag:
+            ev[(i - lag) % ring].synchronize()
+            totals = sol.TotalsFromBytes(tot[(i - lag) % ring].numpy())
+    for j in range(max(0, k - lag), k):
+        ev[j % ring].synchronize()
+        totals = sol.TotalsFromBytes(tot[j % ring].numpy())
     fields = sol.Fields(out=fields_host.numpy())
     t1 = time.perf_counter()
     pst = sol.Info().particle_steps - i0
@@ -733,9 +738,9 @@ def run_e2e(args, wl, rank, world, dev, variant):
     return {"value": total / el, "unit": "particle-timesteps/s",
             "h2d_bytes_per_step": int(state.nbytes / k),
             "d2h_bytes_per_step": int(24 + fields.nbytes / k), "steps": k,
-            "note": "upload of the initial pinned state + per step one C-ABI dsmc_step_graph and an "
-                    "asynchronous totals read into pinned memory (read by the host during the next "
-                    "step) + the sampled fields at the end"}
+            "note": f"a {k}-step run: upload of the initial pinned state + per step one C-ABI "
+                    "dsmc_step_graph and an asynchronous totals read into pinned memory (read by the "
+                    f"host {lag} steps later) + the sampled fields at the end"}
 
 
 # ---------------------------------------------------------- reference arm ---
@@ -772,7 +777,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=None,
-                    help="steps of the end-to-end leg (default: --steps)")
+                    help="steps of the end-to-end leg (default: --steps, at least 1000)")
     ap.add_argument("--tune-steps", type=int, default=10,
                     help="steps per launch shape of the autotuner (0: use --variant)")
     ap.add_argument("--variant", type=int, default=5,

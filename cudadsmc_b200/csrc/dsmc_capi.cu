@@ -53,6 +53,7 @@ struct dsmc_handle {
   dsmcb::GeomGrid ggrid;
   uint32_t* gflags = nullptr;
   float* gclear = nullptr;
+  float2* greach = nullptr;  // per bin entry (null: the mesh's scale is too large for it)
   uint2* gse = nullptr;
   float4* gtri = nullptr;
   float4* gplane = nullptr;
@@ -176,8 +177,8 @@ void free_all(dsmc_handle* h) {
     h->A[i] = h->B[i] = nullptr;
   }
   void* ps[] = {h->orig, h->ntc_list, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
-                h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->gse,
-                h->gtri, h->gplane, h->mt_state, h->mt_cfg};
+                h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->greach,
+                h->gse, h->gtri, h->gplane, h->mt_state, h->mt_cfg};
   for (void* p : ps) cudaFree(p);
   h->mt_state = nullptr;
   h->mt_cfg = nullptr;
@@ -243,6 +244,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.tri = h->gtri;
     p.geom.plane = h->gplane;
     p.geom.clear = h->gclear;
+    p.geom.reach = h->greach;
     p.geom.cgrid = h->gcgrid;
     p.geom.diffuse = h->cfg.wall_diffuse;
     p.geom.nearest = h->cfg.geom_nearest;
@@ -793,6 +795,8 @@ static int install_geometry(dsmc_handle* h, dsmcb::GeomDevice& gd) {
   const uint32_t fc = gc * cfac * cfac * cfac;
   cudaFree(h->gflags);
   cudaFree(h->gclear);
+  cudaFree(h->greach);
+  h->greach = nullptr;
   cudaFree(h->gse);
   cudaFree(h->gtri);
   cudaFree(h->gplane);
@@ -823,6 +827,20 @@ static int install_geometry(dsmc_handle* h, dsmcb::GeomDevice& gd) {
     if (!ce) ce = cudaDeviceSynchronize();
     cudaFree(ddist);
     CK(h, ce, "clearance table");
+    // Per bin entry, how far and how steeply a particle leaving the entry's
+    // triangle must fly for the traversal to find no wall.  The set-off of
+    // 1 um from the wall must stay several roundings of a coordinate: bodies
+    // within 2 m of the origin.
+    float mag = 0.f;
+    for (int k = 0; k < 6; k++) mag = std::max(mag, std::fabs(g.bbox[k]));
+    const size_t entries = g.tri_ids.size();
+    if (mag < 2.0f && entries) {
+      CK(h, dalloc(&h->greach, entries), "geometry alloc");
+      gv.plane = h->gplane;
+      ce = dsmcb::launch_entry_reach(gv, (uint32_t)entries, cmin, 1e-7f, 4e-6f, h->greach, nullptr);
+      if (!ce) ce = cudaDeviceSynchronize();
+      CK(h, ce, "entry reach");
+    }
   }
   h->has_geom = true;
   h->cfg.geometry = 1;
@@ -926,6 +944,16 @@ int dsmc_get_geometry_grid(dsmc_handle* h, float bbox[6], float cell[3], int dim
   if (tri_ids) std::memcpy(tri_ids, g.tri_ids.data(), n * 4);
   if (planes && n) CK(h, cudaMemcpy(planes, h->gplane, n * sizeof(float4), cudaMemcpyDeviceToHost), "read planes");
   if (n_entries) *n_entries = g.tri_ids.size();
+  return DSMC_OK;
+}
+
+int dsmc_get_entry_reach(dsmc_handle* h, float* out, uint64_t cap, uint64_t* n_entries) {
+  if (!h) return DSMC_ERR_ARG;
+  if (!h->has_geom) return fail(h, DSMC_ERR_STATE, "no geometry grid (dsmc_set_mesh)");
+  const size_t total = h->greach ? h->ggrid.tri_ids.size() : 0;
+  const size_t n = std::min<size_t>(cap, total);
+  if (out && n) CK(h, cudaMemcpy(out, h->greach, n * sizeof(float2), cudaMemcpyDeviceToHost), "read reach");
+  if (n_entries) *n_entries = total;
   return DSMC_OK;
 }
 

@@ -128,6 +128,11 @@ __device__ __forceinline__ uint2 geo_ld(const uint2* a) {
   asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(r.x), "=r"(r.y) : "l"(a), "l"(l2_keep()));
   return r;
 }
+__device__ __forceinline__ float2 geo_ld(const float2* a) {
+  float2 r;
+  asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(r.x), "=f"(r.y) : "l"(a), "l"(l2_keep()));
+  return r;
+}
 __device__ __forceinline__ float geo_ld(const float* a) {
   float r;
   asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(a), "l"(l2_keep()));
@@ -228,6 +233,12 @@ struct GeomView {
   // per bin entry, the triangle's plane (unit normal, offset), packed apart
   // from the vertices so that a cell's planes share cache lines
   const float4* plane;
+  // per bin entry, (r, k): a particle leaving the entry's triangle outward
+  // (re-emitted or reflected from it) along a path shorter than r whose
+  // direction makes more than k with the normal (the sine of its elevation)
+  // crosses no listed triangle; r = 0 where that holds for no path; null:
+  // no table
+  const float2* reach;
   // clearance table: per cell of cgrid (the triangle grid refined by a small
   // factor, same bounds), a lower bound of the distance from any point of the
   // cell to the surface

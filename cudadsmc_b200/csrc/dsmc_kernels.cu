@@ -878,6 +878,141 @@ __global__ void k_fine_clearance(const __grid_constant__ GeomView g, GridGeom fi
   }
 }
 
+__device__ __forceinline__ double axis_of(const double3& v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// The slope bound of a triangle U that rises above T's plane, seen from T:
+// the least k such that height(x) - tol <= k * sigma(x) at U's three
+// vertices (so on all of U, both sides being linear) for one in-plane
+// half-plane sigma <= 0 that holds T (an edge's outer side, or a direction
+// of a vertex's normal cone: 3 edges and 7 directions per vertex).  As
+// sigma(x) <= dist(x, T), every point of U then lies at most tol + k * dist
+// above T's plane.  Infinity where no half-plane gives a bound.
+__device__ double rise_slope(const double3 V[3], const double3 un[3], double3 n, const double3 W[3], double tol) {
+  double best = 1e300;
+  for (int c = 0; c < 24; c++) {
+    // c < 3: edge c's outer normal (edge c runs from V[c] to V[c+1]); then 7
+    // directions between the outer normals of the two edges at each vertex
+    double3 u, P;
+    if (c < 3) {
+      u = un[c];
+      P = V[c];
+    } else {
+      const int k = (c - 3) / 7, m = (c - 3) % 7;  // vertex k: edges k - 1 and k
+      const double t = (m + 1) / 8.0;
+      const double3 a = un[(k + 2) % 3], b = un[k];
+      u = make_double3((1 - t) * a.x + t * b.x, (1 - t) * a.y + t * b.y, (1 - t) * a.z + t * b.z);
+      const double l = sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
+      u = make_double3(u.x / l, u.y / l, u.z / l);
+      P = V[k];
+    }
+    double lo = 0.0, hi = 1e300;
+    bool ok = true;
+    for (int q = 0; q < 3 && ok; q++) {
+      const double3 d = make_double3(W[q].x - V[0].x, W[q].y - V[0].y, W[q].z - V[0].z);
+      const double a = n.x * d.x + n.y * d.y + n.z * d.z - tol;
+      const double b = u.x * (W[q].x - P.x) + u.y * (W[q].y - P.y) + u.z * (W[q].z - P.z);
+      if (b > 1e-12) lo = fmax(lo, a / b);
+      else if (b < -1e-12) hi = a > 0.0 ? -1.0 : fmin(hi, a / b);
+      else ok = a <= 0.0;
+    }
+    if (ok && lo <= hi) best = fmin(best, lo);
+  }
+  return best;
+}
+
+// Reach of every bin entry's triangle T, for a particle that leaves T
+// outward (re-emitted or reflected; it starts 1 um above T along T's normal):
+// (r, k) such that a path shorter than r whose direction makes more than k
+// with T's normal (the sine of its elevation) crosses no listed triangle.
+// Every triangle U within rmax of T is listed in a cell that T's box, grown
+// by rmax and one more cell, overlaps.  A U with no vertex more than tol
+// above T's plane cannot be crossed from above it.  A U that rises above
+// the plane either caps r by the distance between the two boxes (a lower
+// bound of the distance between the triangles), or, when its slope bound
+// (rise_slope) is below 1/2, raises k to that bound: a path of elevation
+// above k climbs faster than U rises with the distance from T.  r is lowered
+// by `slack` (the set-off and the rounding of the hit point) and by 0.1 %;
+// (0, 2) where nothing is left.
+__global__ void k_entry_reach(const __grid_constant__ GeomView g, uint32_t entries, float rmax, float tol,
+                              float slack, float2* __restrict__ out) {
+  const float grow = rmax + fmaxf(g.grid.cell.x, fmaxf(g.grid.cell.y, g.grid.cell.z));
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < entries; e += gridDim.x * blockDim.x) {
+    const float4 A = g.tri[kTriStride * (size_t)e], B = g.tri[kTriStride * (size_t)e + 1],
+                 C = g.tri[kTriStride * (size_t)e + 2];
+    const float4 P = g.plane[e];
+    const double3 V[3] = {make_double3(A.x, A.y, A.z), make_double3(B.x, B.y, B.z), make_double3(C.x, C.y, C.z)};
+    // T's unit normal from its vertices in FP64 (the stored plane's orientation)
+    const double3 e1 = make_double3(V[1].x - V[0].x, V[1].y - V[0].y, V[1].z - V[0].z);
+    const double3 e2 = make_double3(V[2].x - V[0].x, V[2].y - V[0].y, V[2].z - V[0].z);
+    double3 n = make_double3(e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x);
+    const double nl = sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+    float2 res = make_float2(0.f, 2.f);
+    if (nl > 0.0) {
+      n = make_double3(n.x / nl, n.y / nl, n.z / nl);
+    }
+    // the normal the wall response uses must agree with the vertices' one
+    if (nl > 0.0 && n.x * P.x + n.y * P.y + n.z * P.z > 0.9999) {
+      // in-plane outer normals of the edges V[c] -> V[c+1]
+      double3 un[3];
+      for (int c = 0; c < 3; c++) {
+        const double3 a = V[c], b = V[(c + 1) % 3];
+        const double3 d = make_double3(b.x - a.x, b.y - a.y, b.z - a.z);
+        double3 u = make_double3(d.y * n.z - d.z * n.y, d.z * n.x - d.x * n.z, d.x * n.y - d.y * n.x);
+        const double l = sqrt(u.x * u.x + u.y * u.y + u.z * u.z);
+        u = make_double3(u.x / l, u.y / l, u.z / l);
+        const double3 o = V[(c + 2) % 3];
+        if (u.x * (o.x - a.x) + u.y * (o.y - a.y) + u.z * (o.z - a.z) > 0.0) u = make_double3(-u.x, -u.y, -u.z);
+        un[c] = u;
+      }
+      const float lo[3] = {fminf(A.x, fminf(B.x, C.x)), fminf(A.y, fminf(B.y, C.y)), fminf(A.z, fminf(B.z, C.z))};
+      const float hi[3] = {fmaxf(A.x, fmaxf(B.x, C.x)), fmaxf(A.y, fmaxf(B.y, C.y)), fmaxf(A.z, fmaxf(B.z, C.z))};
+      const float gmn[3] = {g.grid.gmin.x, g.grid.gmin.y, g.grid.gmin.z};
+      const float cs[3] = {g.grid.cell.x, g.grid.cell.y, g.grid.cell.z};
+      const int dim[3] = {(int)g.grid.dim.x, (int)g.grid.dim.y, (int)g.grid.dim.z};
+      int c0[3], c1[3];
+      for (int k = 0; k < 3; k++) {
+        c0[k] = max(0, (int)floorf((lo[k] - grow - gmn[k]) / cs[k]));
+        c1[k] = min(dim[k] - 1, (int)floorf((hi[k] + grow - gmn[k]) / cs[k]));
+      }
+      double best = rmax, slope = 0.0;
+      for (int z = c0[2]; z <= c1[2]; z++)
+        for (int y = c0[1]; y <= c1[1]; y++)
+          for (int x = c0[0]; x <= c1[0]; x++) {
+            const uint2 se = g.start_end[((uint32_t)z * g.grid.dim.y + (uint32_t)y) * g.grid.dim.x + (uint32_t)x];
+            if (se.x == kNone) continue;
+            for (uint32_t j = se.x; j < se.y; j++) {
+              double3 W[3];
+              for (int k = 0; k < 3; k++) {
+                const float4 q = g.tri[kTriStride * (size_t)j + k];
+                W[k] = make_double3(q.x, q.y, q.z);
+              }
+              double up = -1.0;
+              for (int k = 0; k < 3; k++)
+                up = fmax(up, n.x * (W[k].x - V[0].x) + n.y * (W[k].y - V[0].y) + n.z * (W[k].z - V[0].z));
+              if (up <= tol) continue;
+              const double k_rise = rise_slope(V, un, n, W, tol);
+              if (k_rise < 0.5) {
+                slope = fmax(slope, k_rise);
+                continue;
+              }
+              // no usable slope: the distance between the two boxes
+              double d2 = 0.0;
+              for (int k = 0; k < 3; k++) {
+                const double w0 = axis_of(W[0], k), w1 = axis_of(W[1], k), w2 = axis_of(W[2], k);
+                const double wl = fmin(w0, fmin(w1, w2)), wh = fmax(w0, fmax(w1, w2));
+                const double gap = fmax(0.0, fmax(wl - hi[k], (double)lo[k] - wh));
+                d2 += gap * gap;
+              }
+              best = fmin(best, sqrt(d2));
+            }
+          }
+      const float r = fmaxf(0.f, 0.999f * (float)best - slack);
+      if (r > 0.f) res = make_float2(r, __double2float_ru(slope));
+    }
+    out[e] = res;
+  }
+}
+
 __global__ void k_clearance_at(const __grid_constant__ GeomView g, const float* __restrict__ xyz,
                                uint32_t n, float* __restrict__ out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -891,6 +1026,13 @@ cudaError_t launch_clearance_at(const GeomView& g, const float* xyz, uint32_t n,
                                 cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   k_clearance_at<<<grid_for(n, 256, 8), 256, 0, stream>>>(g, xyz, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_entry_reach(const GeomView& g, uint32_t entries, float rmax, float tol, float slack,
+                               float2* out, cudaStream_t stream) {
+  if (entries == 0) return cudaSuccess;
+  k_entry_reach<<<grid_for(entries, 128, 8), 128, 0, stream>>>(g, entries, rmax, tol, slack, out);
   return cudaGetLastError();
 }
 

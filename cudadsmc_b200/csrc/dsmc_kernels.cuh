@@ -267,6 +267,12 @@ cudaError_t launch_outside_fraction(const GridGeom& grid, const GeomView& geom, 
 cudaError_t launch_fine_clearance(const GeomView& g, const GridGeom& fine, uint32_t fac,
                                   const int* cdist, float cmin, float* out, cudaStream_t stream);
 
+// Per bin entry, (path length, least elevation sine) below and above which
+// a path leaving its triangle outward crosses no listed triangle
+// (k_entry_reach); (0, 2) where none.
+cudaError_t launch_entry_reach(const GeomView& g, uint32_t entries, float rmax, float tol, float slack,
+                               float2* out, cudaStream_t stream);
+
 // out[i] = clearance table entry at point i (xyz interleaved), -1 outside.
 cudaError_t launch_clearance_at(const GeomView& g, const float* xyz, uint32_t n, float* out,
                                 cudaStream_t stream);

@@ -666,7 +666,15 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
       const int r = nearest_leg(G, old_pos, pos, pretested && b == 0, L);
       if (r == kLegFree) break;
       if (r == kLegInside) return false;
+      float2 reach = make_float2(0.f, 2.f);
+      if (G.reach) reach = geo_ld(&G.reach[L.e]);
       wall_response(G, L, old_pos, pos, vel, rng);
+      // a leg within the wall's reach finds no wall (the next pass of the
+      // loop would find none and stop); 1e-5 covers the rounding of the sine
+      NearestLeg next;
+      if (reach.x > 0.f && leg_path(old_pos, pos, next) && next.dist < reach.x &&
+          fmaf(next.d.z, L.P.z, fmaf(next.d.x, L.P.x, __fmul_rn(next.d.y, L.P.y))) > reach.y + 1e-5f)
+        break;
     }
   } else if (p.has_geom) {
     const GeomView& G = p.geom;

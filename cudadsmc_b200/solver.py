@@ -273,6 +273,20 @@ class DSMCSolver:
                     "DownloadState")
         return p, v
 
+    def EntryReach(self):
+        """Per geometry-grid entry (tri_ids order), [entries, 2]: the path
+        length r and the elevation sine k such that a particle leaving the
+        entry's triangle outward along a shorter path, steeper than k,
+        crosses no listed triangle (r = 0: none); empty when the table is
+        off."""
+        ne = ctypes.c_uint64()
+        self._check(lib().dsmc_get_entry_reach(self.h, None, 0, ctypes.byref(ne)), "EntryReach")
+        out = np.zeros((ne.value, 2), np.float32)
+        if ne.value:
+            self._check(lib().dsmc_get_entry_reach(self.h, _ptr(out), ne.value, ctypes.byref(ne)),
+                        "EntryReach")
+        return out
+
     def GeometryGrid(self):
         """The handle's geometry grid (built on the device by SetModel): bbox,
         cell size, dims, per-cell triangle counts, triangle ids in bin order,

@@ -468,6 +468,21 @@ typedef struct dsmc_move_params {
  * The table is built with the mesh (dsmc_set_mesh). */
 int dsmc_clearance_at(dsmc_handle* h, const float* xyz, uint32_t n, float* out, void* stream);
 
+/* Per bin entry of the geometry grid (the order of dsmc_get_geometry_grid's
+ * tri_ids), the reach of the entry's triangle as two floats (r, k): a
+ * particle re-emitted or reflected from the triangle whose remaining path is
+ * shorter than r and whose direction makes more than k with the triangle's
+ * normal (the sine of its elevation) cannot cross a listed triangle, so the
+ * nearest-hit traversal stops without a second walk of the grid.  Triangles
+ * near it that rise above its plane either cap r (by a lower bound of their
+ * distance) or, when their rise is bounded by a slope below 1/2 of the
+ * distance from the triangle, raise k to that slope.  r = 0 where no path
+ * qualifies.  At most cap pairs into out (host memory, 2 floats each);
+ * *n_entries gets the entry count, and 0 when the table is off (a body more
+ * than 2 m from the origin, where the 1 um set-off from the wall nears the
+ * coordinates' rounding). */
+int dsmc_get_entry_reach(dsmc_handle* h, float* out, uint64_t cap, uint64_t* n_entries);
+
 /* IntegrateDev / ProcessCollisionsDev (kernels/dsmc_kernel.cu:1557-1699):
  * free flight, mesh collisions (with the handle's geometry when h != NULL and
  * it has one) and the boundary functor, in place on the six arrays. */
