@@ -473,10 +473,12 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
 
 template <int CAPW, int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_w(const __grid_constant__ StepParams p) {
+  chained_entry();
   order_body<CAPW, WARPS>(p, blockIdx.x, gridDim.x);
 }
 template <int CAPW, int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_order_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
   order_body<CAPW, WARPS>(p, vb, vg);
@@ -550,10 +552,12 @@ __device__ __forceinline__ void ntc_body(const StepParams& p, const uint32_t vb,
 
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_ntc_w(const __grid_constant__ StepParams p) {
+  chained_entry();
   ntc_body<WARPS>(p, blockIdx.x, gridDim.x);
 }
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_ntc_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
   ntc_body<WARPS>(p, vb, vg);
@@ -686,10 +690,12 @@ __device__ __forceinline__ void flight_body(const StepParams& p, const uint32_t 
 
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_w(const __grid_constant__ StepParams p) {
+  chained_entry();
   flight_body<WARPS>(p, blockIdx.x, gridDim.x);
 }
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
   flight_body<WARPS>(p, vb, vg);
@@ -704,6 +710,7 @@ constexpr uint32_t kFlightQ2 = 128;
 
 template <int WARPS, int MINB>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_constant__ StepParams p) {
+  chained_entry();
   __shared__ uint32_t s_q[WARPS][kFlightQ2];
   extern __shared__ uint32_t s_tile[];  // this block's next-step counts per scan tile
   for (uint32_t t = threadIdx.x; t < p.n_scan_tiles; t += blockDim.x) s_tile[t] = 0;
@@ -831,10 +838,12 @@ __device__ __forceinline__ void mesh_body(const StepParams& p, const uint32_t vb
 
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
+  chained_entry();
   mesh_body(p, blockIdx.x, gridDim.x);
 }
 template <int MINB>
 __global__ void __launch_bounds__(256, MINB) k_mesh_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
   mesh_body(p, vb, vg);
@@ -858,9 +867,11 @@ __device__ __forceinline__ void sample_body(const StepParams& p, const uint32_t 
 }
 
 __global__ void __launch_bounds__(256) k_sample_w(const __grid_constant__ StepParams p) {
+  chained_entry();
   sample_body(p, blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(256) k_sample_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
   sample_body(p, vb, vg);
@@ -898,8 +909,7 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  k_order_w<CAPW, WARPS, MINB><<<grid, WARPS * 32, smem, stream>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k_order_w<CAPW, WARPS, MINB>, grid, WARPS * 32, smem, stream, p);
 }
 
 constexpr int kFlightWarps = 8;
@@ -921,9 +931,8 @@ cudaError_t launch_flight_w(const StepParams& p, cudaStream_t stream) {
     ls.per_sm = per_sm;
   }
   // a full wave of warps: the particle count is known only on the device
-  k_flight_w<kFlightWarps, MINB><<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
-                                   p.n_scan_tiles * 4u, stream>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k_flight_w<kFlightWarps, MINB>, (uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
+                        p.n_scan_tiles * 4u, stream, p);
 }
 
 template <int MINB>
@@ -942,9 +951,8 @@ cudaError_t launch_flight_pw(const StepParams& p, cudaStream_t stream) {
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  k_flight_pw<kFlightWarps, MINB><<<(uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
-                                    p.n_scan_tiles * 4u, stream>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k_flight_pw<kFlightWarps, MINB>, (uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
+                        p.n_scan_tiles * 4u, stream, p);
 }
 
 constexpr int kNtcWarps = 8;
@@ -963,8 +971,7 @@ cudaError_t launch_ntc_w(const StepParams& p, cudaStream_t stream) {
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  k_ntc_w<kNtcWarps><<<(uint32_t)(num_sms() * ls.per_sm), kNtcWarps * 32, 0, stream>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k_ntc_w<kNtcWarps>, (uint32_t)(num_sms() * ls.per_sm), kNtcWarps * 32, 0, stream, p);
 }
 
 template <int MINB>
@@ -982,13 +989,11 @@ cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  k_mesh_w<MINB><<<(uint32_t)(num_sms() * ls.per_sm), 256, 0, stream>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k_mesh_w<MINB>, (uint32_t)(num_sms() * ls.per_sm), 256, 0, stream, p);
 }
 
 cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
-  k_sample_w<<<grid_for(p.cells, 256, 8), 256, 0, stream>>>(p);
-  return cudaGetLastError();
+  return launch_chained(k_sample_w, grid_for(p.cells, 256, 8), 256, 0, stream, p);
 }
 
 }  // namespace
@@ -1063,23 +1068,12 @@ cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32
                                 cudaStream_t stream) {
   if (blocks == 0) return cudaSuccess;
   switch (stage) {
-    case 0:
-      k_order_wb<128, 4, 4><<<blocks, 128, collide_smem_bytes<128, 4>(), stream>>>(bv);
-      break;
-    case 1:
-      k_ntc_wb<kNtcWarps><<<blocks, kNtcWarps * 32, 0, stream>>>(bv);
-      break;
-    case 2:
-      k_flight_wb<kFlightWarps, 4><<<blocks, kFlightWarps * 32, flight_smem, stream>>>(bv);
-      break;
-    case 3:
-      k_mesh_wb<2><<<blocks, 256, 0, stream>>>(bv);
-      break;
-    default:
-      k_sample_wb<<<blocks, 256, 0, stream>>>(bv);
-      break;
+    case 0: return launch_chained(k_order_wb<128, 4, 4>, blocks, 128, collide_smem_bytes<128, 4>(), stream, bv);
+    case 1: return launch_chained(k_ntc_wb<kNtcWarps>, blocks, kNtcWarps * 32, 0, stream, bv);
+    case 2: return launch_chained(k_flight_wb<kFlightWarps, 4>, blocks, kFlightWarps * 32, flight_smem, stream, bv);
+    case 3: return launch_chained(k_mesh_wb<2>, blocks, 256, 0, stream, bv);
+    default: return launch_chained(k_sample_wb, blocks, 256, 0, stream, bv);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t launch_cell_w(const StepParams& p, int v, cudaStream_t stream) {

@@ -221,6 +221,18 @@ __device__ __forceinline__ bool intersect_triangle(float3 orig, float3 dir, floa
   return true;
 }
 
+// Programmatic dependent launch.  The step's kernels are launched with
+// programmatic stream serialization (launch_chained): a kernel's CTAs may be
+// dispatched while the kernel before it in the stream drains, and each waits
+// here, before its first access to memory, until that kernel has completed
+// and its writes are visible (griddepcontrol.wait is a no-op for a kernel
+// launched without the attribute).  It then allows the next kernel's launch
+// to begin, which dispatches once every CTA of this one has started.
+__device__ __forceinline__ void chained_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Geometry on the device: the uniform grid over the body, a per-cell flag,
 // per-cell [start,end) into the bin entries, and per bin entry the three
 // vertices with the face normal packed into the .w lanes.
@@ -361,16 +373,23 @@ __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, fl
 #pragma unroll
       for (int k = 0; k < 8; k++)
         P[k] = i0 + k < se.y ? geo_ld(&G.plane[i0 + k]) : make_float4(0.f, 0.f, 0.f, 1.f);
+      // plane pre-test: both ends of the segment on one side -> no crossing;
+      // the others are the candidates, one bit each
+      uint32_t cand = 0u;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
-        const uint32_t i = i0 + k;
-        if (i >= se.y) break;
-        // plane pre-test: both ends of the segment on one side -> no crossing
+        if (i0 + k >= se.y) break;
         const float3 pn = make_float3(P[k].x, P[k].y, P[k].z);
         const float s0 = dot_x(pn, o) - P[k].w;
         const float s1 = fmaf(dist, dot_x(pn, d), s0);
         const float tol = __fmul_rn(1e-7f, fabsf(P[k].w) + 1.f);
-        if ((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol)) continue;
+        if (!((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol))) cand |= 1u << k;
+      }
+      // the candidates' vertices, in triangle order: the j-th round of the
+      // loop loads every lane's j-th candidate at once, whatever its slot
+      while (cand) {
+        const uint32_t i = i0 + (uint32_t)(__ffs(cand) - 1);
+        cand &= cand - 1u;
         const float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
         const float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
         const float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);

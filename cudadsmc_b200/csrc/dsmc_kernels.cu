@@ -160,9 +160,11 @@ __device__ __forceinline__ void scan_body(uint32_t* count, uint32_t* cursor, uin
 __global__ void __launch_bounds__(256) k_scan(uint32_t* count, uint32_t* cursor, uint32_t* start,
                                               uint32_t cells, const uint32_t* tile_sum, Meta* meta,
                                               int bump) {
+  chained_entry();
   scan_body(count, cursor, start, cells, tile_sum, meta, bump, blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(256) k_scan_b(const __grid_constant__ BatchOf<SortArgs> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const SortArgs& a = bv.locate(vb, vg);
   scan_body(a.count, a.cursor, a.start, a.cells, a.tile_sum, a.meta, 1, vb, vg);
@@ -261,11 +263,13 @@ __global__ void __launch_bounds__(256, 4) k_scatter(SoA src, SoA dst, const uint
                                                     uint32_t cells, uint32_t* tile_sum,
                                                     uint32_t n_scan_tiles, Meta* meta,
                                                     uint32_t capacity) {
+  chained_entry();
   scatter_body<STATE>(src, dst, keys, start, cursor, orig, cells, tile_sum, n_scan_tiles, meta, capacity,
                       blockIdx.x, gridDim.x);
 }
 // orig only (the split kernels)
 __global__ void __launch_bounds__(256, 4) k_scatter_b(const __grid_constant__ BatchOf<SortArgs> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const SortArgs& a = bv.locate(vb, vg);
   const SoA none{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -534,9 +538,11 @@ __device__ __forceinline__ void inject_plan_body(const InjectParams& p, uint32_t
 }
 
 __global__ void k_inject_plan(const __grid_constant__ InjectParams p, uint32_t* plan) {
+  chained_entry();
   inject_plan_body(p, plan, blockIdx.x);
 }
 __global__ void k_inject_plan_b(const __grid_constant__ BatchOf<InjectParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const InjectParams& p = bv.locate(vb, vg);
   inject_plan_body(p, p.plan, vb);
@@ -620,9 +626,11 @@ __device__ __forceinline__ void inject_fill_body(const InjectParams& p, const ui
 }
 
 __global__ void k_inject_fill(const __grid_constant__ InjectParams p, const uint32_t* plan) {
+  chained_entry();
   inject_fill_body(p, plan, blockIdx.x, gridDim.x);
 }
 __global__ void k_inject_fill_b(const __grid_constant__ BatchOf<InjectParams> bv) {
+  chained_entry();
   uint32_t vb, vg;
   const InjectParams& p = bv.locate(vb, vg);
   inject_fill_body(p, p.plan, vb, vg);
@@ -662,8 +670,8 @@ cudaError_t launch_index(const GridGeom& g, uint32_t cells, const float* x, cons
 cudaError_t launch_scan(uint32_t* count, uint32_t* cursor, uint32_t* start, uint32_t cells,
                         const uint32_t* tile_sum, uint32_t n_scan_tiles, Meta* meta, int bump_step,
                         cudaStream_t stream) {
-  k_scan<<<n_scan_tiles, 256, 0, stream>>>(count, cursor, start, cells, tile_sum, meta, bump_step);
-  return cudaGetLastError();
+  return launch_chained(k_scan, n_scan_tiles, 256, 0, stream, count, cursor, start, cells, tile_sum, meta,
+                        bump_step);
 }
 
 cudaError_t launch_scatter(bool with_state, const SoA& src, SoA dst, const uint32_t* keys,
@@ -672,13 +680,8 @@ cudaError_t launch_scatter(bool with_state, const SoA& src, SoA dst, const uint3
                            uint32_t n_scan_tiles, Meta* meta, uint32_t capacity,
                            cudaStream_t stream) {
   const uint32_t grid = (uint32_t)num_sms() * 4;
-  if (with_state)
-    k_scatter<true><<<grid, 256, 0, stream>>>(src, dst, keys, start, cursor, orig, cells, tile_sum,
-                                              n_scan_tiles, meta, capacity);
-  else
-    k_scatter<false><<<grid, 256, 0, stream>>>(src, dst, keys, start, cursor, orig, cells,
-                                               tile_sum, n_scan_tiles, meta, capacity);
-  return cudaGetLastError();
+  return launch_chained(with_state ? k_scatter<true> : k_scatter<false>, grid, 256, 0, stream, src, dst, keys,
+                        start, cursor, orig, cells, tile_sum, n_scan_tiles, meta, capacity);
 }
 
 cudaError_t launch_move(const StepParams& p, uint32_t n, uint32_t step, cudaStream_t stream) {
@@ -1058,28 +1061,27 @@ cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream) {
 }
 
 cudaError_t launch_scan_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream) {
-  if (blocks) k_scan_b<<<blocks, 256, 0, stream>>>(bv);
-  return cudaGetLastError();
+  return blocks ? launch_chained(k_scan_b, blocks, 256, 0, stream, bv) : cudaSuccess;
 }
 
 cudaError_t launch_scatter_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream) {
-  if (blocks) k_scatter_b<<<blocks, 256, 0, stream>>>(bv);
-  return cudaGetLastError();
+  return blocks ? launch_chained(k_scatter_b, blocks, 256, 0, stream, bv) : cudaSuccess;
 }
 
 cudaError_t launch_inject_b(const BatchOf<InjectParams>& plan, uint32_t plan_blocks,
                             const BatchOf<InjectParams>& fill, uint32_t fill_blocks, size_t fill_smem,
                             cudaStream_t stream) {
-  if (plan_blocks) k_inject_plan_b<<<plan_blocks, 32, 0, stream>>>(plan);
-  if (fill_blocks) k_inject_fill_b<<<fill_blocks, 256, fill_smem, stream>>>(fill);
-  return cudaGetLastError();
+  cudaError_t e = cudaSuccess;
+  if (plan_blocks) e = launch_chained(k_inject_plan_b, plan_blocks, 32, 0, stream, plan);
+  if (!e && fill_blocks) e = launch_chained(k_inject_fill_b, fill_blocks, 256, fill_smem, stream, fill);
+  return e;
 }
 
 cudaError_t launch_inject(const InjectParams& p, cudaStream_t stream) {
-  k_inject_plan<<<1, 32, 0, stream>>>(p, p.plan);
+  cudaError_t e = launch_chained(k_inject_plan, 1, 32, 0, stream, p, p.plan);
   const uint32_t grid = (uint32_t)num_sms();
-  k_inject_fill<<<grid, 256, p.n_scan_tiles * 4, stream>>>(p, p.plan);
-  return cudaGetLastError();
+  if (!e) e = launch_chained(k_inject_fill, grid, 256, p.n_scan_tiles * 4, stream, p, p.plan);
+  return e;
 }
 
 }  // namespace dsmcb

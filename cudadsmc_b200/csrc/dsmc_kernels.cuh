@@ -20,6 +20,26 @@
 
 namespace dsmcb {
 
+// Launches `kernel` with programmatic stream serialization: its CTAs may be
+// dispatched while the previous kernel in the stream drains; the kernel must
+// call chained_entry() before touching memory.  Kernel nodes captured into
+// a graph keep the programmatic edge.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), uint32_t grid, uint32_t block, size_t smem,
+                                  cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 constexpr int kMaxCellsPerTile = 256;
 constexpr int kScanTile = 2048;       // cells per scan block (256 threads x 8)
 constexpr int kScanShift = 11;

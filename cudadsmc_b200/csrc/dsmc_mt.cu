@@ -90,6 +90,7 @@ __global__ void k_mt_maximums(const uint4* cfg, uint32_t* state, float2* maxrem,
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_ntc_mt(const __grid_constant__ StepParams p,
                                                        uint32_t* mt_state, const uint4* mt_cfg) {
+  chained_entry();
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t col = 0;
   double sum_g = 0.0;
@@ -154,9 +155,8 @@ cudaError_t launch_mt_maximums(const uint4* cfg, uint32_t* state, float2* maxrem
 
 cudaError_t launch_ntc_mt(const StepParams& p, uint32_t* mt_state, const uint4* mt_cfg,
                           cudaStream_t stream) {
-  k_ntc_mt<kNtcMtWarps><<<(uint32_t)num_sms() * 8u, kNtcMtWarps * 32, 0, stream>>>(p, mt_state,
-                                                                                 mt_cfg);
-  return cudaGetLastError();
+  return launch_chained(k_ntc_mt<kNtcMtWarps>, (uint32_t)num_sms() * 8u, kNtcMtWarps * 32, 0, stream, p, mt_state,
+                        mt_cfg);
 }
 
 }  // namespace dsmcb
