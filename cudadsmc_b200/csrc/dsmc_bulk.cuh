@@ -61,6 +61,14 @@ __device__ __forceinline__ void cp_async4(void* smem_dst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;" ::: "memory");
 }
+// Closes this thread's group of asynchronous copies issued since the last
+// commit; cp_async_wait_prior() waits for every group but the newest.
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_prior() {
+  asm volatile("cp.async.wait_group 1;" ::: "memory");
+}
 
 // Waits for an mbarrier phase for at most about a second.
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* m, uint32_t parity) {

@@ -1943,7 +1943,7 @@ int batch_capture(dsmc_batch* b, const std::vector<float>& dt) {
     np[i] = (double)m.n_alive + (double)m.n_pending + 1.0;
     nc[i] = (double)h->cells;
     // every member runs the split kernels with the order kernel's
-    // (128 particles, 4 warps, 4 CTAs) shape and tiles of 32 cells, whatever
+    // (128 particles, 4 warps, 5 CTAs) shape and tiles of 32 cells, whatever
     // shape it uses stepped alone
     P[i] = step_params(h, dt[i], true);
     P[i].cell_variant = 5;

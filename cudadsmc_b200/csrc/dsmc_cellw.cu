@@ -316,6 +316,11 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
   uint32_t lcnt = 0;   // entries in S.lbuf
   WChunk C;
   C.valid = 0;
+  // the previous chunk, gathered into its buffer's state rows by copies that
+  // may still be in flight, written out once the next chunk's gathers are
+  // issued (P.valid == 0: none)
+  WChunk P;
+  P.valid = 0;
   // writes chunk (base, n) from state buffer b to the mid arrays
   auto write_chunk = [&](uint32_t b, uint32_t base, uint32_t n) {
     const uint32_t o = base & 3u;
@@ -330,6 +335,17 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
       p.mid.x[g] = X[q]; p.mid.y[g] = Y[q]; p.mid.z[g] = Z[q];
       p.mid.u[g] = U[q]; p.mid.v[g] = V[q]; p.mid.w[g] = W[q];
     }
+  };
+  // the pending chunk, once every gather but the newest group has landed
+  // (all of them with `all`)
+  auto write_pending = [&](bool all) {
+    if (!P.valid) return;
+    if (all) cp_async_wait_all();
+    else cp_async_wait_prior();
+    __syncwarp();
+    write_chunk(P.buf, P.base, P.n);
+    __syncwarp();
+    P.valid = 0;
   };
   // (sigma g)max and remainder of a chunk's cells, loaded one chunk ahead
   float2 mr_c = make_float2(0.f, 0.f);
@@ -376,12 +392,16 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
         // let them land (again bounded) before the shared memory goes away
         mbar_wait_bounded(&S.mbar[C.buf], par);
         if (n_copy) mbar_wait_bounded(&S.mbar[N.buf], (phase >> N.buf) & 1u);
+        cp_async_wait_all();
+        P.valid = 0;
         break;
       }
     }
     __syncwarp();
 
     if (C.giant) {
+      // the chunk after it reuses the pending chunk's buffer
+      write_pending(true);
       giant_order_warp(p, C.base, C.base + C.n);
       if (do_collide) {
         // the giant cell's pair count, from lane C.cur's (sigma g)max
@@ -397,6 +417,8 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
                      make_uint4(gc, C.base, C.n, M));
       }
     } else if (C.n > 0) {
+      // a pending chunk in this chunk's buffer (an empty chunk came between)
+      if (P.valid && P.buf == C.buf) write_pending(true);
       const uint32_t off = C.base & 3u;
       const uint32_t* OR = reinterpret_cast<const uint32_t*>(S.part[C.buf][Smem::kOrig] + off);
       // element j of the chunk sits at ORA[j + off]
@@ -451,10 +473,11 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
         buffer_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light, M > 0 && !heavy, e);
         list_cells(p.ntc_heavy, &p.meta->n_heavy, heavy, e);
       }
-      cp_async_wait_all();
-      __syncwarp();
-      // C: the chunk, now in sorted order, to the mid arrays
-      write_chunk(C.buf, base, n);
+      cp_async_commit();
+      // C: the previous chunk, in sorted order, to the mid arrays while this
+      // one's gathers are in flight; this one waits for the next
+      write_pending(false);
+      P = C;
     }
     __syncwarp();
     if (n_in_b) {
@@ -466,6 +489,7 @@ __device__ __forceinline__ void order_body(const StepParams& p, const uint32_t v
     C = N;
     mr_c = mr_n;
   }
+  write_pending(true);
   if (do_collide) flush_cells(S.lbuf, lcnt, p.ntc_light, &p.meta->n_light);
   __shared__ unsigned long long s_red[WARPS];
   if (p.meta) block_add(&p.meta->selections, (unsigned long long)sel, s_red);
@@ -1001,7 +1025,7 @@ cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
 // Split variants (cell_kernel_variants() numbers them after the fused
 // CTA-wide ones): (particles per warp chunk, warps per CTA, CTAs per SM the
 // registers are capped for) of the order kernel and the flight kernel's form
-// (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 4;
+// (8 warps per CTA): 0 (256, 4, 4; one particle per lane), 1 (128, 4, 5;
 // one), 2 (128, 8, 3; pairs), 3 (128, 4, 6; pairs).
 int cell_kernel_w_variants() { return 4; }
 
@@ -1019,7 +1043,7 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
         case 0: return launch_order_w<256, 4, 4>(p, stream);
         case 2: return launch_order_w<128, 8, 3>(p, stream);
         case 3: return launch_order_w<128, 4, 6>(p, stream);
-        default: return launch_order_w<128, 4, 4>(p, stream);
+        default: return launch_order_w<128, 4, 5>(p, stream);
       }
     case 1:
       if (p.flags & kDoCollide) return launch_ntc_w(p, stream);
@@ -1042,14 +1066,14 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
 }
 
 // Batched forms of the split kernels for ensembles: the order kernel in the
-// (128 particles, 4 warps, 4 CTAs per SM) shape, single-particle flights.
+// (128 particles, 4 warps, 5 CTAs per SM) shape, single-particle flights.
 cudaError_t cell_batch_waves(uint32_t wave[5], size_t flight_smem) {
   const size_t osmem = collide_smem_bytes<128, 4>();
-  cudaError_t e = cudaFuncSetAttribute(k_order_wb<128, 4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_order_wb<128, 4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)osmem);
   if (e != cudaSuccess) return e;
   int per[5] = {0, 0, 0, 0, 0};
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_order_wb<128, 4, 4>, 128, osmem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_order_wb<128, 4, 5>, 128, osmem);
   if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_ntc_wb<kNtcWarps>, kNtcWarps * 32, 0);
   if (!e)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_flight_wb<kFlightWarps, 4>, kFlightWarps * 32,
@@ -1068,7 +1092,7 @@ cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32
                                 cudaStream_t stream) {
   if (blocks == 0) return cudaSuccess;
   switch (stage) {
-    case 0: return launch_chained(k_order_wb<128, 4, 4>, blocks, 128, collide_smem_bytes<128, 4>(), stream, bv);
+    case 0: return launch_chained(k_order_wb<128, 4, 5>, blocks, 128, collide_smem_bytes<128, 4>(), stream, bv);
     case 1: return launch_chained(k_ntc_wb<kNtcWarps>, blocks, kNtcWarps * 32, 0, stream, bv);
     case 2: return launch_chained(k_flight_wb<kFlightWarps, 4>, blocks, kFlightWarps * 32, flight_smem, stream, bv);
     case 3: return launch_chained(k_mesh_wb<2>, blocks, 256, 0, stream, bv);

@@ -205,7 +205,7 @@ cudaError_t launch_cell(const StepParams& p, cudaStream_t stream);
 // Variants of the cell kernel.  CTA-wide: 0 (512 threads, 2048 particles per
 // chunk, 1 CTA/SM), 1 (256, 1024, 2), 2 (128, 512, 4), 3 (64, 256, up to 8).
 // Warp-autonomous (particles per warp chunk, warps per CTA, CTAs per SM):
-// 4 (256, 4, 4), 5 (128, 4, 4), 6 (128, 8, 3), 7 (128, 4, 6).
+// 4 (256, 4, 4), 5 (128, 4, 5), 6 (128, 8, 3), 7 (128, 4, 6).
 int cell_kernel_variants();
 int cell_kernel_chunk_capacity(int variant);
 // Variants at or above 4 use the warp-autonomous kernel, whose tiles are
