@@ -2021,10 +2021,13 @@ int batch_capture(dsmc_batch* b, const std::vector<float>& dt) {
   e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (!e) e = dsmcb::launch_scan_b(sv(0), total[0], b->stream);
   if (!e) e = dsmcb::launch_scatter_b(sv(1), total[1], b->stream);
-  if (!e) e = dsmcb::launch_cell_stage_b(0, pv(2), total[2], flight_smem, b->stream);
+  bool coop_mesh = true;
+  for (size_t i = 0; i < n; i++)
+    if (P[i].has_geom && !P[i].geom.nearest) coop_mesh = false;
+  if (!e) e = dsmcb::launch_cell_stage_b(0, pv(2), total[2], flight_smem, coop_mesh, b->stream);
   if (!e && ni) e = dsmcb::launch_inject_b(iv(7), total[7], iv(8), total[8], flight_smem, b->stream);
   for (int st = 1; st < 5 && !e; st++)
-    e = dsmcb::launch_cell_stage_b(st, pv(2 + st), total[2 + st], flight_smem, b->stream);
+    e = dsmcb::launch_cell_stage_b(st, pv(2 + st), total[2 + st], flight_smem, coop_mesh, b->stream);
   cudaError_t e2 = cudaStreamEndCapture(b->stream, &b->graph);
   if (e || e2) {
     batch_drop_graph(b);

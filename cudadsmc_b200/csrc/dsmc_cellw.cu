@@ -833,13 +833,191 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_flight_pw(const __grid_con
 
 // The listed flights, one particle per thread over the whole grid (the list's
 // order does not matter: each particle's flight, key and count are its own).
-// The flight with the body is inlined, at 2 CTAs per SM for its registers:
-// the list is a partial wave whose time is one traversal's chain of loads,
-// and a call's spills lengthened it (47 -> 35 us for 61k flights).
+//
+// With nearest wall crossings the first leg of the warp's 32 flights is
+// walked together: each lane lists the grid cells its path visits (the same
+// walk as nearest_wall_hit), the warp then tests the planes of all those
+// cells' triangles 32 at a time whatever flight and cell they belong to, the
+// vertices of the triangles that pass in rounds of 32, and keeps per flight
+// and cell the nearest crossing (the least (t, entry)).  Each lane then
+// applies nearest_wall_hit's rule to its own cells in order - the running
+// nearest crossing, the walk stopped at the first cell whose exit lies
+// beyond it - so the answer is the one the lane alone would find, while the
+// warp's memory rounds follow the total work rather than the slowest lane's
+// cells times the most planes of a cell.  Paths over more than kCoopCells
+// cells walk alone.  The rest of each flight (re-emission, later legs,
+// boundaries) follows per lane.
+constexpr int kCoopCells = 6;
+constexpr int kCoopUnroll = 4;  // plane loads per lane per round
+constexpr int kMeshWarps = 8;
+
+struct MeshCoop {
+  float ox[32], oy[32], oz[32], dx[32], dy[32], dz[32], dist[32];
+  uint32_t cstart[32][kCoopCells];      // first entry of each visited cell
+  uint32_t cpre[32][kCoopCells + 1];    // the lane's entries before cell j
+  float texit[32][kCoopCells];
+  uint32_t lpre[33];                    // the warp's entries before lane L
+  unsigned long long best[32][kCoopCells];  // nearest (t bits, entry) per lane and cell
+  uint2 cand[64];                       // candidate (entry, lane | cell << 8)
+};
+
+// The candidates cand[0, c) (c <= 32): the crossing of each with its lane's
+// segment, kept if nearer than that cell's best.
+__device__ __forceinline__ void coop_crossings(const GeomView& G, MeshCoop& S, uint32_t c) {
+  const uint32_t lane = lane_id();
+  if (lane < c) {
+    const uint2 q = S.cand[lane];
+    const uint32_t L = q.y & 0xffu, j = q.y >> 8;
+    const float3 o = make_float3(S.ox[L], S.oy[L], S.oz[L]);
+    const float3 d = make_float3(S.dx[L], S.dy[L], S.dz[L]);
+    float t;
+    if (entry_crossing(G, q.x, o, d, S.dist[L], &t)) {
+      // +0 for -0: the key's order is the order of t, then of the entry
+      const float tp = t + 0.f;
+      atomicMin(&S.best[L][j], ((unsigned long long)__float_as_uint(tp) << 32) | q.x);
+    }
+  }
+  __syncwarp();
+}
+
+// The first leg's nearest crossing for every lane of the warp (all lanes
+// call it; walk = the lane has a leg).  Returns the lane's kLeg* code with
+// L's t, e and P set; -1 when the lane's path is too long for the joint walk.
+__device__ __forceinline__ int coop_first_leg(const GeomView& G, MeshCoop& S, bool walk, float3 o,
+                                              NearestLeg& L) {
+  const uint32_t lane = lane_id();
+  DdaWalk w;
+  if (walk) walk = dda_begin(G.grid, o, L.d, L.dist, w);
+  int nc = 0;
+  bool alone = false;
+  if (walk) {
+    const int max_iter = dda_max_iter(G.grid);
+    for (int it = 0; it < max_iter; it++) {
+      DdaNext nx;
+      const bool more = dda_peek(w, nx);
+      if (nc == kCoopCells) {
+        alone = true;
+        break;
+      }
+      S.cstart[lane][nc] = dda_cell(G.grid, w.X.i, w.Y.i, w.Z.i);
+      S.texit[lane][nc] = nx.texit;
+      nc++;
+      if (!more) break;
+      dda_take(w, nx);
+    }
+  }
+  if (alone) nc = 0;
+  S.ox[lane] = o.x; S.oy[lane] = o.y; S.oz[lane] = o.z;
+  S.dx[lane] = L.d.x; S.dy[lane] = L.d.y; S.dz[lane] = L.d.z;
+  S.dist[lane] = L.dist;
+  // the visited cells' entry ranges, loaded together
+  uint2 se[kCoopCells];
+#pragma unroll
+  for (int j = 0; j < kCoopCells; j++)
+    se[j] = j < nc ? geo_ld(&G.start_end[S.cstart[lane][j]]) : make_uint2(0u, 0u);
+  uint32_t tot = 0;
+#pragma unroll
+  for (int j = 0; j < kCoopCells; j++) {
+    const uint32_t cnt = (j < nc && se[j].x != kNone) ? se[j].y - se[j].x : 0u;
+    S.cstart[lane][j] = se[j].x;
+    S.cpre[lane][j] = tot;
+    S.best[lane][j] = ~0ull;
+    tot += cnt;
+  }
+  S.cpre[lane][kCoopCells] = tot;
+  // the warp's exclusive prefix over lanes
+  uint32_t incl = tot;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t v = __shfl_up_sync(kFull, incl, d);
+    if ((int)lane >= d) incl += v;
+  }
+  S.lpre[lane] = incl - tot;
+  if (lane == 31) S.lpre[32] = incl;
+  __syncwarp();
+  const uint32_t total = S.lpre[32];
+  // the planes of all listed entries, kCoopUnroll per lane per round
+  uint32_t nq = 0;
+  for (uint32_t base = 0; base < total; base += 32u * kCoopUnroll) {
+    float4 P[kCoopUnroll];
+    uint32_t ent[kCoopUnroll], own[kCoopUnroll];
+#pragma unroll
+    for (int u = 0; u < kCoopUnroll; u++) {
+      const uint32_t k = base + 32u * u + lane;
+      ent[u] = kNone;
+      own[u] = 0;
+      P[u] = make_float4(0.f, 0.f, 0.f, 1.f);
+      if (k < total) {
+        // the lane that owns item k: the last with lpre <= k
+        uint32_t lo = 0, hi = 32;
+        while (hi - lo > 1) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (S.lpre[mid] <= k) lo = mid; else hi = mid;
+        }
+        const uint32_t r = k - S.lpre[lo];
+        uint32_t j = 0;
+        while (j + 1 < kCoopCells && S.cpre[lo][j + 1] <= r) j++;
+        ent[u] = S.cstart[lo][j] + (r - S.cpre[lo][j]);
+        own[u] = lo | (j << 8);
+        P[u] = geo_ld(&G.plane[ent[u]]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kCoopUnroll; u++) {
+      bool c = false;
+      if (ent[u] != kNone) {
+        const uint32_t Lw = own[u] & 0xffu;
+        c = plane_may_cross(P[u], make_float3(S.ox[Lw], S.oy[Lw], S.oz[Lw]),
+                            make_float3(S.dx[Lw], S.dy[Lw], S.dz[Lw]), S.dist[Lw]);
+      }
+      const unsigned m = __ballot_sync(kFull, c);
+      if (c) S.cand[nq + __popc(m & ((1u << lane) - 1u))] = make_uint2(ent[u], own[u]);
+      nq += __popc(m);
+      __syncwarp();
+      if (nq >= 32) {
+        coop_crossings(G, S, 32);
+        nq -= 32;
+        if (lane < nq) S.cand[lane] = S.cand[32 + lane];
+        __syncwarp();
+      }
+    }
+  }
+  if (nq) coop_crossings(G, S, nq);
+  // nearest_wall_hit's rule over the lane's own cells, in walk order
+  float best = 3.0e38f;
+  uint32_t best_i = kNone;
+  for (int j = 0; j < nc; j++) {
+    const unsigned long long b = S.best[lane][j];
+    if (b != ~0ull) {
+      const float t = __uint_as_float((uint32_t)(b >> 32));
+      if (t < best) {
+        best = t;
+        best_i = (uint32_t)b;
+      }
+    }
+    if (best <= S.texit[lane][j]) break;
+  }
+  __syncwarp();
+  if (alone) return -1;
+  if (!walk || best_i == kNone) return kLegFree;
+  L.t = best;
+  L.e = best_i;
+  L.P = geo_ld(&G.plane[best_i]);
+  if (fmaf(L.d.z, L.P.z, fmaf(L.d.x, L.P.x, __fmul_rn(L.d.y, L.P.y))) > 0.f) return kLegInside;
+  return kLegWall;
+}
+
+// COOP: the form with the joint first leg, for nearest wall crossings (the
+// launch has kMeshWarps warps per CTA); the other flies each listed flight
+// alone (first-hit mode).
+template <bool COOP>
 __device__ __forceinline__ void mesh_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
   const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const uint32_t n = p.meta->n_defer;
   uint32_t removed = 0;
+  __shared__ MeshCoop s_coop[COOP ? kMeshWarps : 1];
+  MeshCoop& S = s_coop[COOP ? (threadIdx.x >> 5) % kMeshWarps : 0];
+  const bool coop = COOP && p.has_geom && p.geom.nearest;
   for (uint32_t base = vb * blockDim.x; base < n; base += vg * blockDim.x) {
     const uint32_t i = base + threadIdx.x;
     const bool go = i < n;
@@ -850,6 +1028,28 @@ __device__ __forceinline__ void mesh_body(const StepParams& p, const uint32_t vb
       g = p.defer_list[i];
       pos = make_float3(p.mid.x[g], p.mid.y[g], p.mid.z[g]);
       vel = make_float3(p.mid.u[g], p.mid.v[g], p.mid.w[g]);
+    }
+    if (coop) {
+      // move_particle_body's nearest branch, the first leg walked jointly
+      const GeomView& G = p.geom;
+      float3 old_pos = pos;
+      pos.x = fmaf(vel.x, p.dt, old_pos.x);
+      pos.y = fmaf(vel.y, p.dt, old_pos.y);
+      pos.z = fmaf(vel.z, p.dt, old_pos.z);
+      NearestLeg L0;
+      const bool leg = go && leg_path(old_pos, pos, L0);
+      if (!leg) L0.d = make_float3(0.f, 0.f, 0.f), L0.dist = 0.f;
+      const int r0 = coop_first_leg(G, S, leg, old_pos, L0);
+      if (go) {
+        PhiloxStream rng;
+        rng.init(p.seed, g, step, kPurposeWall);
+        // listed because the path may reach the body: the first clearance
+        // test is already done
+        // (later legs, and first legs too long for the joint walk, walk
+        // alone through a call)
+        live = nearest_legs<false>(G, old_pos, pos, vel, rng, true, r0, L0) && apply_bc(p, pos, vel, rng);
+      }
+    } else if (!COOP && go) {
       // listed because the path may reach the body: the first clearance test
       // is already done
       live = move_particle_body(p, pos, vel, g, step, true);
@@ -860,28 +1060,33 @@ __device__ __forceinline__ void mesh_body(const StepParams& p, const uint32_t vb
   if (p.meta) block_add(&p.meta->removed, removed, s_rm);
 }
 
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
+template <int MINB, bool COOP>
+__global__ void __launch_bounds__(32 * kMeshWarps, MINB) k_mesh_w(const __grid_constant__ StepParams p) {
   chained_entry();
-  mesh_body(p, blockIdx.x, gridDim.x);
+  mesh_body<COOP>(p, blockIdx.x, gridDim.x);
 }
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_mesh_wb(const __grid_constant__ BatchOf<StepParams> bv) {
+template <int MINB, bool COOP>
+__global__ void __launch_bounds__(32 * kMeshWarps, MINB) k_mesh_wb(const __grid_constant__ BatchOf<StepParams> bv) {
   chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
-  mesh_body(p, vb, vg);
+  mesh_body<COOP>(p, vb, vg);
 }
 
 // FP64 sampling after the flights, one cell per thread (the reference's
 // SampleCellStatisticsDev order: each cell's particles in sorted order, with
 // their velocities after the move); returns at once on other steps.
+// The step counter was bumped by the step's scan kernel, which completed
+// before the kernel that this one follows began (each kernel of the step
+// waits for its predecessor), so the counter is read before the wait: on a
+// step without sampling the kernel ends without waiting for the mesh kernel.
 __device__ __forceinline__ void sample_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
-  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
+  const uint32_t step = p.step_override ? p.step_override : __ldcg(&p.meta->step);
   const bool do_sample =
       (p.flags & kDoSample) &&
       ((p.flags & kSampleForce) || (p.sample_every > 0 && step % (uint32_t)p.sample_every == 0));
   if (!do_sample) return;
+  chained_entry();
   for (uint32_t c = vb * blockDim.x + threadIdx.x; c < p.cells; c += vg * blockDim.x) {
     const uint32_t s = __ldg(&p.start[c]), e = __ldg(&p.start[c + 1]);
     GlobalVel a{p.out.u, p.out.v, p.out.w, s};
@@ -891,11 +1096,9 @@ __device__ __forceinline__ void sample_body(const StepParams& p, const uint32_t 
 }
 
 __global__ void __launch_bounds__(256) k_sample_w(const __grid_constant__ StepParams p) {
-  chained_entry();
   sample_body(p, blockIdx.x, gridDim.x);
 }
 __global__ void __launch_bounds__(256) k_sample_wb(const __grid_constant__ BatchOf<StepParams> bv) {
-  chained_entry();
   uint32_t vb, vg;
   const StepParams& p = bv.locate(vb, vg);
   sample_body(p, vb, vg);
@@ -998,7 +1201,7 @@ cudaError_t launch_ntc_w(const StepParams& p, cudaStream_t stream) {
   return launch_chained(k_ntc_w<kNtcWarps>, (uint32_t)(num_sms() * ls.per_sm), kNtcWarps * 32, 0, stream, p);
 }
 
-template <int MINB>
+template <int MINB, bool COOP>
 cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
   static LaunchShapeW cache[8];
   int dev = 0;
@@ -1007,13 +1210,13 @@ cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
   LaunchShapeW& ls = cache[dev & 7];
   if (ls.device != dev) {
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mesh_w<MINB>, 256, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mesh_w<MINB, COOP>, 32 * kMeshWarps, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  return launch_chained(k_mesh_w<MINB>, (uint32_t)(num_sms() * ls.per_sm), 256, 0, stream, p);
+  return launch_chained(k_mesh_w<MINB, COOP>, (uint32_t)(num_sms() * ls.per_sm), 32 * kMeshWarps, 0, stream, p);
 }
 
 cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
@@ -1057,7 +1260,8 @@ cudaError_t launch_split_stage(const StepParams& p, int v, int stage, cudaStream
       }
     case 3:
       // flights that may reach the body (listed only with a body and the move)
-      if (p.has_geom && (p.flags & kDoMove)) return launch_mesh_w<2>(p, stream);
+      if (p.has_geom && (p.flags & kDoMove))
+        return p.geom.nearest ? launch_mesh_w<2, true>(p, stream) : launch_mesh_w<2, false>(p, stream);
       return cudaSuccess;
     default:
       if (p.flags & kDoSample) return launch_sample_w(p, stream);
@@ -1078,7 +1282,7 @@ cudaError_t cell_batch_waves(uint32_t wave[5], size_t flight_smem) {
   if (!e)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_flight_wb<kFlightWarps, 4>, kFlightWarps * 32,
                                                       flight_smem);
-  if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[3], k_mesh_wb<2>, 256, 0);
+  if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[3], k_mesh_wb<2, true>, 32 * kMeshWarps, 0);
   per[4] = 8;
   if (e != cudaSuccess) return e;
   for (int k = 0; k < 5; k++) {
@@ -1089,13 +1293,15 @@ cudaError_t cell_batch_waves(uint32_t wave[5], size_t flight_smem) {
 }
 
 cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32_t blocks, size_t flight_smem,
-                                cudaStream_t stream) {
+                                bool coop_mesh, cudaStream_t stream) {
   if (blocks == 0) return cudaSuccess;
   switch (stage) {
     case 0: return launch_chained(k_order_wb<128, 4, 5>, blocks, 128, collide_smem_bytes<128, 4>(), stream, bv);
     case 1: return launch_chained(k_ntc_wb<kNtcWarps>, blocks, kNtcWarps * 32, 0, stream, bv);
     case 2: return launch_chained(k_flight_wb<kFlightWarps, 4>, blocks, kFlightWarps * 32, flight_smem, stream, bv);
-    case 3: return launch_chained(k_mesh_wb<2>, blocks, 256, 0, stream, bv);
+    case 3:
+      return coop_mesh ? launch_chained(k_mesh_wb<2, true>, blocks, 32 * kMeshWarps, 0, stream, bv)
+                       : launch_chained(k_mesh_wb<2, false>, blocks, 32 * kMeshWarps, 0, stream, bv);
     default: return launch_chained(k_sample_wb, blocks, 256, 0, stream, bv);
   }
 }

@@ -339,73 +339,120 @@ __device__ __forceinline__ int dda_next_axis(const DdaAxis& x, const DdaAxis& y,
   return (x.tmax <= y.tmax && x.tmax <= z.tmax) ? 0 : (y.tmax <= z.tmax ? 1 : 2);
 }
 
+// The walk over the grid's cells along o + s d, s in [t0, t1] (the segment
+// clipped to the grid's box): one axis state per dimension.
+struct DdaWalk {
+  DdaAxis X, Y, Z;
+  float t1;
+};
+
+// Sets the walk up for the segment of length dist; false if it misses the grid.
+__device__ __forceinline__ bool dda_begin(const GridGeom& g, float3 o, float3 d, float dist, DdaWalk& w) {
+  float t0 = 0.f;
+  w.t1 = dist;
+  if (!dda_axis_init(o.x, d.x, g.gmin.x, g.gmax.x, g.cell.x, (int)g.dim.x, t0, w.t1, w.X)) return false;
+  if (!dda_axis_init(o.y, d.y, g.gmin.y, g.gmax.y, g.cell.y, (int)g.dim.y, t0, w.t1, w.Y)) return false;
+  if (!dda_axis_init(o.z, d.z, g.gmin.z, g.gmax.z, g.cell.z, (int)g.dim.z, t0, w.t1, w.Z)) return false;
+  if (t0 > w.t1) return false;
+  dda_axis_start(o.x, d.x, g.gmin.x, g.cell.x, t0, w.X);
+  dda_axis_start(o.y, d.y, g.gmin.y, g.cell.y, t0, w.Y);
+  dda_axis_start(o.z, d.z, g.gmin.z, g.cell.z, t0, w.Z);
+  return true;
+}
+
+__device__ __forceinline__ uint32_t dda_cell(const GridGeom& g, int ix, int iy, int iz) {
+  return ((uint32_t)iz * g.dim.y + (uint32_t)iy) * g.dim.x + (uint32_t)ix;
+}
+
+// The walk's next step: the current cell's exit distance, the axis crossed
+// and the next cell; true if the walk goes on to it (still inside the path
+// and the grid).
+struct DdaNext {
+  float texit;
+  int ax, nx, ny, nz;
+};
+__device__ __forceinline__ bool dda_peek(const DdaWalk& w, DdaNext& n) {
+  n.texit = fminf(w.X.tmax, fminf(w.Y.tmax, w.Z.tmax));
+  n.ax = dda_next_axis(w.X, w.Y, w.Z);
+  n.nx = w.X.i;
+  n.ny = w.Y.i;
+  n.nz = w.Z.i;
+  if (n.ax == 0) n.nx += w.X.step; else if (n.ax == 1) n.ny += w.Y.step; else n.nz += w.Z.step;
+  return n.texit <= w.t1 && n.nx >= 0 && n.nx < w.X.dim && n.ny >= 0 && n.ny < w.Y.dim && n.nz >= 0 &&
+         n.nz < w.Z.dim;
+}
+__device__ __forceinline__ void dda_take(DdaWalk& w, const DdaNext& n) {
+  if (n.ax == 0) { w.X.i = n.nx; w.X.tmax += w.X.tdel; }
+  else if (n.ax == 1) { w.Y.i = n.ny; w.Y.tmax += w.Y.tdel; }
+  else { w.Z.i = n.nz; w.Z.tmax += w.Z.tdel; }
+}
+
+// The walk's iteration limit for a grid.
+__device__ __forceinline__ int dda_max_iter(const GridGeom& g) { return (int)(g.dim.x + g.dim.y + g.dim.z) + 3; }
+
+// Plane pre-test of a triangle for the segment o + s d, s in [0, dist]: false
+// when both ends lie on one side of its plane (beyond a rounding margin).
+__device__ __forceinline__ bool plane_may_cross(float4 P, float3 o, float3 d, float dist) {
+  const float3 pn = make_float3(P.x, P.y, P.z);
+  const float s0 = dot_x(pn, o) - P.w;
+  const float s1 = fmaf(dist, dot_x(pn, d), s0);
+  const float tol = __fmul_rn(1e-7f, fabsf(P.w) + 1.f);
+  return !((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol));
+}
+
+// Whether the segment crosses bin entry i's triangle, at *t in [0, dist].
+__device__ __forceinline__ bool entry_crossing(const GeomView& G, uint32_t i, float3 o, float3 d, float dist,
+                                               float* t) {
+  const float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
+  const float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
+  const float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
+  return intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
+                                make_float3(C.x, C.y, C.z), t) &&
+         *t >= 0.f && *t <= dist;
+}
+
 __device__ __forceinline__ bool nearest_wall_hit(const GeomView& G, float3 o, float3 d, float dist,
                                                  float* t_out, uint32_t* entry_out) {
-  const GridGeom& g = G.grid;
-  float t0 = 0.f, t1 = dist;
-  DdaAxis X, Y, Z;
-  if (!dda_axis_init(o.x, d.x, g.gmin.x, g.gmax.x, g.cell.x, (int)g.dim.x, t0, t1, X)) return false;
-  if (!dda_axis_init(o.y, d.y, g.gmin.y, g.gmax.y, g.cell.y, (int)g.dim.y, t0, t1, Y)) return false;
-  if (!dda_axis_init(o.z, d.z, g.gmin.z, g.gmax.z, g.cell.z, (int)g.dim.z, t0, t1, Z)) return false;
-  if (t0 > t1) return false;
-  dda_axis_start(o.x, d.x, g.gmin.x, g.cell.x, t0, X);
-  dda_axis_start(o.y, d.y, g.gmin.y, g.cell.y, t0, Y);
-  dda_axis_start(o.z, d.z, g.gmin.z, g.cell.z, t0, Z);
-  auto cell_of = [&](int ix, int iy, int iz) {
-    return ((uint32_t)iz * g.dim.y + (uint32_t)iy) * g.dim.x + (uint32_t)ix;
-  };
+  DdaWalk w;
+  if (!dda_begin(G.grid, o, d, dist, w)) return false;
   float best = 3.0e38f;
   uint32_t best_i = kNone;
-  uint2 se = geo_ld(&G.start_end[cell_of(X.i, Y.i, Z.i)]);
-  const int max_iter = (int)(g.dim.x + g.dim.y + g.dim.z) + 3;
+  uint2 se = geo_ld(&G.start_end[dda_cell(G.grid, w.X.i, w.Y.i, w.Z.i)]);
+  const int max_iter = dda_max_iter(G.grid);
   for (int it = 0; it < max_iter; it++) {
     // the walk's next cell, and its triangle range on the way
-    const float texit = fminf(X.tmax, fminf(Y.tmax, Z.tmax));
-    const int ax = dda_next_axis(X, Y, Z);
-    int nx = X.i, ny = Y.i, nz = Z.i;
-    if (ax == 0) nx += X.step; else if (ax == 1) ny += Y.step; else nz += Z.step;
-    const bool more = texit <= t1 && nx >= 0 && nx < X.dim && ny >= 0 && ny < Y.dim && nz >= 0 && nz < Z.dim;
+    DdaNext nx;
+    const bool more = dda_peek(w, nx);
     uint2 se_next = make_uint2(0u, 0u);
-    if (more) se_next = geo_ld(&G.start_end[cell_of(nx, ny, nz)]);
+    if (more) se_next = geo_ld(&G.start_end[dda_cell(G.grid, nx.nx, nx.ny, nx.nz)]);
     for (uint32_t i0 = se.x; i0 < se.y; i0 += 8) {
       // the planes of up to 8 of the cell's triangles in one round of loads
       float4 P[8];
 #pragma unroll
       for (int k = 0; k < 8; k++)
         P[k] = i0 + k < se.y ? geo_ld(&G.plane[i0 + k]) : make_float4(0.f, 0.f, 0.f, 1.f);
-      // plane pre-test: both ends of the segment on one side -> no crossing;
-      // the others are the candidates, one bit each
+      // the triangles whose plane the segment may cross are the candidates,
+      // one bit each
       uint32_t cand = 0u;
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         if (i0 + k >= se.y) break;
-        const float3 pn = make_float3(P[k].x, P[k].y, P[k].z);
-        const float s0 = dot_x(pn, o) - P[k].w;
-        const float s1 = fmaf(dist, dot_x(pn, d), s0);
-        const float tol = __fmul_rn(1e-7f, fabsf(P[k].w) + 1.f);
-        if (!((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol))) cand |= 1u << k;
+        if (plane_may_cross(P[k], o, d, dist)) cand |= 1u << k;
       }
       // the candidates' vertices, in triangle order: the j-th round of the
       // loop loads every lane's j-th candidate at once, whatever its slot
       while (cand) {
         const uint32_t i = i0 + (uint32_t)(__ffs(cand) - 1);
         cand &= cand - 1u;
-        const float4 A = geo_ld(&G.tri[kTriStride * (size_t)i]);
-        const float4 B = geo_ld(&G.tri[kTriStride * (size_t)i + 1]);
-        const float4 C = geo_ld(&G.tri[kTriStride * (size_t)i + 2]);
         float t;
-        if (intersect_triangle_rel(o, d, make_float3(A.x, A.y, A.z), make_float3(B.x, B.y, B.z),
-                                   make_float3(C.x, C.y, C.z), &t) &&
-            t >= 0.f && t <= dist && t < best) {
+        if (entry_crossing(G, i, o, d, dist, &t) && t < best) {
           best = t;
           best_i = i;
         }
       }
     }
-    if (best <= texit || !more) break;
-    if (ax == 0) { X.i = nx; X.tmax += X.tdel; }
-    else if (ax == 1) { Y.i = ny; Y.tmax += Y.tdel; }
-    else { Z.i = nz; Z.tmax += Z.tdel; }
+    if (best <= nx.texit || !more) break;
+    dda_take(w, nx);
     se = se_next;
   }
   if (best_i == kNone) return false;

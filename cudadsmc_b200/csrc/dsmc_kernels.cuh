@@ -332,8 +332,10 @@ cudaError_t launch_inject_b(const BatchOf<InjectParams>& plan, uint32_t plan_blo
 // Full-wave block counts of the batched cell stages: order, NTC, flight, mesh,
 // sampling.
 cudaError_t cell_batch_waves(uint32_t wave[5], size_t flight_smem);
-// Stage 0 order, 1 NTC, 2 flight, 3 mesh, 4 sampling.
+// Stage 0 order, 1 NTC, 2 flight, 3 mesh, 4 sampling.  coop_mesh: every
+// member with a body uses nearest wall crossings (the mesh stage walks first
+// legs a warp at a time).
 cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32_t blocks, size_t flight_smem,
-                                cudaStream_t stream);
+                                bool coop_mesh, cudaStream_t stream);
 
 }  // namespace dsmcb

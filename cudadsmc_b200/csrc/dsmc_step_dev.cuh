@@ -642,6 +642,48 @@ __device__ __forceinline__ void wall_response(const GeomView& G, const NearestLe
   old_pos = hp;
 }
 
+// nearest_leg out of line, for legs walked by one lane where the caller
+// keeps its registers for other work.
+static __device__ __noinline__ int nearest_leg_call(const GeomView& G, float3 old_pos, float3 pos, bool pretested,
+                                                    NearestLeg& L) {
+  return nearest_leg(G, old_pos, pos, pretested, L);
+}
+
+// The legs of a flight with nearest wall crossings, after each re-emission
+// the rest of the flight (extension for bodies with diffuse walls).  first:
+// the first leg's answer when it is already known (r0 >= 0: its kLeg* code
+// and L0 its crossing), else r0 < 0 and the first leg is walked here
+// (pretested: its clearance test is done).  Returns false if the particle
+// is inside the body.
+template <bool CALL>
+__device__ __forceinline__ bool nearest_legs(const GeomView& G, float3& old_pos, float3& pos, float3& vel,
+                                             PhiloxStream& rng, bool pretested, int r0, const NearestLeg& L0) {
+  for (uint32_t b = 0; b < kCollisionLimit; b++) {
+    NearestLeg L;
+    int r;
+    if (b == 0 && r0 >= 0) {
+      L = L0;
+      r = r0;
+    } else if (CALL) {
+      r = nearest_leg_call(G, old_pos, pos, pretested && b == 0, L);
+    } else {
+      r = nearest_leg(G, old_pos, pos, pretested && b == 0, L);
+    }
+    if (r == kLegFree) break;
+    if (r == kLegInside) return false;
+    float2 reach = make_float2(0.f, 2.f);
+    if (G.reach) reach = geo_ld(&G.reach[L.e]);
+    wall_response(G, L, old_pos, pos, vel, rng);
+    // a leg within the wall's reach finds no wall (the next pass of the
+    // loop would find none and stop); 1e-5 covers the rounding of the sine
+    NearestLeg next;
+    if (reach.x > 0.f && leg_path(old_pos, pos, next) && next.dist < reach.x &&
+        fmaf(next.d.z, L.P.z, fmaf(next.d.x, L.P.x, __fmul_rn(next.d.y, L.P.y))) > reach.y + 1e-5f)
+      break;
+  }
+  return true;
+}
+
 // One particle's flight with the body: IntegrateDev / ProcessCollisionsDev,
 // kernels/dsmc_kernel.cu:1557-1657.  Returns false if the particle left.
 // pretested: the caller already found that the path from pos may reach the
@@ -660,22 +702,8 @@ __device__ __forceinline__ bool move_particle_body(const StepParams& p, float3& 
   if (p.has_geom && p.geom.nearest) {
     // nearest wall crossing along the path, repeated for the rest of the
     // flight after each re-emission (extension for bodies with diffuse walls)
-    const GeomView& G = p.geom;
-    for (uint32_t b = 0; b < kCollisionLimit; b++) {
-      NearestLeg L;
-      const int r = nearest_leg(G, old_pos, pos, pretested && b == 0, L);
-      if (r == kLegFree) break;
-      if (r == kLegInside) return false;
-      float2 reach = make_float2(0.f, 2.f);
-      if (G.reach) reach = geo_ld(&G.reach[L.e]);
-      wall_response(G, L, old_pos, pos, vel, rng);
-      // a leg within the wall's reach finds no wall (the next pass of the
-      // loop would find none and stop); 1e-5 covers the rounding of the sine
-      NearestLeg next;
-      if (reach.x > 0.f && leg_path(old_pos, pos, next) && next.dist < reach.x &&
-          fmaf(next.d.z, L.P.z, fmaf(next.d.x, L.P.x, __fmul_rn(next.d.y, L.P.y))) > reach.y + 1e-5f)
-        break;
-    }
+    const NearestLeg none{};
+    if (!nearest_legs<false>(p.geom, old_pos, pos, vel, rng, pretested, -1, none)) return false;
   } else if (p.has_geom) {
     const GeomView& G = p.geom;
     uint32_t st_cubid = kNone, end_cubid = kNone;
