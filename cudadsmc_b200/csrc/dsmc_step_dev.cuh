@@ -13,17 +13,15 @@ constexpr uint32_t kHeavyMin = 8;
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
-// Adds the lanes of `mask` holding `key` to count[key] (one atomic per
-// distinct key per warp, no return value) and to the block's histogram of scan
-// tiles.
+// Adds the lane's key to count[key] and to the block's histogram of scan
+// tiles: one atomic each per lane, no return value (measured faster than
+// matching the warp's equal keys first, or than one tile atomic per warp
+// when the lanes share a tile).  mask: the calling lanes.
 __device__ __forceinline__ void warp_count_key(uint32_t* count, uint32_t key, unsigned mask,
                                                uint32_t* s_tile) {
-  const unsigned peers = __match_any_sync(mask, key);
-  if ((int)lane_id() == __ffs(peers) - 1) {
-    const uint32_t cnt = __popc(peers);
-    atomicAdd(&count[key], cnt);
-    atomicAdd(&s_tile[key >> kScanShift], cnt);
-  }
+  (void)mask;
+  atomicAdd(&count[key], 1u);
+  atomicAdd(&s_tile[key >> kScanShift], 1u);
 }
 
 // Adds the lanes of `mask` holding `key` to count[key] and to the per scan
