@@ -546,6 +546,12 @@ __device__ __forceinline__ bool move_free(const StepParams& p, float3& pos, floa
   pos.x = fmaf(vel.x, p.dt, pos.x);
   pos.y = fmaf(vel.y, p.dt, pos.y);
   pos.z = fmaf(vel.z, p.dt, pos.z);
+  // a particle still inside the box crossed no face: every boundary functor
+  // leaves it as it is
+  const GridGeom& g = p.grid;
+  if (pos.x >= g.gmin.x && pos.x <= g.gmax.x && pos.y >= g.gmin.y && pos.y <= g.gmax.y && pos.z >= g.gmin.z &&
+      pos.z <= g.gmax.z)
+    return true;
   PhiloxStream rng;
   rng.init(p.seed, gidx, step, kPurposeWall);
   return apply_bc(p, pos, vel, rng);
