@@ -1136,7 +1136,7 @@ cudaError_t launch_order_w(const StepParams& p, cudaStream_t stream) {
   const uint32_t need = (p.n_tiles + WARPS - 1) / WARPS;
   if (grid > need) grid = need;
   if (grid == 0) return cudaSuccess;
-  return launch_chained(k_order_w<CAPW, WARPS, MINB>, grid, WARPS * 32, smem, stream, p);
+  return launch_chained(k_order_w<CAPW, WARPS, MINB>, grid, WARPS * 32, smem, stream, true, p);
 }
 
 constexpr int kFlightWarps = 8;
@@ -1159,7 +1159,7 @@ cudaError_t launch_flight_w(const StepParams& p, cudaStream_t stream) {
   }
   // a full wave of warps: the particle count is known only on the device
   return launch_chained(k_flight_w<kFlightWarps, MINB>, (uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
-                        p.n_scan_tiles * 4u, stream, p);
+                        p.n_scan_tiles * 4u, stream, true, p);
 }
 
 template <int MINB>
@@ -1179,7 +1179,7 @@ cudaError_t launch_flight_pw(const StepParams& p, cudaStream_t stream) {
     ls.per_sm = per_sm;
   }
   return launch_chained(k_flight_pw<kFlightWarps, MINB>, (uint32_t)(num_sms() * ls.per_sm), kFlightWarps * 32,
-                        p.n_scan_tiles * 4u, stream, p);
+                        p.n_scan_tiles * 4u, stream, true, p);
 }
 
 constexpr int kNtcWarps = 8;
@@ -1198,7 +1198,7 @@ cudaError_t launch_ntc_w(const StepParams& p, cudaStream_t stream) {
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  return launch_chained(k_ntc_w<kNtcWarps>, (uint32_t)(num_sms() * ls.per_sm), kNtcWarps * 32, 0, stream, p);
+  return launch_chained(k_ntc_w<kNtcWarps>, (uint32_t)(num_sms() * ls.per_sm), kNtcWarps * 32, 0, stream, true, p);
 }
 
 template <int MINB, bool COOP>
@@ -1216,11 +1216,11 @@ cudaError_t launch_mesh_w(const StepParams& p, cudaStream_t stream) {
     ls.device = dev;
     ls.per_sm = per_sm;
   }
-  return launch_chained(k_mesh_w<MINB, COOP>, (uint32_t)(num_sms() * ls.per_sm), 32 * kMeshWarps, 0, stream, p);
+  return launch_chained(k_mesh_w<MINB, COOP>, (uint32_t)(num_sms() * ls.per_sm), 32 * kMeshWarps, 0, stream, true, p);
 }
 
 cudaError_t launch_sample_w(const StepParams& p, cudaStream_t stream) {
-  return launch_chained(k_sample_w, grid_for(p.cells, 256, 8), 256, 0, stream, p);
+  return launch_chained(k_sample_w, grid_for(p.cells, 256, 8), 256, 0, stream, true, p);
 }
 
 }  // namespace
@@ -1296,13 +1296,13 @@ cudaError_t launch_cell_stage_b(int stage, const BatchOf<StepParams>& bv, uint32
                                 bool coop_mesh, cudaStream_t stream) {
   if (blocks == 0) return cudaSuccess;
   switch (stage) {
-    case 0: return launch_chained(k_order_wb<128, 4, 5>, blocks, 128, collide_smem_bytes<128, 4>(), stream, bv);
-    case 1: return launch_chained(k_ntc_wb<kNtcWarps>, blocks, kNtcWarps * 32, 0, stream, bv);
-    case 2: return launch_chained(k_flight_wb<kFlightWarps, 4>, blocks, kFlightWarps * 32, flight_smem, stream, bv);
+    case 0: return launch_chained(k_order_wb<128, 4, 5>, blocks, 128, collide_smem_bytes<128, 4>(), stream, false, bv);
+    case 1: return launch_chained(k_ntc_wb<kNtcWarps>, blocks, kNtcWarps * 32, 0, stream, false, bv);
+    case 2: return launch_chained(k_flight_wb<kFlightWarps, 4>, blocks, kFlightWarps * 32, flight_smem, stream, false, bv);
     case 3:
-      return coop_mesh ? launch_chained(k_mesh_wb<2, true>, blocks, 32 * kMeshWarps, 0, stream, bv)
-                       : launch_chained(k_mesh_wb<2, false>, blocks, 32 * kMeshWarps, 0, stream, bv);
-    default: return launch_chained(k_sample_wb, blocks, 256, 0, stream, bv);
+      return coop_mesh ? launch_chained(k_mesh_wb<2, true>, blocks, 32 * kMeshWarps, 0, stream, false, bv)
+                       : launch_chained(k_mesh_wb<2, false>, blocks, 32 * kMeshWarps, 0, stream, false, bv);
+    default: return launch_chained(k_sample_wb, blocks, 256, 0, stream, false, bv);
   }
 }
 

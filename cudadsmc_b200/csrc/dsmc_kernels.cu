@@ -670,7 +670,7 @@ cudaError_t launch_index(const GridGeom& g, uint32_t cells, const float* x, cons
 cudaError_t launch_scan(uint32_t* count, uint32_t* cursor, uint32_t* start, uint32_t cells,
                         const uint32_t* tile_sum, uint32_t n_scan_tiles, Meta* meta, int bump_step,
                         cudaStream_t stream) {
-  return launch_chained(k_scan, n_scan_tiles, 256, 0, stream, count, cursor, start, cells, tile_sum, meta,
+  return launch_chained(k_scan, n_scan_tiles, 256, 0, stream, true, count, cursor, start, cells, tile_sum, meta,
                         bump_step);
 }
 
@@ -680,7 +680,7 @@ cudaError_t launch_scatter(bool with_state, const SoA& src, SoA dst, const uint3
                            uint32_t n_scan_tiles, Meta* meta, uint32_t capacity,
                            cudaStream_t stream) {
   const uint32_t grid = (uint32_t)num_sms() * 4;
-  return launch_chained(with_state ? k_scatter<true> : k_scatter<false>, grid, 256, 0, stream, src, dst, keys,
+  return launch_chained(with_state ? k_scatter<true> : k_scatter<false>, grid, 256, 0, stream, true, src, dst, keys,
                         start, cursor, orig, cells, tile_sum, n_scan_tiles, meta, capacity);
 }
 
@@ -1061,26 +1061,26 @@ cudaError_t launch_init_fill(const InitParams& p, cudaStream_t stream) {
 }
 
 cudaError_t launch_scan_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream) {
-  return blocks ? launch_chained(k_scan_b, blocks, 256, 0, stream, bv) : cudaSuccess;
+  return blocks ? launch_chained(k_scan_b, blocks, 256, 0, stream, false, bv) : cudaSuccess;
 }
 
 cudaError_t launch_scatter_b(const BatchOf<SortArgs>& bv, uint32_t blocks, cudaStream_t stream) {
-  return blocks ? launch_chained(k_scatter_b, blocks, 256, 0, stream, bv) : cudaSuccess;
+  return blocks ? launch_chained(k_scatter_b, blocks, 256, 0, stream, false, bv) : cudaSuccess;
 }
 
 cudaError_t launch_inject_b(const BatchOf<InjectParams>& plan, uint32_t plan_blocks,
                             const BatchOf<InjectParams>& fill, uint32_t fill_blocks, size_t fill_smem,
                             cudaStream_t stream) {
   cudaError_t e = cudaSuccess;
-  if (plan_blocks) e = launch_chained(k_inject_plan_b, plan_blocks, 32, 0, stream, plan);
-  if (!e && fill_blocks) e = launch_chained(k_inject_fill_b, fill_blocks, 256, fill_smem, stream, fill);
+  if (plan_blocks) e = launch_chained(k_inject_plan_b, plan_blocks, 32, 0, stream, false, plan);
+  if (!e && fill_blocks) e = launch_chained(k_inject_fill_b, fill_blocks, 256, fill_smem, stream, false, fill);
   return e;
 }
 
 cudaError_t launch_inject(const InjectParams& p, cudaStream_t stream) {
-  cudaError_t e = launch_chained(k_inject_plan, 1, 32, 0, stream, p, p.plan);
+  cudaError_t e = launch_chained(k_inject_plan, 1, 32, 0, stream, true, p, p.plan);
   const uint32_t grid = (uint32_t)num_sms();
-  if (!e) e = launch_chained(k_inject_fill, grid, 256, p.n_scan_tiles * 4, stream, p, p.plan);
+  if (!e) e = launch_chained(k_inject_fill, grid, 256, p.n_scan_tiles * 4, stream, true, p, p.plan);
   return e;
 }
 

@@ -155,7 +155,7 @@ cudaError_t launch_mt_maximums(const uint4* cfg, uint32_t* state, float2* maxrem
 
 cudaError_t launch_ntc_mt(const StepParams& p, uint32_t* mt_state, const uint4* mt_cfg,
                           cudaStream_t stream) {
-  return launch_chained(k_ntc_mt<kNtcMtWarps>, (uint32_t)num_sms() * 8u, kNtcMtWarps * 32, 0, stream, p, mt_state,
+  return launch_chained(k_ntc_mt<kNtcMtWarps>, (uint32_t)num_sms() * 8u, kNtcMtWarps * 32, 0, stream, true, p, mt_state,
                         mt_cfg);
 }
 
