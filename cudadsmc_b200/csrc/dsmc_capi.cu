@@ -390,7 +390,10 @@ cudaError_t enqueue_step(dsmc_handle* h, float dt) {
                                  h->capacity, h->stream);
   });
   if (e) return e;
-  const dsmcb::StepParams p = step_params(h, dt, split);
+  dsmcb::StepParams p = step_params(h, dt, split);
+  // the sampling kernel closes a captured graph (the graph replay after it
+  // waits for every node of this one)
+  p.graph_tail = h->capturing ? 1 : 0;
   // the inflow branch (not while the injection itself is being timed: its
   // events are on the handle's stream)
   const bool fork = split && !h->inflows.empty() && h->side &&

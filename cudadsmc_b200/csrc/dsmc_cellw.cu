@@ -1076,17 +1076,27 @@ __global__ void __launch_bounds__(32 * kMeshWarps, MINB) k_mesh_wb(const __grid_
 // FP64 sampling after the flights, one cell per thread (the reference's
 // SampleCellStatisticsDev order: each cell's particles in sorted order, with
 // their velocities after the move); returns at once on other steps.
-// The step counter was bumped by the step's scan kernel, which completed
-// before the kernel that this one follows began (each kernel of the step
-// waits for its predecessor), so the counter is read before the wait: on a
-// step without sampling the kernel ends without waiting for the mesh kernel.
+// A kernel of the step must not complete before the one it follows: a
+// chained kernel after it (the next step's scan, launched directly) waits
+// only for it.  In a captured step graph this kernel is the graph's last
+// (graph_tail; only the inflow kernels, which run beside the mesh kernel by
+// design, may follow it), and the next replay waits for the whole graph: on
+// a step without sampling it then ends without waiting for the mesh kernel.
+// The step counter it reads first was bumped by the step's scan kernel,
+// which completed before the kernel this one follows began.
 __device__ __forceinline__ void sample_body(const StepParams& p, const uint32_t vb, const uint32_t vg) {
-  const uint32_t step = p.step_override ? p.step_override : __ldcg(&p.meta->step);
+  if (p.graph_tail) {
+    const uint32_t step = p.step_override ? p.step_override : __ldcg(&p.meta->step);
+    const bool idle = !(p.flags & kDoSample) ||
+                      (!(p.flags & kSampleForce) && !(p.sample_every > 0 && step % (uint32_t)p.sample_every == 0));
+    if (idle) return;
+  }
+  chained_entry();
+  const uint32_t step = p.step_override ? p.step_override : p.meta->step;
   const bool do_sample =
       (p.flags & kDoSample) &&
       ((p.flags & kSampleForce) || (p.sample_every > 0 && step % (uint32_t)p.sample_every == 0));
   if (!do_sample) return;
-  chained_entry();
   for (uint32_t c = vb * blockDim.x + threadIdx.x; c < p.cells; c += vg * blockDim.x) {
     const uint32_t s = __ldg(&p.start[c]), e = __ldg(&p.start[c + 1]);
     GlobalVel a{p.out.u, p.out.v, p.out.w, s};

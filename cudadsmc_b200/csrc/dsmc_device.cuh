@@ -227,7 +227,10 @@ __device__ __forceinline__ bool intersect_triangle(float3 orig, float3 dir, floa
 // here, before its first access to memory, until that kernel has completed
 // and its writes are visible (griddepcontrol.wait is a no-op for a kernel
 // launched without the attribute).  It then allows the next kernel's launch
-// to begin, which dispatches once every CTA of this one has started.
+// to begin, which dispatches once every CTA of this one has started.  Every
+// CTA of a chained kernel calls this first, whatever work it has: a kernel
+// waits only for its direct predecessor, so the chain orders the whole step
+// only if no kernel can complete before the one it follows.
 __device__ __forceinline__ void chained_entry() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");

@@ -153,6 +153,8 @@ struct StepParams {
   uint32_t* defer_list;    // split variants: flights that may reach the body
                            // (capacity entries; the orig buffer, dead once the
                            // collide kernel has read it)
+  int graph_tail;          // 1: the sampling kernel ends a captured step graph (nothing
+                           // after it in the graph reads the step's keys or counts)
 };
 
 // A batched launch: one grid for several members (instances of the step),
