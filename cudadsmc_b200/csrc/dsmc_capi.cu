@@ -54,6 +54,7 @@ struct dsmc_handle {
   uint32_t* gflags = nullptr;
   float* gclear = nullptr;
   float2* greach = nullptr;  // per bin entry (null: the mesh's scale is too large for it)
+  float4* gslab = nullptr;   // per cell of the triangle grid
   uint2* gse = nullptr;
   float4* gtri = nullptr;
   float4* gplane = nullptr;
@@ -177,7 +178,7 @@ void free_all(dsmc_handle* h) {
     h->A[i] = h->B[i] = nullptr;
   }
   void* ps[] = {h->orig, h->ntc_list, h->keys, h->cursor, h->count, h->start, h->tile_sum, h->maxrem, h->seeds,
-                h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->greach,
+                h->acc, h->cellbuf, h->meta, h->inj_rem, h->inj_plan, h->gflags, h->gclear, h->greach, h->gslab,
                 h->gse, h->gtri, h->gplane, h->mt_state, h->mt_cfg};
   for (void* p : ps) cudaFree(p);
   h->mt_state = nullptr;
@@ -245,6 +246,7 @@ dsmcb::StepParams base_params(dsmc_handle* h, float dt) {
     p.geom.plane = h->gplane;
     p.geom.clear = h->gclear;
     p.geom.reach = h->greach;
+    p.geom.slab = h->gslab;
     p.geom.cgrid = h->gcgrid;
     p.geom.diffuse = h->cfg.wall_diffuse;
     p.geom.nearest = h->cfg.geom_nearest;
@@ -800,6 +802,8 @@ static int install_geometry(dsmc_handle* h, dsmcb::GeomDevice& gd) {
   cudaFree(h->gclear);
   cudaFree(h->greach);
   h->greach = nullptr;
+  cudaFree(h->gslab);
+  h->gslab = nullptr;
   cudaFree(h->gse);
   cudaFree(h->gtri);
   cudaFree(h->gplane);
@@ -837,13 +841,19 @@ static int install_geometry(dsmc_handle* h, dsmcb::GeomDevice& gd) {
     float mag = 0.f;
     for (int k = 0; k < 6; k++) mag = std::max(mag, std::fabs(g.bbox[k]));
     const size_t entries = g.tri_ids.size();
+    gv.plane = h->gplane;
     if (mag < 2.0f && entries) {
       CK(h, dalloc(&h->greach, entries), "geometry alloc");
-      gv.plane = h->gplane;
       ce = dsmcb::launch_entry_reach(gv, (uint32_t)entries, cmin, 1e-7f, 4e-6f, h->greach, nullptr);
       if (!ce) ce = cudaDeviceSynchronize();
       CK(h, ce, "entry reach");
     }
+    // per cell, the slab that holds its triangles (the mesh kernel's cell
+    // pre-test)
+    CK(h, dalloc(&h->gslab, gc), "geometry alloc");
+    ce = dsmcb::launch_cell_slab(gv, gc, h->gslab, nullptr);
+    if (!ce) ce = cudaDeviceSynchronize();
+    CK(h, ce, "cell slabs");
   }
   h->has_geom = true;
   h->cfg.geometry = 1;

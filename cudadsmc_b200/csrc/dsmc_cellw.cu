@@ -910,15 +910,27 @@ __device__ __forceinline__ int coop_first_leg(const GeomView& G, MeshCoop& S, bo
   S.ox[lane] = o.x; S.oy[lane] = o.y; S.oz[lane] = o.z;
   S.dx[lane] = L.d.x; S.dy[lane] = L.d.y; S.dz[lane] = L.d.z;
   S.dist[lane] = L.dist;
-  // the visited cells' entry ranges, loaded together
+  // the visited cells' entry ranges and slabs, loaded together; a cell whose
+  // slab the path stays outside contributes no entries
   uint2 se[kCoopCells];
+  bool pass[kCoopCells];
 #pragma unroll
-  for (int j = 0; j < kCoopCells; j++)
+  for (int j = 0; j < kCoopCells; j++) {
     se[j] = j < nc ? geo_ld(&G.start_end[S.cstart[lane][j]]) : make_uint2(0u, 0u);
+    pass[j] = true;
+  }
+  if (G.slab) {
+    float4 sl[kCoopCells];
+#pragma unroll
+    for (int j = 0; j < kCoopCells; j++)
+      sl[j] = j < nc ? geo_ld(&G.slab[S.cstart[lane][j]]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < kCoopCells; j++) pass[j] = slab_may_cross(sl[j], o, L.d, L.dist);
+  }
   uint32_t tot = 0;
 #pragma unroll
   for (int j = 0; j < kCoopCells; j++) {
-    const uint32_t cnt = (j < nc && se[j].x != kNone) ? se[j].y - se[j].x : 0u;
+    const uint32_t cnt = (j < nc && se[j].x != kNone && pass[j]) ? se[j].y - se[j].x : 0u;
     S.cstart[lane][j] = se[j].x;
     S.cpre[lane][j] = tot;
     S.best[lane][j] = ~0ull;

@@ -254,6 +254,12 @@ struct GeomView {
   // crosses no listed triangle; r = 0 where that holds for no path; null:
   // no table
   const float2* reach;
+  // per grid cell, a slab that holds every vertex of the cell's listed
+  // triangles: (m, e) with |m . x - e| <= 1 on all of them (m the slab's
+  // normal over its half thickness); a path that stays outside the slab
+  // crosses none of the cell's triangles.  (0, 0, 0, 0) passes every path;
+  // null: no slabs
+  const float4* slab;
   // clearance table: per cell of cgrid (the triangle grid refined by a small
   // factor, same bounds), a lower bound of the distance from any point of the
   // cell to the surface
@@ -392,6 +398,18 @@ __device__ __forceinline__ void dda_take(DdaWalk& w, const DdaNext& n) {
 
 // The walk's iteration limit for a grid.
 __device__ __forceinline__ int dda_max_iter(const GridGeom& g) { return (int)(g.dim.x + g.dim.y + g.dim.z) + 3; }
+
+// Slab pre-test of a grid cell (GeomView::slab) for the segment o + s d,
+// s in [0, dist]: false when both ends lie beyond the same face of the slab.
+// The margin covers the rounding of the two products, whose terms grow with
+// the slab's inverse thickness.
+__device__ __forceinline__ bool slab_may_cross(float4 S, float3 o, float3 d, float dist) {
+  const float s0 = fmaf(S.z, o.z, fmaf(S.x, o.x, __fmul_rn(S.y, o.y))) - S.w;
+  const float s1 = fmaf(dist, fmaf(S.z, d.z, fmaf(S.x, d.x, __fmul_rn(S.y, d.y))), s0);
+  const float big = fabsf(S.x) + fabsf(S.y) + fabsf(S.z);
+  const float tol = 1.f + fmaf(4e-7f * big, fabsf(o.x) + fabsf(o.y) + fabsf(o.z) + dist, 4e-7f * fabsf(S.w));
+  return !((s0 > tol && s1 > tol) || (s0 < -tol && s1 < -tol));
+}
 
 // Plane pre-test of a triangle for the segment o + s d, s in [0, dist]: false
 // when both ends lie on one side of its plane (beyond a rounding margin).

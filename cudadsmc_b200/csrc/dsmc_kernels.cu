@@ -1016,6 +1016,48 @@ __global__ void k_entry_reach(const __grid_constant__ GeomView g, uint32_t entri
   }
 }
 
+// The slab of every grid cell (GeomView::slab): n the normalised sum of the
+// cell's triangle normals, [lo, hi] the range of n . v over every vertex of
+// every listed triangle (FP64), widened by a margin; m = n / h, e = c / h
+// with c the middle and h the half width.  Cells whose normals disagree
+// (the sum shorter than half the count) pass every path.
+__global__ void k_cell_slab(const __grid_constant__ GeomView g, uint32_t cells, float4* __restrict__ out) {
+  for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+    const uint2 se = g.start_end[c];
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (se.x != kNone && se.y > se.x) {
+      double nx = 0.0, ny = 0.0, nz = 0.0;
+      for (uint32_t i = se.x; i < se.y; i++) {
+        const float4 P = g.plane[i];
+        nx += P.x; ny += P.y; nz += P.z;
+      }
+      const double l = sqrt(nx * nx + ny * ny + nz * nz);
+      if (l >= 0.5 * (double)(se.y - se.x)) {
+        nx /= l; ny /= l; nz /= l;
+        double lo = 1e300, hi = -1e300, mag = 0.0;
+        for (uint32_t i = se.x; i < se.y; i++)
+          for (int k = 0; k < 3; k++) {
+            const float4 v = g.tri[kTriStride * (size_t)i + k];
+            const double t = nx * v.x + ny * v.y + nz * v.z;
+            lo = fmin(lo, t);
+            hi = fmax(hi, t);
+            mag = fmax(mag, fabs((double)v.x) + fabs((double)v.y) + fabs((double)v.z));
+          }
+        const double cmid = 0.5 * (lo + hi);
+        const double h = 0.5 * (hi - lo) + 1e-6 + 1e-6 * mag;
+        r = make_float4((float)(nx / h), (float)(ny / h), (float)(nz / h), (float)(cmid / h));
+      }
+    }
+    out[c] = r;
+  }
+}
+
+cudaError_t launch_cell_slab(const GeomView& g, uint32_t cells, float4* out, cudaStream_t stream) {
+  if (cells == 0) return cudaSuccess;
+  k_cell_slab<<<grid_for(cells, 128, 8), 128, 0, stream>>>(g, cells, out);
+  return cudaGetLastError();
+}
+
 __global__ void k_clearance_at(const __grid_constant__ GeomView g, const float* __restrict__ xyz,
                                uint32_t n, float* __restrict__ out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {

@@ -298,6 +298,9 @@ cudaError_t launch_fine_clearance(const GeomView& g, const GridGeom& fine, uint3
 cudaError_t launch_entry_reach(const GeomView& g, uint32_t entries, float rmax, float tol, float slack,
                                float2* out, cudaStream_t stream);
 
+// The slab of every cell of the triangle grid (k_cell_slab; GeomView::slab).
+cudaError_t launch_cell_slab(const GeomView& g, uint32_t cells, float4* out, cudaStream_t stream);
+
 // out[i] = clearance table entry at point i (xyz interleaved), -1 outside.
 cudaError_t launch_clearance_at(const GeomView& g, const float* xyz, uint32_t n, float* out,
                                 cudaStream_t stream);
