@@ -103,6 +103,7 @@ SIGNATURES = [
     ("dsmc_get_geometry_grid", _I, [_P, _P, _P, _P, _P, _P, _P, ctypes.c_uint64, _P,
                                     ctypes.POINTER(ctypes.c_uint64)]),
     ("dsmc_get_entry_reach", _I, [_P, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
+    ("dsmc_get_cell_slabs", _I, [_P, _P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     ("dsmc_read_raw_mesh", _I, [ctypes.c_char_p, _P, ctypes.POINTER(_U32), _P,
                                 ctypes.POINTER(_U32), _P]),
     ("dsmc_mesh_icosphere", _I, [_I, ctypes.c_float, _P, _P, ctypes.POINTER(_U32), _P,

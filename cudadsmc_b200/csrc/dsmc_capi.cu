@@ -970,6 +970,17 @@ int dsmc_get_entry_reach(dsmc_handle* h, float* out, uint64_t cap, uint64_t* n_e
   return DSMC_OK;
 }
 
+int dsmc_get_cell_slabs(dsmc_handle* h, float* out, uint64_t cap, uint64_t* n_cells) {
+  if (!h) return DSMC_ERR_ARG;
+  if (!h->has_geom) return fail(h, DSMC_ERR_STATE, "no geometry grid (dsmc_set_mesh)");
+  const auto& g = h->ggrid;
+  const size_t total = h->gslab ? (size_t)g.dim[0] * g.dim[1] * g.dim[2] : 0;
+  const size_t n = std::min<size_t>(cap, total);
+  if (out && n) CK(h, cudaMemcpy(out, h->gslab, n * sizeof(float4), cudaMemcpyDeviceToHost), "read slabs");
+  if (n_cells) *n_cells = total;
+  return DSMC_OK;
+}
+
 int dsmc_read_raw_mesh(const char* path, float* verts, uint32_t* nverts, uint32_t* tris,
                        uint32_t* ntris, float* face_normals) {
   if (!path || !nverts || !ntris) return DSMC_ERR_ARG;

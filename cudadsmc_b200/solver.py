@@ -287,6 +287,17 @@ class DSMCSolver:
                         "EntryReach")
         return out
 
+    def CellSlabs(self):
+        """Per cell of the geometry grid, [cells, 4]: (m.x, m.y, m.z, e) with
+        |m . v - e| <= 1 for every vertex v of the cell's listed triangles
+        (zeros: the cell passes every path)."""
+        nc = ctypes.c_uint64()
+        self._check(lib().dsmc_get_cell_slabs(self.h, None, 0, ctypes.byref(nc)), "CellSlabs")
+        out = np.zeros((nc.value, 4), np.float32)
+        if nc.value:
+            self._check(lib().dsmc_get_cell_slabs(self.h, _ptr(out), nc.value, ctypes.byref(nc)), "CellSlabs")
+        return out
+
     def GeometryGrid(self):
         """The handle's geometry grid (built on the device by SetModel): bbox,
         cell size, dims, per-cell triangle counts, triangle ids in bin order,

@@ -483,6 +483,15 @@ int dsmc_clearance_at(dsmc_handle* h, const float* xyz, uint32_t n, float* out, 
  * coordinates' rounding). */
 int dsmc_get_entry_reach(dsmc_handle* h, float* out, uint64_t cap, uint64_t* n_entries);
 
+/* Per cell of the geometry grid (cell-major, x fastest), the slab that holds
+ * every vertex of the cell's listed triangles, as 4 floats (m.x, m.y, m.z,
+ * e): |m . v - e| <= 1 for each such vertex v (m the triangles' mean normal
+ * over the slab's half thickness); (0, 0, 0, 0) for an empty cell or one
+ * whose normals disagree.  The mesh step skips a cell whose slab a path
+ * stays outside.  At most cap cells into out (host memory); *n_cells gets
+ * the cell count. */
+int dsmc_get_cell_slabs(dsmc_handle* h, float* out, uint64_t cap, uint64_t* n_cells);
+
 /* IntegrateDev / ProcessCollisionsDev (kernels/dsmc_kernel.cu:1557-1699):
  * free flight, mesh collisions (with the handle's geometry when h != NULL and
  * it has one) and the boundary functor, in place on the six arrays. */

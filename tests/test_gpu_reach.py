@@ -160,3 +160,40 @@ def test_reach_stops_at_a_dent(cuda):
     assert np.mean((r[near] < cap) | (k[near] > 0.1)) > 0.5
     assert checked > 0
     sol.close()
+
+
+@pytest.mark.parametrize("mesh", ["sphere", "capsule", "crater"])
+def test_cell_slabs_hold_their_triangles(cuda, mesh):
+    """Every vertex of a cell's listed triangles lies inside the cell's slab
+    (|m . v - e| <= 1), and the slabs are thin where the surface is smooth."""
+    center = np.array([0.5, 0.25, 0.25])
+    if mesh == "capsule":
+        verts, tris = mesh_capsule(0.15, 20.0, 0.26, (0.4, 0.25, 0.25), 4000, 7)
+        grid = (24, 32, 32)
+    else:
+        verts, tris = mesh_icosphere(3, 0.1, tuple(center))
+        grid = (16, 16, 16)
+        if mesh == "crater":
+            v = verts.astype(np.float64) - center
+            u = v / np.linalg.norm(v, axis=1, keepdims=True)
+            v *= (1.0 - 0.35 * np.clip((u[:, 0] - 0.8) / 0.2, 0.0, 1.0))[:, None]
+            verts = (v + center).astype(np.float32)
+    sol = solver_with(verts, tris, grid)
+    _, cell, dim, count, ids, _, _ = sol.GeometryGrid()
+    slabs = sol.CellSlabs().astype(np.float64)
+    assert slabs.shape == (int(np.prod(dim)), 4)
+    start = np.concatenate([np.zeros(1, np.int64), np.cumsum(count.astype(np.int64))])
+    v = verts.astype(np.float64)
+    used = 0
+    for c in np.nonzero(count)[0]:
+        m, e = slabs[c, :3], slabs[c, 3]
+        if not np.any(m):
+            continue
+        used += 1
+        pts = v[tris[ids[start[c]:start[c + 1]]]].reshape(-1, 3)
+        assert np.all(np.abs(pts @ m - e) <= 1.0 + 1e-6), c
+    # most cells of a smooth body get a slab, a thin one
+    assert used > 0.9 * np.count_nonzero(count)
+    thick = 1.0 / np.linalg.norm(slabs[:, :3], axis=1)[np.any(slabs[:, :3], axis=1)]
+    assert np.median(thick) < 0.25 * float(np.min(cell))
+    sol.close()
