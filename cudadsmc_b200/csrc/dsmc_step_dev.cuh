@@ -78,6 +78,7 @@ struct PhiloxRng {
 
 // Stream purposes in Philox counter word 3.
 constexpr uint32_t kPurposeCollide = 0x636f6c6cu;
+constexpr uint32_t kPurposePairs = 0x70616972u;  // a light cell's pair choices
 constexpr uint32_t kPurposeWall = 0x77616c6cu;
 constexpr uint32_t kPurposeInit = 0x696e6974u;
 constexpr uint32_t kPurposeInject = 0x696e6a65u;
@@ -254,19 +255,38 @@ __device__ __forceinline__ uint32_t ntc_pairs_fast(const StepParams& p, uint32_t
 }
 
 // NTC selections of one cell in the Philox mode (one lane): distinct pairs,
-// acceptance sigma*g > R (sigma*g)max; returns the collisions.
+// acceptance sigma*g > R (sigma*g)max; returns the collisions.  The pairs
+// are drawn from the cell's pair stream and the acceptance and scattering
+// numbers from its collision stream, so the next pair is known before this
+// one is decided: its velocities are loaded while this pair is evaluated
+// (loads issued before this pair's stores; where the two pairs share a
+// particle the next pair takes this pair's result instead).
 template <class Acc>
 __device__ __forceinline__ uint32_t ntc_select_fast(const StepParams& p, uint32_t cell, uint32_t n,
                                                     Acc acc, uint32_t step, uint32_t M, float2& vm,
                                                     double& sum_g) {
-  PhiloxStreamInline r;
+  PhiloxStreamInline r, q;
   r.init(p.seed, cell, step, kPurposeCollide);
+  q.init(p.seed, cell, step, kPurposePairs);
   uint32_t ncol = 0;
+  if (M == 0) return 0;
+  auto draw = [&](uint32_t& a, uint32_t& b) {
+    a = __umulhi(q.next(), n);
+    b = a + 1u + __umulhi(q.next(), n - 1u);
+    if (b >= n) b -= n;
+  };
+  uint32_t pi, pj;
+  draw(pi, pj);
+  float3 v1 = acc.get(pi), v2 = acc.get(pj);
   for (uint32_t i = 0; i < M; i++) {
-    const uint32_t pi = __umulhi(r.next(), n);
-    uint32_t pj = pi + 1u + __umulhi(r.next(), n - 1u);
-    if (pj >= n) pj -= n;
-    const float3 v1 = acc.get(pi), v2 = acc.get(pj);
+    uint32_t ni = 0, nj = 0;
+    float3 w1 = v1, w2 = v2;
+    const bool more = i + 1 < M;
+    if (more) {
+      draw(ni, nj);
+      w1 = acc.get(ni);
+      w2 = acc.get(nj);
+    }
     const float mag = rel_speed(v1, v2);
     const float v = sigma_g_fast(p, mag);
     if (v > r.uniform() * vm.x) {
@@ -277,8 +297,14 @@ __device__ __forceinline__ uint32_t ntc_select_fast(const StepParams& p, uint32_
       scatter_pair(v1, v2, mag, rc, rp, o1, o2);
       acc.set(pi, o1);
       acc.set(pj, o2);
+      if (ni == pi) w1 = o1; else if (ni == pj) w1 = o2;
+      if (nj == pi) w2 = o1; else if (nj == pj) w2 = o2;
     }
     if (v > vm.x) vm.x = v;
+    pi = ni;
+    pj = nj;
+    v1 = w1;
+    v2 = w2;
   }
   return ncol;
 }

@@ -45,6 +45,7 @@
 #define FO_NONE 0xffffffffu
 #define FO_PI 3.14159265358979323846
 #define FO_PURPOSE_COLLIDE 0x636f6c6cu
+#define FO_PURPOSE_PAIRS 0x70616972u
 #define FO_PURPOSE_WALL 0x77616c6cu
 #define FO_PURPOSE_INJECT 0x696e6a65u
 #define FO_PURPOSE_HEAVY 0x68650000u
@@ -166,16 +167,18 @@ static uint32_t pairs_fast(const orc_fast* f, uint32_t n, float* vmx, float* rem
 }
 
 /* The selections of one cell by one lane (ntc_select_fast): M pairs of
- * distinct particles from the cell's own stream, accepted when
- * sigma g > R (sigma g)max, (sigma g)max raised as they come. */
+ * distinct particles drawn from the cell's pair stream, accepted when
+ * sigma g > R (sigma g)max with R and the scattering angles from the cell's
+ * collision stream, (sigma g)max raised as they come. */
 static uint32_t select_lane(const orc_fast* f, uint32_t cell, uint32_t n, const vel_view* acc,
                             uint32_t M, float* vmx, double* sum_g, uint32_t* ties) {
-  pstream r;
+  pstream r, q;
   ps_init(&r, f->key, cell, f->step, FO_PURPOSE_COLLIDE);
+  ps_init(&q, f->key, cell, f->step, FO_PURPOSE_PAIRS);
   uint32_t ncol = 0;
   for (uint32_t i = 0; i < M; i++) {
-    const uint32_t pi = umulhi(ps_next(&r), n);
-    uint32_t pj = pi + 1u + umulhi(ps_next(&r), n - 1u);
+    const uint32_t pi = umulhi(ps_next(&q), n);
+    uint32_t pj = pi + 1u + umulhi(ps_next(&q), n - 1u);
     if (pj >= n) pj -= n;
     float v1[3], v2[3];
     vget(acc, pi, v1);

@@ -166,8 +166,9 @@ def test_collide_philox_matches_oracle(cuda, omega):
 
 def test_philox_stream_matches_oracle(cuda):
     """The device's Philox-4x32-10 words (through the stage collide's first
-    pair draws of a 2-particle cell: pi = umulhi(r0, 2), pj = 1 - pi) and the
-    oracle's known-answer generator give the same pair choices."""
+    pair draws of a 2-particle cell from its pair stream: pi = umulhi(r0, 2),
+    pj = 1 - pi) and the oracle's known-answer generator give the same pair
+    choices."""
     ncells = 1024
     counts = np.full(ncells, 2, np.int64)
     start = np.zeros(ncells + 1, np.uint32)
@@ -196,9 +197,9 @@ def test_philox_stream_matches_oracle(cuda):
     torch.cuda.synchronize()
     vg = np.stack([t.cpu().numpy() for t in (u, v, w)])
     assert info[:, 0].min() == 1 and info[:, 1].min() == 1
-    # the first word of each cell's stream decides the slot order: check it
-    # against the known-answer Philox of the oracle directly
-    first = np.array([O.philox([0, c, 5, 0x636f6c6c], O.seed_words(SEED))[0] for c in range(ncells)],
+    # the first word of each cell's pair stream decides the slot order: check
+    # it against the known-answer Philox of the oracle directly
+    first = np.array([O.philox([0, c, 5, 0x70616972], O.seed_words(SEED))[0] for c in range(ncells)],
                      np.uint64)
     pi = (first * 2) >> 32
     assert set(np.unique(pi).tolist()) == {0, 1}
