@@ -208,6 +208,47 @@ def test_philox_stream_matches_oracle(cuda):
     assert np.max(np.abs(vg - vo)) <= 1e-6 * 1000.0
 
 
+@pytest.mark.parametrize("count", [2, 3])
+def test_light_cell_pairs_sharing_particles(cuda, count):
+    """Light cells of 2 or 3 particles with 5 pairs each and a low
+    (sigma g)max, so that most pairs collide: consecutive pairs share
+    particles, and the next pair's velocities (loaded while the current pair
+    is decided) must be replaced by the current pair's results.  Velocities
+    match the oracle's sequential selections (cells with a near-tie
+    acceptance excluded, as everywhere)."""
+    ncells = 2048
+    counts = np.full(ncells, count, np.int64)
+    start = np.zeros(ncells + 1, np.uint32)
+    start[1:] = np.cumsum(counts)
+    n = int(start[-1])
+    rng = np.random.default_rng(21 + count)
+    vel = rng.normal(0.0, 500.0, (3, n)).astype(np.float32)
+    cs = O.cross_section_of(D_AR)
+    mr = np.zeros((ncells, 2), np.float32)
+    mr[:, 0] = np.float32(cs * 1.0)  # below every sigma g: the first pair is accepted
+    mr[:, 1] = np.float32(0.5)
+    fnum, cell_volume = 1e15, float(np.float32(1.0 / 4096))
+    # 5.2 + remainder 0.5 selections per cell: M = 5 (a light cell)
+    dt = float(np.float32(5.2 / (0.5 * fnum / cell_volume * count * (count - 1) * float(mr[0, 0]))))
+    f = O.fast_params(SEED, 11, fnum, dt, cell_volume, cs, 0.5, 0.0, ntc_local=1, warp_cap=2048)
+    vo, mr_o = vel.copy(), mr.copy()
+    info, _ = O.collide_fast(f, vo[0], vo[1], vo[2], start, mr_o)
+    assert np.all(info[:, 0] == 5) and info[:, 1].min() >= 1 and info[:, 1].mean() > 2.5
+    u, v, w = (T(vel[k].copy(), cuda) for k in range(3))
+    mr_t = T(mr.copy(), cuda)
+    p = stages.collide_params(ncells, cell_volume, cs, fnum, 0.0, dt, ntc_local=1, rng="philox",
+                              seed=SEED, step=11)
+    stages.collide(p, u, v, w, U32(start, cuda), mr_t)
+    torch.cuda.synchronize()
+    vg = np.stack([t.cpu().numpy() for t in (u, v, w)])
+    ok = np.repeat(info[:, 3] == 0, counts)
+    assert ok.mean() > 0.99
+    speed = np.maximum(np.linalg.norm(vo.astype(np.float64), axis=0), 1.0)
+    # five collisions per particle at most: 5 x 1e-6 of the speed
+    assert np.max(np.max(np.abs(vg - vo), axis=0)[ok] / speed[ok]) <= 5e-6
+    assert np.array_equal(mr_t.cpu().numpy()[:, 1], mr_o[:, 1])
+
+
 def sphere_solver(dim=(32, 16, 16), dom=(0.6, 0.3, 0.3), density=1e20, ppc=8.0, radius=0.06,
                   level=3, variant=None, faces=None, temp=200.0, stream=1500.0, dt=4e-6):
     cell_v = (dom[0] / dim[0]) * (dom[1] / dim[1]) * (dom[2] / dim[2])
