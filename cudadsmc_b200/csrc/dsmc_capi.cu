@@ -1184,9 +1184,11 @@ int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out)
   uint32_t kmax = 0;
   for (uint32_t cell = 0; cell < h->cells; cell++) {
     const float* f = fields5 + 5 * (size_t)cell;
-    // n V_c / F_N particles in the part of the cell outside the body
-    const double expect = (std::isfinite(f[0]) && f[0] > 0.f)
-                              ? (double)f[0] * h->cell_volume / c.fnum * frac[cell] : 0.0;
+    // n is averaged over the whole cell volume (as dsmc_read_fields gives
+    // it), so a cell the body cuts receives its n V_c / F_N particles in the
+    // part outside the body; a cell the body covers stays empty
+    const double expect = (std::isfinite(f[0]) && f[0] > 0.f && frac[cell] > 0.f)
+                              ? (double)f[0] * h->cell_volume / c.fnum : 0.0;
     const double fl = std::floor(expect);
     const uint32_t k = (uint32_t)fl + (unit_draw(mix) < expect - fl ? 1u : 0u);
     slot[cell] = (uint32_t)n;

@@ -114,7 +114,9 @@ class DSMCSolver:
         return n.value
 
     def InitFromFields(self, fields):
-        """Seeds the particles from per-cell (n, u, v, w, T) fields [cells, 5]."""
+        """Seeds the particles from per-cell (n, u, v, w, T) fields [cells, 5],
+        n averaged over the whole cell volume as Fields() gives it (a cell the
+        body cuts receives n V_c / F_N particles outside the body)."""
         f = np.ascontiguousarray(fields, np.float32).reshape(-1, 5)
         if f.shape[0] != self.settings.getCellsCount():
             raise ValueError("fields must hold one (n, u, v, w, T) row per cell")

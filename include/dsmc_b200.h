@@ -232,9 +232,13 @@ int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out);
  * free-stream fill (extension; the reference only has the uniform fill,
  * kernels/dsmc_kernel.cu:394-427): fields5 holds per cell (x fastest) the
  * number density n [m^-3], the mean velocity (u, v, w) [m/s] and the
- * temperature T [K].  Each cell receives n V_c / F_N particles (rounded
- * stochastically from the seed) drawn from the Maxwellian at (u, v, w, T);
- * cells covered by the mesh stay empty, as in dsmc_init_state; non-finite or
+ * temperature T [K].  n is the density averaged over the whole cell volume,
+ * the convention of dsmc_read_fields, so that fields sampled from a run seed
+ * each cell with the particle count it had: each cell receives n V_c / F_N
+ * particles (rounded stochastically from the seed) drawn from the Maxwellian
+ * at (u, v, w, T), in a cell the mesh cuts all of them in the part outside
+ * the body; a cell none of whose 4 x 4 x 4 sub-cell centres lies outside the
+ * mesh counts as covered and stays empty, as in dsmc_init_state; non-finite or
  * non-positive n gives an empty cell, a non-finite or non-positive T the
  * configured temperature.  Resets the sampling accumulators. */
 int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out);

@@ -69,3 +69,46 @@ def test_field_seeding(cuda):
     sol.RunSimulationStep(2e-6, 5)
     sol.Sync()
     sol.close()
+
+
+def test_field_seeding_fills_cut_cells_with_their_count(cuda):
+    """n is averaged over the whole cell (the convention of Fields()), so a
+    cell the body cuts receives all of its n V_c / F_N particles outside the
+    body, and sampled fields seed each cell with the count it had."""
+    sol = solver(seed=5)
+    dims = (32, 16, 16)
+    cells = dims[0] * dims[1] * dims[2]
+    h = np.array([1.2 / 32, 0.6 / 16, 0.6 / 16])
+    idx = np.arange(cells)
+    ijk = np.stack([idx % dims[0], (idx // dims[0]) % dims[1], idx // (dims[0] * dims[1])], 1)
+    lo = ijk * h
+    near = np.linalg.norm(np.clip(C, lo, lo + h) - C, axis=1)
+    # cells partly inside the body with a sub-cell centre (4 x 4 x 4 per
+    # cell, where the fill looks for the part outside the body) outside the
+    # sphere, and so outside its inscribed icosphere
+    g = (np.arange(4) + 0.5) / 4
+    sub = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    r_sub = np.linalg.norm(lo[:, None, :] + sub[None] * h - C, axis=2)
+    cut = (near < 0.97 * R) & (r_sub.max(axis=1) > 1.001 * R)
+    f = np.zeros((cells, 5), np.float32)
+    f[:, 0] = 1e20
+    f[:, 1] = 1000.0
+    f[:, 4] = 200.0
+    n = sol.InitFromFields(f)
+    a = sol.DownloadState()
+    assert a.shape[1] == n
+    r = np.linalg.norm(a[:3].T - C, axis=1)
+    assert np.sum(r < R * 0.99) <= 1e-3 * n
+    cx = np.minimum((a[:3].T / h).astype(np.int64), np.array(dims) - 1)
+    per = np.bincount(cx[:, 0] + dims[0] * (cx[:, 1] + dims[1] * cx[:, 2]), minlength=cells)
+    per_cell = 1e20 * float(np.prod(h)) / sol.settings.cfg.fnum  # 10
+    want = per_cell * np.count_nonzero(cut)
+    assert np.count_nonzero(cut) > 80
+    # every cell receives n V_c / F_N = 10 (the fractional part of the product
+    # is rounding); seeding only the part of each cell outside the body would
+    # give about half
+    assert abs(per[cut].sum() / want - 1) < 0.06
+    # cells away from the body hold the same count
+    clear = near > 1.2 * R
+    assert abs(per[clear].mean() / per_cell - 1) < 0.01
+    sol.close()
