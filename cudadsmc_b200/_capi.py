@@ -123,6 +123,7 @@ SIGNATURES = [
     ("dsmc_step", _I, [_P, ctypes.c_float, _I]),
     ("dsmc_step_graph", _I, [_P, ctypes.c_float, _I]),
     ("dsmc_init_from_fields", _I, [_P, _P, _P]),
+    ("dsmc_init_from_fields_two_stream", _I, [_P, _P, ctypes.c_float, _P]),
     ("dsmc_gemm_bf16", _I, [_I, _I, _I, _P, _I, _I, _P, _I, _I, _P, _I, ctypes.c_float, _P, _I, _P,
                             _I, _I, _P]),
     ("dsmc_gemm_check", _I, [_P]),

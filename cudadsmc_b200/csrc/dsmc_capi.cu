@@ -1056,11 +1056,12 @@ namespace {
 
 // Scratch of the extension fills inside the sampling accumulators (40 bytes
 // per cell, reset after the fill): per-cell Maxwellian state, an outside
-// point and the outside fraction.
+// point, the outside fraction and the free-stream share of a two-stream fill.
 float4* fill_state(dsmc_handle* h) { return reinterpret_cast<float4*>(h->acc); }
 float4* fill_point(dsmc_handle* h) { return reinterpret_cast<float4*>(h->acc) + h->cells; }
 float* fill_frac(dsmc_handle* h) { return reinterpret_cast<float*>(fill_point(h) + h->cells); }
-static_assert(2 * sizeof(float4) + sizeof(float) <= 5 * sizeof(double),
+float* fill_mix(dsmc_handle* h) { return fill_frac(h) + h->cells; }
+static_assert(2 * sizeof(float4) + 2 * sizeof(float) <= 5 * sizeof(double),
               "fill scratch must fit the accumulators");
 
 // Fraction of every cell outside the mesh (all ones without one).
@@ -1168,15 +1169,48 @@ int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out) 
   return finish_fill(h, ip, slot, count, n, n_out);
 }
 
-int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out) {
+namespace {
+
+// Free-stream share alpha of a cell with mean velocity u and temperature T
+// seen as a mixture of the free stream (U, T_inf) and a Maxwellian at the
+// wall temperature T_w with drift u_b: the mixture's mean and energy match
+// the cell's when
+//   alpha e_inf + (1 - alpha) e_w + |u - alpha U|^2 / (1 - alpha) = 3kT/m + |u|^2
+// (e = 3kT/m + |drift|^2 of a component), solved by bisection on
+// [0, 0.98]; 0 where the cell is colder than the wall or no root lies there.
+double two_stream_share(const double u[3], double T, const double U[3], double T_inf, double T_w,
+                        double kb_m) {
+  const double e_inf = 3.0 * kb_m * T_inf + U[0] * U[0] + U[1] * U[1] + U[2] * U[2];
+  const double e_w = 3.0 * kb_m * T_w;
+  const double rhs = 3.0 * kb_m * T + u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  auto f = [&](double a) {
+    const double d0 = u[0] - a * U[0], d1 = u[1] - a * U[1], d2 = u[2] - a * U[2];
+    return a * e_inf + (1.0 - a) * e_w + (d0 * d0 + d1 * d1 + d2 * d2) / (1.0 - a) - rhs;
+  };
+  double lo = 0.0, hi = 0.98;
+  if (!(f(lo) < 0.0 && f(hi) > 0.0)) return 0.0;
+  for (int it = 0; it < 60; it++) {
+    const double mid = 0.5 * (lo + hi);
+    (f(mid) > 0.0 ? hi : lo) = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+
+// dsmc_init_from_fields and its two-stream form (weight > 0).
+int seed_from_fields(dsmc_handle* h, const float* fields5, float weight, uint32_t* n_out) {
   if (!h || !fields5) return fail(h, DSMC_ERR_ARG, "null argument");
   const dsmc_config& c = h->cfg;
+  if (!(weight >= 0.f && weight <= 1.f)) return fail(h, DSMC_ERR_ARG, "two-stream weight outside [0, 1]");
+  const bool two = weight > 0.f;
+  if (two && !(c.wall_temp > 0.f)) return fail(h, DSMC_ERR_ARG, "two-stream fill needs a wall temperature");
   std::vector<float> frac;
   int st = outside_fractions(h, frac);
   if (st) return st;
   std::vector<uint32_t> slot(h->cells + 1), count(h->cells + 1, 0u);
   std::vector<float4> state(h->cells);
   std::vector<float2> maxrem(h->cells);
+  std::vector<float> share(two ? h->cells : 0);
+  const double U[3] = {c.stream_vel[0], c.stream_vel[1], c.stream_vel[2]};
   const bool geo = h->has_geom && c.geometry;
   const float kb_m = 1.3806e-23f / c.gas_mass;
   uint64_t mix = c.seed ^ 0x2545F4914F6CDD1Dull;
@@ -1198,6 +1232,26 @@ int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out)
     const float T = (std::isfinite(f[4]) && f[4] > 0.f) ? f[4] : c.temp;
     state[cell] = make_float4(std::isfinite(f[1]) ? f[1] : 0.f, std::isfinite(f[2]) ? f[2] : 0.f,
                               std::isfinite(f[3]) ? f[3] : 0.f, std::sqrt(kb_m * T));
+    if (two) {
+      // the share alpha from the free stream, the rest a Maxwellian whose
+      // drift and temperature keep the cell's mean and energy (the wall
+      // temperature itself at weight 1)
+      const double u[3] = {state[cell].x, state[cell].y, state[cell].z};
+      const double a = weight * two_stream_share(u, T, U, c.temp, c.wall_temp, kb_m);
+      share[cell] = (float)a;
+      if (a > 0.0) {
+        double ub[3], ub2 = 0.0, uu = 0.0, UU = 0.0;
+        for (int q = 0; q < 3; q++) {
+          ub[q] = (u[q] - a * U[q]) / (1.0 - a);
+          ub2 += ub[q] * ub[q];
+          uu += u[q] * u[q];
+          UU += U[q] * U[q];
+        }
+        const double e = (3.0 * kb_m * T + uu - a * (3.0 * kb_m * c.temp + UU)) / (1.0 - a) - ub2;
+        state[cell] = make_float4((float)ub[0], (float)ub[1], (float)ub[2],
+                                  (float)std::sqrt(std::max(e / 3.0, 0.0)));
+      }
+    }
     // (sigma g)max scaled to the cell's temperature like the initial value
     // (InitSimulationProperties, kernels/dsmc_kernel.cu:329-331)
     maxrem[cell] = make_float2(h->max_rel_vel * std::sqrt(std::max(T, c.temp) / c.temp),
@@ -1207,17 +1261,35 @@ int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out)
                         h->stream), "seed upload");
   CK(h, cudaMemcpyAsync(h->maxrem, maxrem.data(), h->cells * sizeof(float2), cudaMemcpyHostToDevice,
                         h->stream), "seed upload");
+  if (two)
+    CK(h, cudaMemcpyAsync(fill_mix(h), share.data(), h->cells * sizeof(float), cudaMemcpyHostToDevice,
+                          h->stream), "seed upload");
   dsmcb::InitParams ip{};
   ip.ppc = kmax;
   ip.kind = DSMC_INIT_MAXWELL;
   ip.seed = make_uint2((uint32_t)c.seed, (uint32_t)(c.seed >> 32));
   ip.cell_state = fill_state(h);
+  if (two) {
+    ip.cell_mix = fill_mix(h);
+    ip.stream = make_float3(c.stream_vel[0], c.stream_vel[1], c.stream_vel[2]);
+    ip.vstd = std::sqrt(kb_m * c.temp);
+  }
   ip.reject_inside = geo;
   if (geo) {
     ip.geom = base_params(h, c.dt).geom;
     ip.cell_point = fill_point(h);
   }
   return finish_fill(h, ip, slot, count, n, n_out);
+}
+
+}  // namespace
+
+int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out) {
+  return seed_from_fields(h, fields5, 0.f, n_out);
+}
+
+int dsmc_init_from_fields_two_stream(dsmc_handle* h, const float* fields5, float weight, uint32_t* n_out) {
+  return seed_from_fields(h, fields5, weight, n_out);
 }
 
 int dsmc_upload_state(dsmc_handle* h, const float* pos, const float* vel, uint32_t n, int soa) {

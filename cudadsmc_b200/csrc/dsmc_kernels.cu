@@ -482,6 +482,11 @@ __global__ void k_init_fill(const __grid_constant__ InitParams p) {
         const float4 cs = p.cell_state[cell];
         drift = make_float3(cs.x, cs.y, cs.z);
         sd = cs.w;
+        // a two-stream cell: a share of its particles from the free stream
+        if (p.cell_mix && r.uniform() < p.cell_mix[cell]) {
+          drift = p.stream;
+          sd = p.vstd;
+        }
       }
       const float r1 = r.uniform(), r2 = r.uniform(), r3 = r.uniform(), r4 = r.uniform();
       const float m1 = sd * sqrtf(-2.f * logf(r1)), m2 = sd * sqrtf(-2.f * logf(r3));

@@ -276,6 +276,8 @@ struct InitParams {
   const uint32_t* cell_slot;  // per cell: first particle index, kNone = skipped cell
   const uint32_t* cell_count; // per cell: particles to fill (<= ppc)
   const float4* cell_state;   // optional per cell (u, v, w, sqrt(kT/m)) of the Maxwellian
+  const float* cell_mix;      // optional per cell (with cell_state): the fraction of particles
+                              // drawn from the free stream (stream, vstd) instead
   int reject_inside;          // redraw positions that fall inside the mesh
   GeomView geom;
   const float4* cell_point;   // optional per cell: a point outside the mesh (w = 1) or none (w = 0)

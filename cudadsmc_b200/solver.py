@@ -124,6 +124,18 @@ class DSMCSolver:
         self._check(lib().dsmc_init_from_fields(self.h, _ptr(f), ctypes.byref(n)), "InitFromFields")
         return n.value
 
+    def InitFromFieldsTwoStream(self, fields, weight=1.0):
+        """InitFromFields with each cell a mixture of the free stream and a
+        Maxwellian at the wall temperature that keeps the cell's mean
+        velocity and energy (weight in [0, 1] scales the free-stream share)."""
+        f = np.ascontiguousarray(fields, np.float32).reshape(-1, 5)
+        if f.shape[0] != self.settings.getCellsCount():
+            raise ValueError("fields must hold one (n, u, v, w, T) row per cell")
+        n = ctypes.c_uint32()
+        self._check(lib().dsmc_init_from_fields_two_stream(self.h, _ptr(f), ctypes.c_float(weight),
+                                                           ctypes.byref(n)), "InitFromFieldsTwoStream")
+        return n.value
+
     def RunSimulationStep(self, dt, nsteps=1):
         self._check(lib().dsmc_step(self.h, dt, nsteps), "RunSimulationStep")
 

@@ -74,6 +74,23 @@ def make_solver(cond, seed):
     return sol
 
 
+def two_stream_weight(cond):
+    """Weight of the two-stream seeding (InitFromFieldsTwoStream) of a
+    condition: 0 at Kn 0.01, where the cells are near equilibrium, rising
+    with log Kn to 1 from Kn 0.32 on, where free-stream molecules and
+    molecules re-emitted by the wall share the cells."""
+    return float(np.clip((math.log10(cond[1]) + 2.0) / 1.5, 0.0, 1.0))
+
+
+def seed_from(sol, norm, cond, seeding):
+    """Seeds sol from normalized per-cell fields: a local Maxwellian per cell
+    ("maxwell") or the two-stream mixture weighted by the condition's Kn."""
+    f = physical_fields(norm, cond)
+    if seeding == "two-stream":
+        return sol.InitFromFieldsTwoStream(f, two_stream_weight(cond))
+    return sol.InitFromFields(f)
+
+
 def normalized_fields(sol, cond):
     """The sampled fields divided by the free stream (n_inf, U, U, U, T_inf);
     NaN in cells that received no particle."""
@@ -215,7 +232,8 @@ def generate(conds, seed, settle, sample, group=64, log=print):
     return out
 
 
-def convergence(conds, seeds, refs, ref_noise, window, max_steps, threshold, warm=None, stride=None):
+def convergence(conds, seeds, refs, ref_noise, window, max_steps, threshold, warm=None, stride=None,
+                seeding="maxwell"):
     """Steps until the systematic block-state error of the trailing window of
     `window` steps (its two halves give the noise, which is subtracted)
     against the reference falls to `threshold`, checked every `stride` steps
@@ -228,7 +246,7 @@ def convergence(conds, seeds, refs, ref_noise, window, max_steps, threshold, war
     sols = [make_solver(c, s) for c, s in zip(conds, seeds)]
     for i, sol in enumerate(sols):
         if warm is not None:
-            sol.InitFromFields(physical_fields(warm[i], conds[i]))
+            seed_from(sol, warm[i], conds[i], seeding)
         else:
             sol.InitSystemState()
     batch = cb.DSMCBatch(sols)
@@ -289,6 +307,9 @@ def main():
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--ideal", action="store_true",
                     help="also seed runs from the converged reference fields")
+    ap.add_argument("--seeding", choices=("two-stream", "maxwell"), default="two-stream",
+                    help="fill of the warm runs: the two-stream mixture weighted by Kn, or a local "
+                         "Maxwellian per cell (also run beside the two-stream fill for comparison)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
 
@@ -343,6 +364,7 @@ def main():
     pred_err_raw = [field_error(pred_blocks[i], refs[i]) for i in range(args.test)]
     cold_steps, warm_steps, cold_wall, warm_wall = [], [], 0.0, 0.0
     cold_curves, warm_curves = [], []
+    maxwell_steps = []  # warm runs from a local Maxwellian per cell, beside the two-stream fill
     for i in range(0, args.test, args.group):
         sl = slice(i, min(args.test, i + args.group))
         d, cc, w = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
@@ -351,17 +373,23 @@ def main():
         cold_curves += cc
         cold_wall += w
         d, cc, w = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
-                               args.max_steps, args.threshold, warm=pred[sl], stride=args.stride)
+                               args.max_steps, args.threshold, warm=pred[sl], stride=args.stride,
+                               seeding=args.seeding)
         warm_steps += d
         warm_curves += cc
         warm_wall += w
+        if args.seeding != "maxwell":
+            d, _, _ = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
+                                  args.max_steps, args.threshold, warm=pred[sl], stride=args.stride)
+            maxwell_steps += d
     # the seeding itself: runs seeded with the converged reference fields
     ideal_steps, ideal_curves = [], []
     if args.ideal:
         for i in range(0, args.test, args.group):
             sl = slice(i, min(args.test, i + args.group))
             d, cc, _ = convergence(test_c[sl], seeds_run[sl], refs[sl], ref_noise[sl], args.window,
-                                   args.max_steps, args.threshold, warm=ref_cells[sl], stride=args.stride)
+                                   args.max_steps, args.threshold, warm=ref_cells[sl], stride=args.stride,
+                                   seeding=args.seeding)
             ideal_steps += d
             ideal_curves += cc
     cs = np.array([s if s is not None else np.nan for s in cold_steps], np.float64)
@@ -389,6 +417,12 @@ def main():
                        "not_converged": int(np.sum(~np.isfinite(ws)))},
         "steps_speedup": {"median_ratio": float(np.median(cs[both] / ws[both])) if both.any() else None,
                           "ratio_of_means": float(np.mean(cs[both]) / np.mean(ws[both])) if both.any() else None},
+        "seeding": args.seeding,
+        "maxwell_warm_steps": {
+            "median": float(np.nanmedian([np.nan if d is None else d for d in maxwell_steps])),
+            "median_ratio": float(np.median([c / m for c, m in zip(cold_steps, maxwell_steps)
+                                             if c is not None and m is not None]))}
+        if maxwell_steps else None,
         "wall_s": {"cold": cold_wall, "warm": warm_wall},
         "cold_error_at_end": {"median": float(np.median(floor))},
         "seeded_from_reference": {
@@ -401,7 +435,8 @@ def main():
         "warm_curve_median": [float(np.median([c[k] for c in warm_curves if len(c) > k]))
                               for k in range(max(len(c) for c in warm_curves))],
         "conditions": [{"mach": float(c[0]), "kn": float(c[1]), "tw_ratio": float(c[2]), "r": float(c[3]),
-                        "pred_err": float(pe), "cold": cold_steps[i], "warm": warm_steps[i]}
+                        "pred_err": float(pe), "cold": cold_steps[i], "warm": warm_steps[i],
+                        "warm_maxwell": maxwell_steps[i] if maxwell_steps else None}
                        for i, (c, pe) in enumerate(zip(test_c, pred_err))],
     }
     js = json.dumps(res)

@@ -243,6 +243,20 @@ int dsmc_init_state(dsmc_handle* h, const float stream_vel[3], uint32_t* n_out);
  * configured temperature.  Resets the sampling accumulators. */
 int dsmc_init_from_fields(dsmc_handle* h, const float* fields5, uint32_t* n_out);
 
+/* dsmc_init_from_fields with each cell's Maxwellian replaced by a two-stream
+ * mixture (extension): a share alpha of the cell's particles is drawn from
+ * the free stream (the configured stream velocity and temperature), the
+ * rest from a Maxwellian whose drift and temperature keep the cell's mean
+ * velocity and energy.  alpha is weight times the share at which that rest
+ * has the wall temperature (the configured wall_temp, which must be
+ * positive), found per cell by bisection on [0, 0.98]; 0 where the cell is
+ * colder than the wall or no such share exists.  In rarefied flow a cell
+ * holds free-stream molecules beside molecules re-emitted by the wall, and a
+ * single Maxwellian with their mean and temperature relaxes to that only
+ * over a transit of the domain.  weight in [0, 1] (0: dsmc_init_from_fields
+ * itself); particle counts as dsmc_init_from_fields. */
+int dsmc_init_from_fields_two_stream(dsmc_handle* h, const float* fields5, float weight, uint32_t* n_out);
+
 /* Host <-> device particle state.  soa != 0: six arrays of n floats
  * (x,y,z,u,v,w) back to back; soa == 0: pos4 and vel4 float4 AoS as the
  * reference's particles_state_t.  Upload resets the cell order. */

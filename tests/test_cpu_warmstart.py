@@ -71,3 +71,10 @@ def test_inputs_and_free_stream():
     assert np.all(np.abs(x) <= 1.0 + 1e-6)
     n_inf, U = W.free_stream((2.0, 0.01, 1.0, 0.1))
     assert 5e20 < n_inf < 8e20 and 500 < U < 540
+
+
+def test_two_stream_weight_ramps_with_log_kn():
+    assert W.two_stream_weight((5.0, 0.01, 2.0, 0.1)) == 0.0
+    assert W.two_stream_weight((5.0, 0.005, 2.0, 0.1)) == 0.0
+    assert abs(W.two_stream_weight((5.0, 0.1, 2.0, 0.1)) - 2.0 / 3.0) < 1e-12
+    assert W.two_stream_weight((5.0, 0.5, 2.0, 0.1)) == 1.0

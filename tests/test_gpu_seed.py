@@ -1,6 +1,8 @@
 """Initial states: the Maxwellian fill and the field-seeded fill keep
 particles out of the body, and the seeded fill follows the given per-cell
 density, drift and temperature."""
+import math
+
 import numpy as np
 import pytest
 
@@ -112,3 +114,68 @@ def test_field_seeding_fills_cut_cells_with_their_count(cuda):
     clear = near > 1.2 * R
     assert abs(per[clear].mean() / per_cell - 1) < 0.01
     sol.close()
+
+
+def two_stream_share(u, T, U, T_inf, T_w):
+    """The free-stream share alpha at which the rest of a cell (mean u, x
+    only, temperature T) is a Maxwellian at T_w, by bisection."""
+    k = KB / M_AR
+    e_inf, e_w, rhs = 3 * k * T_inf + U * U, 3 * k * T_w, 3 * k * T + u * u
+
+    def f(a):
+        return a * e_inf + (1 - a) * e_w + (u - a * U) ** 2 / (1 - a) - rhs
+
+    lo, hi = 0.0, 0.98
+    assert f(lo) < 0 < f(hi)
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (lo, mid) if f(mid) > 0 else (mid, hi)
+    return 0.5 * (lo + hi)
+
+
+def test_two_stream_seeding(cuda):
+    """Each cell a mixture of the free stream (1000 m/s, 200 K) and a
+    Maxwellian at the wall temperature (300 K): the cell's mean velocity and
+    temperature are kept, and the share of particles in a box around the
+    free stream matches the mixture's; weight 0 is the plain seeding."""
+    dims = (32, 16, 16)
+    cells = dims[0] * dims[1] * dims[2]
+    f = np.zeros((cells, 5), np.float32)
+    f[:, 0] = 1e20
+    f[:, 1] = 500.0
+    f[:, 4] = 1600.0
+    sol = solver(seed=7)
+    n = sol.InitFromFieldsTwoStream(f, 1.0)
+    a = sol.DownloadState().astype(np.float64)
+    assert a.shape[1] == n
+    r = np.linalg.norm(a[:3].T - C, axis=1)
+    assert np.sum(r < R * 0.99) <= 1e-3 * n
+    u = a[3:6].mean(axis=1)
+    # the two streams lie 2200 m/s apart: the mean of about 80k particles
+    # scatters by about 3.5 m/s
+    assert abs(u[0] - 500.0) < 15 and abs(u[1]) < 5 and abs(u[2]) < 5
+    T = M_AR * a[3:6].var(axis=1).sum() / (3 * KB)
+    assert abs(T / 1600.0 - 1) < 0.02
+    alpha = two_stream_share(500.0, 1600.0, 1000.0, 200.0, 300.0)
+    ub = (500.0 - alpha * 1000.0) / (1 - alpha)
+    s_inf, s_w = math.sqrt(KB * 200.0 / M_AR), math.sqrt(KB * 300.0 / M_AR)
+
+    def phi(x):
+        return 0.5 * (1 + math.erf(x / math.sqrt(2)))
+
+    box = (np.abs(a[3] - 1000.0) < 2 * s_inf) & (np.abs(a[4]) < 2 * s_inf) & (np.abs(a[5]) < 2 * s_inf)
+    p_beam = (phi(2) - phi(-2)) ** 3
+    p_body = (phi((1000 + 2 * s_inf - ub) / s_w) - phi((1000 - 2 * s_inf - ub) / s_w)) * \
+        (phi(2 * s_inf / s_w) - phi(-2 * s_inf / s_w)) ** 2
+    assert abs(box.mean() - (alpha * p_beam + (1 - alpha) * p_body)) < 0.01
+    sol.close()
+    # weight 0: the plain seeding, particle for particle
+    s1, s2 = solver(seed=9), solver(seed=9)
+    n1 = s1.InitFromFields(f)
+    n2 = s2.InitFromFieldsTwoStream(f, 0.0)
+    assert n1 == n2
+    assert np.array_equal(s1.DownloadState(), s2.DownloadState())
+    with pytest.raises(Exception):
+        s2.InitFromFieldsTwoStream(f, 1.5)
+    s1.close()
+    s2.close()
