@@ -6,7 +6,7 @@ import math
 import numpy as np
 import pytest
 
-from cudadsmc_b200 import DSMCSolver, mesh_icosphere, settings_t
+from cudadsmc_b200 import DSMCSolver, DsmcError, mesh_icosphere, settings_t
 
 pytestmark = pytest.mark.gpu
 
@@ -175,7 +175,7 @@ def test_two_stream_seeding(cuda):
     n2 = s2.InitFromFieldsTwoStream(f, 0.0)
     assert n1 == n2
     assert np.array_equal(s1.DownloadState(), s2.DownloadState())
-    with pytest.raises(Exception):
+    with pytest.raises(DsmcError):
         s2.InitFromFieldsTwoStream(f, 1.5)
     s1.close()
     s2.close()
