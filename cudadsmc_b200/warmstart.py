@@ -1,7 +1,11 @@
 """Learned warm start of the sphere flow: generate steady fields with this
 DSMC, train the surrogate on them, and compare the time to steady state of
 warm-started runs (particles seeded from the predicted fields) with the
-plain cold start (free-stream fill) on held-out conditions.
+plain cold start (free-stream fill) on held-out conditions.  The warm runs
+use the two-stream fill, each cell a mixture of the free stream and
+molecules at the wall temperature weighted by the condition's Kn
+(`--seeding two-stream`, the default), and also, for comparison, a local
+Maxwellian per cell (`--seeding maxwell` runs that one alone).
 
 The flow: argon VHS (omega 0.81) at T_inf = 200 K over a diffuse sphere of
 radius r in a 1.2 x 0.6 x 0.6 m box of 64 x 32 x 32 cells, inflow at -x and
